@@ -1,0 +1,55 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line(
+        "markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    path = os.path.join(ROOT, "tests", "golden", "ref_fixtures.npz")
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def golden_csr(golden, name):
+    import scipy.sparse as sp
+    shape = tuple(int(v) for v in golden[name + "__shape"])
+    return sp.csr_matrix((golden[name + "__data"],
+                          golden[name + "__indices"],
+                          golden[name + "__indptr"]), shape=shape)
+
+
+def assert_csr_equal(A, B, rtol=1e-12, eliminate=False):
+    """Bit-exact structure and values within rtol of the largest entry."""
+    A = A.tocsr().copy()
+    B = B.tocsr().copy()
+    if eliminate:
+        A.eliminate_zeros()
+        B.eliminate_zeros()
+    assert A.shape == B.shape
+    np.testing.assert_array_equal(np.asarray(A.indptr, np.int64),
+                                  np.asarray(B.indptr, np.int64))
+    np.testing.assert_array_equal(np.asarray(A.indices, np.int64),
+                                  np.asarray(B.indices, np.int64))
+    scale = max(float(np.abs(B.data).max(initial=0.0)), 1e-300)
+    err = float(np.abs(A.data - B.data).max(initial=0.0)) / scale
+    assert err <= rtol, f"CSR values differ: {err:.3e} > {rtol:.1e}"
+
+
+def assert_close(a, b, rtol=1e-12, what=""):
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    assert a.shape == b.shape, f"{what}: shape {a.shape} vs {b.shape}"
+    scale = max(float(np.abs(b).max(initial=0.0)), 1e-300)
+    err = float(np.abs(a - b).max(initial=0.0)) / scale
+    assert err <= rtol, f"{what}: rel err {err:.3e} > {rtol:.1e}"
