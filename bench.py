@@ -1,0 +1,357 @@
+"""Benchmark of the assembly -> CSR -> solve hot path on B200.
+
+Default workload: Tet10 3D elasticity, box 2.0 x 0.25 x 0.25 m,
+80 x 10 x 10 Kuhn cells (48,000 Tet10 elements, 71,001 nodes, 213,003
+DOFs, 211,680 free), E = 210 GPa, nu = 0.3, clamped at x = 0, 1 MPa
+traction in -z on x = 2 m, FP32 PCG with FP64 reliable updates to 1e-10
+relative residual. One step = pattern build + Tet10 element matrices +
+CSR reduction + traction load + Dirichlet masking + solve.
+
+value  : solved (free) DOF/s with the mesh already resident in HBM.
+e2e    : the same through the public API solve_elasticity_tet10(...) with
+         host numpy inputs (host->device copies and the solution read-back
+         inside the timed region).
+--impl reference : the CPU oracle (a NumPy/SciPy restatement of the
+         reference: vectorised assembly + SuperLU) on a bounded sample of
+         the workload, on the host cores.
+
+Multi-GPU: the path solves independent systems, so --gpus N runs N
+replicas (one process per GPU) and reports the aggregate DOF/s.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("solved DOF/s at 1e-8 rel err vs FP64 plain GPU path; "
+          "p50/p99 latency")
+E, NU = 210e9, 0.3
+BC = {"xmin": (0.0, 0.0, 0.0)}
+TRACTION = {"xmax": (0.0, 0.0, -1e6)}
+BEAM = dict(xlim=(0.0, 2.0), ylim=(0.0, 0.25), zlim=(0.0, 0.25))
+FULL = (80, 10, 10)
+CPU_SAMPLE = (40, 5, 5)
+RTOL = 1e-10
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+             "sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(self.NAMES, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _beam(shape):
+    from cloudfem_b200.mesh import box_mesh_tet10
+    return box_mesh_tet10(*shape, **BEAM)
+
+
+def _free_dofs(mesh):
+    return 3 * mesh.n_nodes - 3 * len(mesh.boundaries["xmin"])
+
+
+def pcg_bytes(n_nodes, nnzb, iters, updates):
+    """Algorithmic HBM bytes of one mixed-precision (bs = 3) solve launch.
+
+    Phase A per iteration: FP32 3x3 blocks + column index (40 B / block),
+    row pointers, read z and p, write p and q (4 x 12 B / node).
+    Phase B: read p, q, r, dinv (36 B), fixed mask (3 B), x (24 B), write
+    x, r, z: 12*3 + 36 + 3 + 24 + 24 + 12*2 = 147 B / node.
+    Phase R (reliable update, plus INIT once): FP64 blocks + index
+    (76 B / block), row pointers, read x, b (48 B), fixed mask (3 B), write
+    r, z (24 B).
+    """
+    a = nnzb * 40 + 4 * (n_nodes + 1) + 48 * n_nodes
+    b = 147 * n_nodes
+    r = nnzb * 76 + 4 * (n_nodes + 1) + 75 * n_nodes
+    return iters * (a + b) + (updates + 1) * r
+
+
+def _device_step(dm, mesh, precision):
+    """Pattern + assembly + loads + masking + solve on resident inputs."""
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200._driver import last_solve_info, solve_block
+    from cloudfem_b200.device import fixed_vector
+    from cloudfem_b200.physics.elastic3d import _assemble
+    dm._pattern = None                      # rebuild the CSR structure
+    vals, rhs = _assemble(dm, mesh, N.OP_T10_ELAST, E, NU, None, TRACTION,
+                          None, 0.0, 0.0, tet10=True)
+    idx, v = fixed_vector(mesh, BC)
+    x = solve_block(dm, 3, vals, rhs, idx, v, precision, RTOL,
+                    what="bench solve")
+    return x, last_solve_info()[0]
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import DeviceMesh
+    from cloudfem_b200.physics.elastic_tet10 import solve_elasticity_tet10
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rt = N.runtime(local_rank)
+    mesh = _beam(FULL)
+    free = _free_dofs(mesh)
+    dm = DeviceMesh(mesh, local_rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    # FP64 plain reference solution (accuracy gate) and its speed.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x64, info64 = _device_step(dm, mesh, "fp64")
+    torch.cuda.synchronize()
+    fp64_s = time.perf_counter() - t0
+    u64 = x64.clone()
+
+    for _ in range(args.warmup):
+        _device_step(dm, mesh, args.precision)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing (value)
+    times, infos = [], []
+    l0 = rt.launches()
+    barrier()
+    with Clocks(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)                # evict L2 between steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            x, info = _device_step(dm, mesh, args.precision)
+            e1.record()
+            infos.append(info)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    barrier()
+    launches = rt.launches() - l0
+    err = float(torch.linalg.norm(x - u64) / torch.linalg.norm(u64))
+
+    # ---- end-to-end through the public API (host inputs and outputs)
+    for _ in range(1):
+        solve_elasticity_tet10(mesh, E, NU, bc=BC, traction=TRACTION,
+                               precision=args.precision, rtol=RTOL)
+    e2e_times = []
+    barrier()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve_elasticity_tet10(mesh, E, NU, bc=BC, traction=TRACTION,
+                               precision=args.precision, rtol=RTOL)
+        torch.cuda.synchronize()
+        e2e_times.append((time.perf_counter() - t0) * 1e3)
+    barrier()
+
+    ms = float(np.sum(times))
+    e2e_ms = float(np.sum(e2e_times))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        return None
+
+    pat = dm.pattern
+    last = infos[-1]
+    bytes_launch = pcg_bytes(mesh.n_nodes, pat.nnz, last.iterations,
+                             last.residual_updates)
+    peak, peak_kind = _peaks()
+    achieved = bytes_launch / (last.kernel_ms * 1e-3) / 1e9
+    h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
+    d2h = 3 * mesh.n_nodes * 8
+    out = {
+        "metric": METRIC,
+        "value": world * free * args.steps / (ms * 1e-3),
+        "unit": "DOF/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 PCG + f64 residual/update" if args.precision == "mixed"
+                 else "f64",
+        "data": "synthetic (structured Kuhn Tet10 beam, no dataset)",
+        "config": {
+            "workload": "tet10_elasticity_beam_80x10x10",
+            "elements": int(mesh.n_elements), "nodes": int(mesh.n_nodes),
+            "dofs": int(3 * mesh.n_nodes), "free_dofs": int(free),
+            "precision": args.precision, "rtol": RTOL,
+            "iterations": last.iterations,
+            "residual_updates": last.residual_updates,
+            "rel_err_vs_fp64_plain": err,
+            "fp64_plain": {"iterations": info64.iterations,
+                           "dof_per_s": free / fp64_s,
+                           "kernel_ms": info64.kernel_ms},
+            "l2": "256 MiB buffer written between timed steps",
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {"value": world * free * args.steps / (e2e_ms * 1e-3),
+                "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {
+            "kernel": "k_pcg_persistent",
+            "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+            "bytes_per_launch": bytes_launch,
+            "kernel_ms": last.kernel_ms,
+            "traffic": None,
+        },
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline()
+    return out
+
+
+def cpu_baseline(shape=CPU_SAMPLE):
+    """The oracle (NumPy + SuperLU) on a bounded sample of the workload."""
+    from oracle import cfem_oracle as O
+    m = O.box_mesh_tet10(*shape, **BEAM)
+    free = 3 * m.n_nodes - 3 * len(m.boundaries["xmin"])
+    t0 = time.perf_counter()
+    O.solve_elasticity_tet10(m, E, NU, bc=BC, traction=TRACTION)
+    dt = time.perf_counter() - t0
+    return {"value": free / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"Tet10 beam {shape[0]}x{shape[1]}x{shape[2]} cells "
+                      f"({free} free DOFs), one solve, {dt:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    per = []
+    for i in range(args.warmup + args.steps):
+        c = cpu_baseline()
+        if i >= args.warmup:
+            per.append(c)
+    value = float(np.mean([c["value"] for c in per]))
+    c = per[-1]
+    c["value"] = value
+    return {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": "DOF/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": float(np.mean([c["seconds"] for c in per])) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "tet10_elasticity_beam_80x10x10",
+                   "sample": c["sample"]},
+        "cpu_baseline": c,
+        "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl",
+                                    timeout=datetime.timedelta(seconds=300))
+        out = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,221 @@
+// Context, error state and small sparse helpers of libcfem.
+#include "cfem_common.cuh"
+#include "cfem_tables.cuh"
+
+#include <string.h>
+
+namespace cfem {
+
+static thread_local char g_err[1024] = "";
+std::atomic<int64_t> g_launches{0};
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int set_device(int device) {
+    CFEM_CUDA(cudaSetDevice(device));
+    return CFEM_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+__global__ void k_axpby(int64_t n, double a, const double *__restrict__ x,
+                        double b, const double *__restrict__ y,
+                        double *__restrict__ out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double xv = x ? a * x[i] : 0.0;
+        double yv = y ? b * y[i] : 0.0;
+        out[i] = xv + yv;
+    }
+}
+
+__global__ void k_to_fp32(int64_t n, const double *__restrict__ in,
+                          float *__restrict__ out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = (float)in[i];
+}
+
+// y = alpha A x + beta y, one thread per block row (setup-time use only).
+template <int BS>
+__global__ void k_spmv(int64_t n, const int32_t *__restrict__ rp,
+                       const int32_t *__restrict__ ci,
+                       const double *__restrict__ v, double alpha,
+                       const double *__restrict__ x, double beta,
+                       double *__restrict__ y) {
+    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double acc[BS];
+#pragma unroll
+    for (int c = 0; c < BS; ++c) acc[c] = 0.0;
+    for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+        int64_t j = ci[k];
+#pragma unroll
+        for (int c = 0; c < BS; ++c)
+#pragma unroll
+            for (int d = 0; d < BS; ++d)
+                acc[c] += v[(int64_t)k * BS * BS + c * BS + d] * x[j * BS + d];
+    }
+#pragma unroll
+    for (int c = 0; c < BS; ++c) {
+        double yv = beta == 0.0 ? 0.0 : beta * y[r * BS + c];
+        y[r * BS + c] = alpha * acc[c] + yv;
+    }
+}
+
+// Adds a canonical CSR addend into pattern values (subset pattern).
+__global__ void k_csr_add_subset(int64_t n, const int32_t *__restrict__ rp,
+                                 const int32_t *__restrict__ col,
+                                 const int32_t *__restrict__ aptr,
+                                 const int32_t *__restrict__ aidx,
+                                 const double *__restrict__ aval,
+                                 double *__restrict__ vals, int *bad) {
+    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int32_t lo0 = rp[r], hi0 = rp[r + 1];
+    for (int32_t t = aptr[r]; t < aptr[r + 1]; ++t) {
+        int32_t c = aidx[t];
+        int32_t lo = lo0, hi = hi0;
+        while (lo < hi) {
+            int32_t mid = (lo + hi) >> 1;
+            if (col[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        if (lo < hi0 && col[lo] == c) vals[lo] += aval[t];
+        else atomicExch(bad, 1);
+    }
+}
+
+}  // namespace cfem
+
+using namespace cfem;
+
+extern "C" {
+
+const char *cfem_last_error(void) { return g_err; }
+
+int cfem_version(void) { return 10000; }
+
+int cfem_ctx_create(int device, cfem_ctx **out) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(out != nullptr, CFEM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    CFEM_CUDA(cudaGetDeviceCount(&ndev));
+    CFEM_CHECK(device >= 0 && device < ndev, CFEM_ERR_INVALID,
+               "device %d out of range (%d devices)", device, ndev);
+    CFEM_TRY(set_device(device));
+    cudaDeviceProp prop;
+    CFEM_CUDA(cudaGetDeviceProperties(&prop, device));
+    CFEM_CHECK(prop.major == 10, CFEM_ERR_UNSUPPORTED,
+               "libcfem is built for sm_100a; device %d is sm_%d%d (%s)",
+               device, prop.major, prop.minor, prop.name);
+    CFEM_TRY(upload_tables(device));
+    cfem_ctx *c = new cfem_ctx();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    c->launches_at_create = g_launches.load();
+    *out = c;
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+int cfem_ctx_destroy(cfem_ctx *ctx) {
+    delete ctx;
+    return CFEM_OK;
+}
+
+int64_t cfem_ctx_launch_count(const cfem_ctx *ctx) {
+    (void)ctx;
+    return g_launches.load();
+}
+
+int cfem_axpby(cfem_ctx *ctx, int64_t n, double a, const double *d_x,
+               double b, const double *d_y, double *d_out, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_out && n >= 0, CFEM_ERR_INVALID, "cfem_axpby: bad args");
+    if (n == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned g = grid_for(n, 256);
+    if (g > (unsigned)ctx->num_sms * 16) g = ctx->num_sms * 16;
+    CFEM_LAUNCH(k_axpby, g, 256, 0, s, n, a, d_x, b, d_y, d_out);
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+int cfem_to_fp32(cfem_ctx *ctx, int64_t n, const double *d_in, float *d_out,
+                 void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_in && d_out && n >= 0, CFEM_ERR_INVALID,
+               "cfem_to_fp32: bad args");
+    if (n == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    unsigned g = grid_for(n, 256);
+    if (g > (unsigned)ctx->num_sms * 16) g = ctx->num_sms * 16;
+    CFEM_LAUNCH(k_to_fp32, g, 256, 0, (cudaStream_t)stream, n, d_in, d_out);
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
+              const int32_t *d_row_ptr, const int32_t *d_col,
+              const double *d_vals, double alpha, const double *d_x,
+              double beta, double *d_y, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_row_ptr && d_col && d_vals && d_x && d_y &&
+                   n_rows >= 0 && (bs == 1 || bs == 3),
+               CFEM_ERR_INVALID, "cfem_spmv: bad args");
+    if (n_rows == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned g = grid_for(n_rows, 128);
+    if (bs == 1)
+        CFEM_LAUNCH(k_spmv<1>, g, 128, 0, s, n_rows, d_row_ptr, d_col, d_vals,
+                    alpha, d_x, beta, d_y);
+    else
+        CFEM_LAUNCH(k_spmv<3>, g, 128, 0, s, n_rows, d_row_ptr, d_col, d_vals,
+                    alpha, d_x, beta, d_y);
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+int cfem_csr_add_subset(cfem_ctx *ctx, const cfem_pattern *p,
+                        const int32_t *d_aptr, const int32_t *d_aidx,
+                        const double *d_aval, int64_t n_rows, double *d_vals,
+                        void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && p && d_aptr && d_vals && n_rows == p->n_nodes,
+               CFEM_ERR_INVALID, "cfem_csr_add_subset: bad args");
+    if (n_rows == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    int *d_bad = nullptr;
+    CFEM_TRY(tmp_alloc(&d_bad, 1, s));
+    CFEM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+    CFEM_LAUNCH(k_csr_add_subset, grid_for(n_rows, 128), 128, 0, s, n_rows,
+                p->row_ptr, p->col, d_aptr, d_aidx, d_aval, d_vals, d_bad);
+    int bad = 0;
+    CFEM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+    tmp_free(d_bad, s);
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    CFEM_CHECK(!bad, CFEM_ERR_INVALID,
+               "addend has entries outside the mesh sparsity pattern");
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,446 @@
+"""Device-resident meshes, patterns, assembly and solves over libcfem.
+
+This is the host half of the drop-in boundary: it keeps the reference's
+host-side semantics (coefficient callables evaluated on the host into
+per-element or per-quadrature-point arrays, boundary dictionaries, SciPy
+CSR results) and hands all element, CSR and solver work to the CUDA
+library through the C ABI of ``include/cfem.h``. Device memory is held in
+torch tensors (plumbing only); every kernel is libcfem's.
+"""
+
+import ctypes
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _native as N
+from ._native import ptr
+
+# Keast 5-point rule (cloudfem/fem/tet10.py:84-100).
+_A, _B = 0.5, 1.0 / 6.0
+KEAST_L = np.array([[0.25, 0.25, 0.25, 0.25], [_A, _B, _B, _B],
+                    [_B, _A, _B, _B], [_B, _B, _A, _B], [_B, _B, _B, _A]])
+KEAST_W = np.array([-4.0 / 5.0] + [9.0 / 20.0] * 4)
+
+# Local corner triples of the four faces (cloudfem/fem/tet_heat.py:112 and
+# the Tet10 table of cloudfem/fem/tet10.py:287-292).
+FACES_P1 = ((0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3))
+FACES_T10 = (((0, 1, 2), (4, 5, 6)), ((0, 3, 1), (7, 8, 4)),
+             ((0, 2, 3), (6, 9, 7)), ((1, 3, 2), (8, 9, 5)))
+
+
+def _torch():
+    import torch
+    return torch
+
+
+# ------------------------------------------------------------ host helpers
+
+def evaluate(spec, pts):
+    """Evaluate a float or callable(x, y, z) at points (..., 3).
+
+    Constants stay Python floats. Callables are tried once on whole arrays
+    and fall back to one call per point (the reference's convention) when
+    they do not broadcast.
+    """
+    if not callable(spec):
+        return float(spec)
+    shape = pts.shape[:-1]
+    flat = pts.reshape(-1, 3)
+    try:
+        with np.errstate(all="ignore"):
+            v = np.asarray(spec(flat[:, 0], flat[:, 1], flat[:, 2]),
+                           dtype=float)
+        if v.shape == (flat.shape[0],):
+            return v.reshape(shape)
+        if v.ndim == 0:
+            return np.full(shape, float(v))
+    except Exception:  # noqa: BLE001 - callable is scalar-only
+        pass
+    return np.fromiter((spec(x, y, z) for x, y, z in flat), dtype=float,
+                       count=flat.shape[0]).reshape(shape)
+
+
+def centroids(nodes, elements):
+    return nodes[elements[:, :4]].mean(axis=1)
+
+
+def keast_points(nodes, elements):
+    p = nodes[elements[:, :4]]
+    return np.einsum("qc,ecd->eqd", KEAST_L, p)
+
+
+def fixed_scalar(mesh, bc):
+    """{name|'all': value|callable} -> sorted node ids and values.
+
+    Later names overwrite earlier ones, as the dict in
+    cloudfem/fem/tet_poisson.py:85-93 does.
+    """
+    n = mesh.n_nodes
+    if not bc:
+        return np.zeros(0, np.int64), np.zeros(0)
+    val = np.zeros(n)
+    has = np.zeros(n, dtype=bool)
+    for name, value in bc.items():
+        ids = (np.arange(n) if name == "all"
+               else np.asarray(mesh.boundaries[name], dtype=np.int64))
+        v = evaluate(value, mesh.nodes[ids])
+        val[ids] = v
+        has[ids] = True
+    idx = np.nonzero(has)[0]
+    return idx, val[idx]
+
+
+def fixed_vector(mesh, bc):
+    """elastic3d.py:204-218: (name|'all') -> (ux, uy, uz), None = free."""
+    n = mesh.n_nodes
+    val = np.zeros(3 * n)
+    has = np.zeros(3 * n, dtype=bool)
+    for name, vals in (bc or {}).items():
+        ids = (np.arange(n) if name == "all"
+               else np.asarray(mesh.boundaries[name], dtype=np.int64))
+        for comp, v in enumerate(vals):
+            if v is None:
+                continue
+            dofs = 3 * ids + comp
+            val[dofs] = evaluate(v, mesh.nodes[ids])
+            has[dofs] = True
+    idx = np.nonzero(has)[0]
+    return idx, val[idx]
+
+
+# ------------------------------------------------------------ device objects
+
+class Pattern:
+    """Node-level sparsity of a mesh (owned libcfem handle)."""
+
+    def __init__(self, rt, handle, n_nodes, nnz):
+        self.rt = rt
+        self.handle = handle
+        self.n_nodes = n_nodes
+        self.nnz = nnz
+        rp, col = N._vp(), N._vp()
+        N.check(rt.lib.cfem_pattern_node_csr(handle, ctypes.byref(rp),
+                                             ctypes.byref(col)))
+        self.row_ptr = rp
+        self.col = col
+
+    def expand(self, bs):
+        """Device DOF-level CSR indptr / indices for bs DOFs per node."""
+        torch = _torch()
+        dev = self.rt.device
+        indptr = torch.empty(self.n_nodes * bs + 1, dtype=torch.int32,
+                             device=dev)
+        indices = torch.empty(max(self.nnz * bs * bs, 1), dtype=torch.int32,
+                              device=dev)
+        N.check(self.rt.lib.cfem_pattern_expand(
+            self.handle, bs, ptr(indptr), ptr(indices), self.rt.stream()))
+        return indptr, indices[: self.nnz * bs * bs]
+
+    def to_scipy(self, bs, vals):
+        """scipy csr_matrix of block values (nnz*bs*bs) in DOF order."""
+        torch = _torch()
+        indptr, indices = self.expand(bs)
+        if bs > 1:
+            flat = torch.empty_like(vals)
+            N.check(self.rt.lib.cfem_block_to_csr(
+                self.handle, bs, ptr(vals), ptr(flat), self.rt.stream()))
+        else:
+            flat = vals
+        n = self.n_nodes * bs
+        A = sp.csr_matrix((flat.cpu().numpy(), indices.cpu().numpy(),
+                           indptr.cpu().numpy()), shape=(n, n))
+        A.has_sorted_indices = True
+        return A
+
+    def __del__(self):
+        try:
+            self.rt.lib.cfem_pattern_destroy(self.handle)
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+class DeviceMesh:
+    """Nodes (N, 3) f64 and int32 connectivity (M, 4|10) resident in HBM."""
+
+    def __init__(self, mesh, device=None):
+        torch = _torch()
+        self.rt = N.runtime(device)
+        self.host = mesh
+        nodes = np.ascontiguousarray(mesh.nodes, dtype=np.float64)
+        els = np.asarray(mesh.elements)
+        if els.ndim != 2 or els.shape[1] not in (4, 10):
+            raise ValueError(f"elements must be (M, 4) or (M, 10), got "
+                             f"{els.shape}")
+        if nodes.ndim != 2 or nodes.shape[1] != 3:
+            raise ValueError(f"nodes must be (N, 3), got {nodes.shape}")
+        if els.size and (els.min() < 0 or els.max() >= nodes.shape[0]):
+            raise ValueError("element connectivity references a node id "
+                             f"outside [0, {nodes.shape[0]})")
+        self.n_nodes = nodes.shape[0]
+        self.n_elems = els.shape[0]
+        self.npe = els.shape[1]
+        dev = self.rt.device
+        self.nodes = torch.from_numpy(nodes).to(dev, non_blocking=True)
+        self.elems = torch.from_numpy(
+            np.ascontiguousarray(els, dtype=np.int32)).to(dev,
+                                                          non_blocking=True)
+        self._pattern = None
+
+    @property
+    def pattern(self):
+        if self._pattern is None:
+            h = N._vp()
+            N.check(self.rt.lib.cfem_pattern_create(
+                self.rt.ctx, ptr(self.elems), self.n_elems, self.npe,
+                self.n_nodes, self.rt.stream(), ctypes.byref(h)))
+            n, nnz = N._i64(), N._i64()
+            N.check(self.rt.lib.cfem_pattern_info(h, ctypes.byref(n),
+                                                  ctypes.byref(nnz)))
+            self._pattern = Pattern(self.rt, h, n.value, nnz.value)
+        return self._pattern
+
+    # ------------------------------------------------------ coefficients
+    def coef(self, spec, where):
+        """cfem_coef for a float/callable sampled at 'centroid' or 'qp'.
+
+        Returns (struct, keepalive) - the tensor must outlive the launch.
+        """
+        if not callable(spec):
+            return N.Coef(None, float(spec), N.COEF_CONST, 0), None
+        host = self.host
+        els = np.asarray(host.elements)
+        if where == "qp":
+            vals = evaluate(spec, keast_points(host.nodes, els))
+            mode = N.COEF_QP
+        else:
+            vals = evaluate(spec, centroids(host.nodes, els))
+            mode = N.COEF_ELEM
+        if np.isscalar(vals):
+            return N.Coef(None, float(vals), N.COEF_CONST, 0), None
+        t = _torch().from_numpy(np.ascontiguousarray(vals, dtype=float)).to(
+            self.rt.device)
+        return N.Coef(ptr(t), 0.0, mode, 0), t
+
+    def nodal_coef(self, values):
+        t = _torch().from_numpy(
+            np.ascontiguousarray(values, dtype=float)).to(self.rt.device)
+        if t.numel() != self.n_nodes:
+            raise ValueError(f"nodal field has {t.numel()} values, mesh has "
+                             f"{self.n_nodes} nodes")
+        return N.Coef(ptr(t), 0.0, N.COEF_NODAL, 0), t
+
+    # ------------------------------------------------------ assembly
+    def assemble(self, op, coef=1.0, load=None, vals=None, rhs=None,
+                 accumulate=False):
+        """Scalar operator into device (vals[nnz], rhs[N])."""
+        torch = _torch()
+        pat = self.pattern
+        dev = self.rt.device
+        where = "qp" if op == N.OP_T10_STIFF else "centroid"
+        kc, keep1 = self.coef(coef, where)
+        if vals is None:
+            vals = torch.empty(pat.nnz, dtype=torch.float64, device=dev)
+        lc, keep2 = (self.coef(load, where) if load is not None
+                     else (N.Coef(None, 0.0, N.COEF_CONST, 0), None))
+        if rhs is None and load is not None:
+            rhs = torch.empty(self.n_nodes, dtype=torch.float64, device=dev)
+        N.check(self.rt.lib.cfem_assemble(
+            self.rt.ctx, pat.handle, op, ptr(self.nodes), ptr(self.elems),
+            ctypes.byref(kc), ctypes.byref(lc), ptr(vals), ptr(rhs),
+            1 if accumulate else 0, self.rt.stream()))
+        del keep1, keep2
+        return vals, rhs
+
+    def assemble_elastic(self, op, E, nu, body=None, T=None, alpha=0.0,
+                         T_ref=0.0, vals=None, rhs=None):
+        torch = _torch()
+        pat = self.pattern
+        dev = self.rt.device
+        where = "qp" if op == N.OP_T10_ELAST else "centroid"
+        keep = []
+        b3 = (N.Coef * 3)()
+        comps = list(body) if body is not None else [0.0, 0.0, 0.0]
+        if len(comps) != 3:
+            raise ValueError("body force needs three components")
+        for c, v in enumerate(comps):
+            b3[c], k = self.coef(0.0 if v is None else v, where)
+            keep.append(k)
+        tcoef = None
+        if T is not None and alpha != 0.0:
+            if callable(T):
+                tcoef, k = self.coef(T, where)
+            else:
+                tcoef, k = self.nodal_coef(T)
+            keep.append(k)
+        if vals is None:
+            vals = torch.empty(pat.nnz * 9, dtype=torch.float64, device=dev)
+        if rhs is None:
+            rhs = torch.empty(3 * self.n_nodes, dtype=torch.float64,
+                              device=dev)
+        N.check(self.rt.lib.cfem_assemble_elastic(
+            self.rt.ctx, pat.handle, op, ptr(self.nodes), ptr(self.elems),
+            float(E), float(nu), b3,
+            ctypes.byref(tcoef) if tcoef is not None else None,
+            float(alpha), float(T_ref), ptr(vals), ptr(rhs), 0,
+            self.rt.stream()))
+        del keep
+        return vals, rhs
+
+    # ------------------------------------------------------ faces
+    def boundary_faces(self, name, tet10=False):
+        """Exterior faces on a named node set, in the reference's order.
+
+        Faces whose key (sorted corner triple) occurs once among all element
+        faces and whose corners are all in the set, listed at their first
+        occurrence in element order (tet_heat.py:97-120, tet10.py:329-352).
+        Only faces with all corners in the set can share a key with such a
+        face, so counting among the device-selected candidates is exact.
+        """
+        torch = _torch()
+        host = self.host
+        ids = np.asarray(host.boundaries[name], dtype=np.int64)
+        width = 6 if tet10 else 3
+        if ids.size == 0 or self.n_elems == 0:
+            return np.zeros((0, width), dtype=np.int64)
+        inset = torch.zeros(self.n_nodes, dtype=torch.uint8,
+                            device=self.rt.device)
+        inset[torch.from_numpy(ids).to(self.rt.device)] = 1
+        out = torch.empty(self.n_elems * 4, dtype=torch.int64,
+                          device=self.rt.device)
+        cnt = N._i64()
+        N.check(self.rt.lib.cfem_face_candidates(
+            self.rt.ctx, ptr(self.elems), self.n_elems, self.npe,
+            1 if tet10 else 0, ptr(inset), self.n_nodes, ptr(out),
+            ctypes.byref(cnt), self.rt.stream()))
+        cand = out[: cnt.value].cpu().numpy()
+        if cand.size == 0:
+            return np.zeros((0, width), dtype=np.int64)
+        e, f = cand // 4, cand % 4
+        els = np.asarray(host.elements, dtype=np.int64)
+        if tet10:
+            table = np.array([c + m for c, m in FACES_T10])
+        else:
+            table = np.array(FACES_P1)
+        full = els[e[:, None], table[f]]
+        keys = np.sort(full[:, :3], axis=1)
+        _, first, counts = np.unique(keys, axis=0, return_index=True,
+                                     return_counts=True)
+        keep = np.sort(first[counts == 1])
+        return full[keep]
+
+
+# ------------------------------------------------------------ solver
+
+class SolveResult:
+    def __init__(self, stats):
+        self.status = int(stats.status)
+        self.iterations = int(stats.iterations)
+        self.residual_updates = int(stats.residual_updates)
+        self.relres = float(stats.relres)
+        self.bnorm = float(stats.bnorm)
+        self.kernel_ms = float(stats.kernel_ms)
+
+    def __repr__(self):
+        return (f"SolveResult(status={N.STATUS_NAMES.get(self.status)}, "
+                f"iterations={self.iterations}, relres={self.relres:.3e}, "
+                f"residual_updates={self.residual_updates})")
+
+
+class BlockSystem:
+    """One SPD block-CSR system on the device, ready for cfem_pcg_solve."""
+
+    def __init__(self, rt, n_rows, bs, row_ptr, col, vals64, b, x,
+                 fixed=None, vals32=None, precond=None, keep=()):
+        self.rt = rt
+        self.n_rows = n_rows
+        self.bs = bs
+        self.row_ptr = row_ptr        # c_void_p or tensor
+        self.col = col
+        self.vals64 = vals64
+        self.vals32 = vals32
+        self.b = b
+        self.x = x
+        self.fixed = fixed
+        self.precond = (precond if precond is not None else
+                        (N.PRECOND_BLOCK if bs == 3 else N.PRECOND_JACOBI))
+        self.keep = keep
+
+    def ensure_fp32(self):
+        torch = _torch()
+        if self.vals32 is None:
+            n = self.vals64.numel()
+            self.vals32 = torch.empty(n, dtype=torch.float32,
+                                      device=self.vals64.device)
+            N.check(self.rt.lib.cfem_to_fp32(
+                self.rt.ctx, n, ptr(self.vals64), ptr(self.vals32),
+                self.rt.stream()))
+        return self.vals32
+
+    def linsys(self, mode, rtol, max_iter):
+        def p(v):
+            return v if isinstance(v, N._vp) else ptr(v)
+        v32 = self.ensure_fp32() if mode == N.SOLVE_MIXED else None
+        return N.LinSys(self.n_rows, self.bs, self.precond, p(self.row_ptr),
+                        p(self.col), ptr(self.vals64), ptr(v32), ptr(self.b),
+                        ptr(self.x), ptr(self.fixed), float(rtol),
+                        int(max_iter), int(mode))
+
+
+def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None):
+    """Solve a batch of BlockSystems in one persistent launch."""
+    if not systems:
+        return []
+    rt = systems[0].rt
+    arr = (N.LinSys * len(systems))()
+    for i, s in enumerate(systems):
+        mi = max_iter if max_iter is not None else max(
+            1000, 20 * int(np.sqrt(s.n_rows * s.bs)) + 2000)
+        arr[i] = s.linsys(mode, rtol, mi)
+    stats = (N.SolveStats * len(systems))()
+    N.check(rt.lib.cfem_pcg_solve(rt.ctx, arr, len(systems), stats,
+                                  rt.stream()))
+    return [SolveResult(s) for s in stats]
+
+
+def raise_for(result, what="solve"):
+    if result.status == N.CFEM_OK:
+        return
+    if result.status == N.CFEM_ERR_BREAKDOWN:
+        raise RuntimeError(
+            f"{what} failed: {N.STATUS_NAMES[result.status]} "
+            f"(singular or indefinite system; check the boundary conditions)")
+    raise RuntimeError(f"{what} failed: {N.STATUS_NAMES.get(result.status)} "
+                       f"after {result.iterations} iterations, relative "
+                       f"residual {result.relres:.3e}")
+
+
+def fixed_mask(rt, n, idx, vals, x=None):
+    """Device uint8 mask and an x vector holding the Dirichlet values."""
+    torch = _torch()
+    dev = rt.device
+    mask = np.zeros(n, dtype=np.uint8)
+    mask[idx] = 1
+    d_mask = torch.from_numpy(mask).to(dev)
+    if x is None:
+        xh = np.zeros(n)
+        xh[idx] = vals
+        d_x = torch.from_numpy(xh).to(dev)
+    else:
+        d_x = x
+        if len(idx):
+            d_x[torch.from_numpy(np.asarray(idx, np.int64)).to(dev)] = \
+                torch.from_numpy(np.asarray(vals, float)).to(dev)
+    return d_mask, d_x
+
+
+def csr_to_device(rt, A):
+    """Canonical scipy CSR -> device (indptr, indices, data) tensors."""
+    torch = _torch()
+    A = sp.csr_matrix(A, dtype=float)
+    A.sum_duplicates()
+    A.sort_indices()
+    dev = rt.device
+    return (torch.from_numpy(A.indptr.astype(np.int32)).to(dev),
+            torch.from_numpy(A.indices.astype(np.int32)).to(dev),
+            torch.from_numpy(A.data.astype(np.float64)).to(dev), A)

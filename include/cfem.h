@@ -1,0 +1,238 @@
+/*
+ * cfem.h - C ABI of libcfem, the B200 (sm_100a) implementation of
+ * CloudFEM's tetrahedral assembly -> CSR -> sparse-solve hot path.
+ *
+ * The reference (zhangkalin627-svg/CloudFEM) is pure Python: every entry
+ * point below replaces the per-element Python loop plus SciPy call that
+ * the cited reference function runs. All pointers named d_* are device
+ * pointers on the context's device; every other pointer is host memory.
+ * Calls are asynchronous on the given stream (NULL = legacy default
+ * stream) unless the comment says they synchronise.
+ *
+ * Index conventions follow the reference: node ids are 0-based, element
+ * connectivity is row-major (n_elems, npe) with npe = 4 (Tet4,
+ * cloudfem/mesh/tet_mesh.py:11) or 10 (Tet10, cloudfem/mesh/tet10_mesh.py:36,
+ * local slots 4..9 on EDGES (0,1),(1,2),(2,0),(0,3),(1,3),(2,3)); vector
+ * problems interleave DOFs as 3*node + component
+ * (cloudfem/physics/elastic3d.py:80-85).
+ *
+ * Errors: every function returns a CFEM_* status; cfem_last_error()
+ * returns the calling thread's message for the last failure.
+ */
+#ifndef CFEM_H
+#define CFEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CFEM_API __attribute__((visibility("default")))
+#else
+#define CFEM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    CFEM_OK = 0,
+    CFEM_ERR_INVALID = 1,       /* bad argument (the reference's ValueError) */
+    CFEM_ERR_CUDA = 2,          /* CUDA runtime failure                      */
+    CFEM_ERR_NOMEM = 3,         /* device allocation failed                  */
+    CFEM_ERR_NOT_CONVERGED = 4, /* iteration cap or stagnation               */
+    CFEM_ERR_BREAKDOWN = 5,     /* p'Ap <= 0, singular block, non-finite     */
+    CFEM_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up        */
+    CFEM_ERR_UNSUPPORTED = 7    /* device is not sm_100 / feature missing    */
+};
+
+/* Element operators of cfem_assemble (values are block bs x bs per node pair). */
+enum {
+    CFEM_OP_P1_STIFF = 1,   /* tet_poisson.py:35-69   k V G G^T, load f V/4     */
+    CFEM_OP_P1_MASS = 2,    /* tet_heat.py:72-94      rho V/20 (1+d_ij)         */
+    CFEM_OP_T10_STIFF = 3,  /* tet10.py:138-165       Keast-5 k G G^T, f N      */
+    CFEM_OP_T10_MASS = 4,   /* tet10.py:229-249       rho V MASS_REF            */
+    CFEM_OP_P1_ELAST = 5,   /* elastic3d.py:105-169   V B^T D B, body, thermal  */
+    CFEM_OP_T10_ELAST = 6   /* elastic_tet10.py:135-192 Keast-5 B^T D B, ...    */
+};
+
+/* How a coefficient array is sampled. */
+enum {
+    CFEM_COEF_CONST = 0,    /* one scalar (field `constant`)                */
+    CFEM_COEF_ELEM = 1,     /* (n_elems,) at element centroids             */
+    CFEM_COEF_QP = 2,       /* (n_elems, 5) at the Keast-5 points          */
+    CFEM_COEF_NODAL = 3     /* (n_nodes,) nodal field, interpolated         */
+};
+
+typedef struct cfem_coef {
+    const double *d_values; /* NULL for CFEM_COEF_CONST                   */
+    double constant;
+    int32_t mode;
+    int32_t pad_;
+} cfem_coef;
+
+/* Solver precision modes. */
+enum {
+    CFEM_SOLVE_FP64 = 0,    /* plain FP64 Jacobi-PCG                        */
+    CFEM_SOLVE_MIXED = 1    /* FP32 PCG + FP64 residual/update/final dot   */
+};
+enum {
+    CFEM_PRECOND_JACOBI = 0, /* point Jacobi on the diagonal               */
+    CFEM_PRECOND_BLOCK = 1   /* bs x bs nodal block Jacobi                 */
+};
+
+/* One sparse SPD system for cfem_pcg_solve. The matrix is block CSR with
+ * bs x bs row-major blocks (bs = 1 is plain CSR). Dirichlet DOFs are given
+ * by `d_fixed` (1 = fixed) and hold their value in `d_x` on entry; the
+ * solve is then the reference's elimination (tet_poisson.py:72-110,
+ * elastic3d.py:192-233): A_ff x_f = b_f - A_fD x_D. */
+typedef struct cfem_linsys {
+    int64_t n_rows;          /* block rows                                  */
+    int32_t bs;              /* 1 or 3                                      */
+    int32_t precond;         /* CFEM_PRECOND_*                              */
+    const int32_t *d_row_ptr;
+    const int32_t *d_col;
+    const double *d_vals64;  /* FP64 values (required)                      */
+    const float *d_vals32;   /* FP32 copy (CFEM_SOLVE_MIXED), else NULL     */
+    const double *d_b;       /* right-hand side, n_rows*bs                  */
+    double *d_x;             /* in: guess + Dirichlet values; out: solution */
+    const uint8_t *d_fixed;  /* n_rows*bs mask, or NULL                     */
+    double rtol;             /* ||b - A x||_free <= rtol * ||b_lift||_free  */
+    int32_t max_iter;
+    int32_t mode;            /* CFEM_SOLVE_*                                */
+} cfem_linsys;
+
+typedef struct cfem_solve_stats {
+    int32_t status;          /* CFEM_OK / NOT_CONVERGED / BREAKDOWN        */
+    int32_t iterations;
+    int32_t residual_updates;/* FP64 true-residual replacements            */
+    int32_t pad_;
+    double relres;           /* final ||r||/||b_lift|| (FP64, true residual)*/
+    double bnorm;
+    double kernel_ms;        /* device time of the persistent launch (the
+                                same value in every record of a batch)     */
+} cfem_solve_stats;
+
+typedef struct cfem_ctx cfem_ctx;
+typedef struct cfem_pattern cfem_pattern;
+
+/* ---- library / context ------------------------------------------------- */
+CFEM_API const char *cfem_last_error(void);
+CFEM_API int cfem_version(void);
+/* Creates a context on `device` (must be compute capability 10.x). */
+CFEM_API int cfem_ctx_create(int device, cfem_ctx **out);
+CFEM_API int cfem_ctx_destroy(cfem_ctx *ctx);
+/* Number of kernels this library launched through `ctx` so far. */
+CFEM_API int64_t cfem_ctx_launch_count(const cfem_ctx *ctx);
+
+/* ---- sparsity pattern (replaces sp.coo_matrix(...).tocsr() structure) ---
+ * Builds the node-level CSR of all (el[i], el[j]) pairs by a stable radix
+ * sort of (row, col) keys followed by a unique pass, so indices are sorted
+ * and canonical like SciPy's (e.g. tet_poisson.py:68, tet10.py:162), plus
+ * the per-entry contribution lists (sorted by element id) used by the
+ * deterministic segmented reduction in cfem_assemble. Synchronises. */
+CFEM_API int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
+                        int64_t n_elems, int32_t npe, int64_t n_nodes,
+                        void *stream, cfem_pattern **out);
+CFEM_API int cfem_pattern_destroy(cfem_pattern *p);
+CFEM_API int cfem_pattern_info(const cfem_pattern *p, int64_t *n_nodes,
+                      int64_t *nnz);
+/* Device pointers of the node-level CSR (owned by the pattern). */
+CFEM_API int cfem_pattern_node_csr(const cfem_pattern *p, const int32_t **d_row_ptr,
+                          const int32_t **d_col);
+/* Expands the node pattern to the scalar DOF CSR of a bs-DOF problem:
+ * d_indptr (n_nodes*bs+1), d_indices (nnz*bs*bs). */
+CFEM_API int cfem_pattern_expand(const cfem_pattern *p, int32_t bs, int32_t *d_indptr,
+                        int32_t *d_indices, void *stream);
+/* Block values (nnz*bs*bs, block-major) -> scalar CSR value order. */
+CFEM_API int cfem_block_to_csr(const cfem_pattern *p, int32_t bs,
+                      const double *d_bvals, double *d_vals, void *stream);
+
+/* ---- element assembly ---------------------------------------------------
+ * Computes every element matrix (one thread per P1 element, one warp per
+ * Tet10 element with shape gradients staged in shared memory) and reduces
+ * them into d_vals in element order per CSR entry (deterministic, no
+ * atomics). d_vals has nnz*bs*bs entries (bs = 3 for the *_ELAST ops).
+ * `coef` is k / rho_cp; `load` the scalar source f (STIFF ops). Loads go
+ * into d_rhs (n_nodes*bs; NULL to skip). If `accumulate` is 1 the results
+ * are added to d_vals / d_rhs, else they overwrite them. */
+CFEM_API int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
+                  const double *d_nodes, const int32_t *d_elems,
+                  const cfem_coef *coef, const cfem_coef *load,
+                  double *d_vals, double *d_rhs, int32_t accumulate,
+                  void *stream);
+/* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
+ * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),
+ * thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or QP). */
+CFEM_API int cfem_assemble_elastic(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
+                          const double *d_nodes, const int32_t *d_elems,
+                          double E, double nu, const cfem_coef *body3,
+                          const cfem_coef *temp, double alpha, double T_ref,
+                          double *d_vals, double *d_rhs, int32_t accumulate,
+                          void *stream);
+
+/* ---- boundary faces -----------------------------------------------------
+ * Exterior-face candidates of tet_heat.py:97-120 / tet10.py:329-352: the
+ * local faces (element*4 + face, ascending) whose three corners are all in
+ * the node mask d_in_set (n_nodes bytes). Faces are listed with the local
+ * corner order (0,1,2),(0,1,3),(0,2,3),(1,2,3) when faces10 == 0 and the
+ * Tet10 table ((0,1,2),(0,3,1),(0,2,3),(1,3,2)) when faces10 == 1. Writes
+ * at most n_elems*4 ids to d_out and the count to *n_out. Synchronises. */
+CFEM_API int cfem_face_candidates(cfem_ctx *ctx, const int32_t *d_elems,
+                         int64_t n_elems, int32_t npe, int32_t faces10,
+                         const uint8_t *d_in_set, int64_t n_nodes,
+                         int64_t *d_out, int64_t *n_out, void *stream);
+
+/* ---- sparse helpers -----------------------------------------------------
+ * d_vals_out = a*d_x + b*d_y over n values (sums such as C + theta h K,
+ * tet_heat.py:239-240). */
+CFEM_API int cfem_axpby(cfem_ctx *ctx, int64_t n, double a, const double *d_x,
+               double b, const double *d_y, double *d_out, void *stream);
+/* Adds a canonical scalar CSR (d_aptr, d_aidx, d_aval; n_rows rows) whose
+ * pattern is a subset of the node pattern into d_vals (bs = 1), as
+ * K + K_add in tet_heat.py:227-230. Sets CFEM_ERR_INVALID if an entry of
+ * the addend is outside the pattern. */
+CFEM_API int cfem_csr_add_subset(cfem_ctx *ctx, const cfem_pattern *p,
+                        const int32_t *d_aptr, const int32_t *d_aidx,
+                        const double *d_aval, int64_t n_rows,
+                        double *d_vals, void *stream);
+/* y = alpha*A x + beta*y for block CSR (bs = 1 or 3), FP64. */
+CFEM_API int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
+              const int32_t *d_row_ptr, const int32_t *d_col,
+              const double *d_vals, double alpha, const double *d_x,
+              double beta, double *d_y, void *stream);
+/* FP32 copy of n values (the mixed solver's matrix). */
+CFEM_API int cfem_to_fp32(cfem_ctx *ctx, int64_t n, const double *d_in, float *d_out,
+                 void *stream);
+
+/* Dirichlet elimination of tet_poisson.py:72-110 on a scalar CSR:
+ * fixed rows become identity rows, fixed columns are removed from free
+ * rows (the reference stores them as explicit zeros), and
+ * rhs_out = rhs - A[:, fixed] v with rhs_out[fixed] = v. Output CSR
+ * buffers need n+1 and nnz_in + n_fixed entries; *nnz_out receives the
+ * entry count. Synchronises. */
+CFEM_API int cfem_dirichlet_csr(cfem_ctx *ctx, int64_t n, const int32_t *d_indptr,
+                       const int32_t *d_indices, const double *d_vals,
+                       const double *d_rhs, const uint8_t *d_fixed,
+                       const double *d_fixed_val, int32_t *d_out_indptr,
+                       int32_t *d_out_indices, double *d_out_vals,
+                       double *d_rhs_out, int64_t *nnz_out, void *stream);
+
+/* ---- solver -------------------------------------------------------------
+ * Jacobi-preconditioned CG on a batch of independent systems in ONE
+ * persistent cooperative launch (two grid barriers per iteration, per-
+ * system scalars reduced in a fixed order, so each result is bitwise the
+ * same alone and in any batch). CFEM_SOLVE_MIXED runs the CG in FP32 and
+ * keeps FP64 for the true residual r = b - A x, the solution update and
+ * the convergence test (reliable updates). Replaces spla.spsolve /
+ * spla.factorized (tet_poisson.py:121, tet10.py:177, elastic3d.py:230).
+ * Writes one stats record per system. Synchronises. Returns CFEM_OK when
+ * the launch ran; per-system outcomes are in stats[i].status. */
+CFEM_API int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
+                   int32_t n_systems, cfem_solve_stats *stats, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFEM_H */

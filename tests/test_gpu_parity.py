@@ -1,0 +1,183 @@
+"""CUDA path vs the reference's golden vectors and the oracle.
+
+Integer structure (indptr / indices, face lists, meshes) must match bit
+for bit; matrix and load values within 1e-12 of the largest entry; FP64
+solutions within 1e-10 relative (the reference's SuperLU answer is itself
+only pinned to round-off times the condition number).
+"""
+
+import numpy as np
+import pytest
+
+import cases as C
+from conftest import assert_close, assert_csr_equal, golden_csr
+
+pytestmark = pytest.mark.gpu
+
+E, NU = 210e9, 0.3
+SOL_RTOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def cf():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    import cloudfem_b200.fem.tet10 as t10
+    import cloudfem_b200.fem.tet_heat as th
+    import cloudfem_b200.fem.tet_poisson as tp
+    import cloudfem_b200.mesh as mesh
+    import cloudfem_b200.physics.elastic3d as e3
+    import cloudfem_b200.physics.elastic_tet10 as e10
+
+    class NS:
+        pass
+    ns = NS()
+    ns.tp, ns.th, ns.t10, ns.e3, ns.e10, ns.mesh = tp, th, t10, e3, e10, mesh
+    return ns
+
+
+def _box(spec, fn):
+    nx, ny, nz, xl, yl, zl = spec
+    return fn(nx, ny, nz, xlim=xl, ylim=yl, zlim=zl)
+
+
+def test_p1_assemble(cf, golden):
+    m = _box(C.P1_BOX, cf.mesh.box_mesh)
+    A, b = cf.tp.assemble(m, k=C.k_fn, f=C.f_fn)
+    assert_csr_equal(A, golden_csr(golden, "p1_K"))
+    assert_close(b, golden["p1_F"], 1e-12, "p1 rhs")
+    A, b = cf.tp.assemble(m, k=2.5, f=1.0)
+    assert_csr_equal(A, golden_csr(golden, "p1_Kconst"))
+    assert_close(b, golden["p1_Fconst"], 1e-12, "p1 const rhs")
+
+
+def test_p1_dirichlet_and_solve(cf, golden):
+    m = _box(C.P1_BOX, cf.mesh.box_mesh)
+    A, b = cf.tp.assemble(m, k=C.k_fn, f=C.f_fn)
+    bc = {"xmin": 0.0, "zmax": C.bc_fn}
+    Abc, bbc = cf.tp.apply_dirichlet(A, b, m, bc)
+    assert_csr_equal(Abc, golden_csr(golden, "p1_Kbc"), eliminate=True)
+    assert_close(bbc, golden["p1_Fbc"], 1e-12, "p1 lifted rhs")
+    u = cf.tp.solve_tet_poisson(m, k=C.k_fn, f=C.f_fn, bc=bc)
+    assert_close(u, golden["p1_u"], SOL_RTOL, "p1 solution")
+    mc = cf.mesh.box_mesh(C.P1_CUBE, C.P1_CUBE, C.P1_CUBE)
+    u = cf.tp.solve_tet_poisson(mc, f=C.f_sss, bc={s: 0.0 for s in C.FACES})
+    assert_close(u, golden["p1cube_u"], SOL_RTOL, "p1 cube solution")
+
+
+def test_p1_heat_terms_and_faces(cf, golden):
+    m = _box(C.P1_BOX, cf.mesh.box_mesh)
+    assert_csr_equal(cf.th.assemble_mass_tet(m, rho_cp=C.rho_fn),
+                     golden_csr(golden, "p1_C"))
+    K, F = cf.th.assemble_boundary_terms(
+        m, neumann={"xmax": C.q_fn, "ymin": 2.0},
+        robin={"zmin": (C.h_fn, C.tinf_fn), "xmin": (4.0, 10.0)})
+    assert_csr_equal(K, golden_csr(golden, "p1_Krobin"))
+    assert_close(F, golden["p1_Frobin"], 1e-12, "robin load")
+    np.testing.assert_array_equal(cf.th._boundary_faces(m, "zmin"),
+                                  golden["p1_faces_zmin"])
+    np.testing.assert_array_equal(cf.e3.boundary_faces(m, "xmax"),
+                                  golden["p1_faces3_xmax"])
+
+
+def test_p1_transient(cf, golden):
+    m = _box(C.P1_BOX, cf.mesh.box_mesh)
+    times, hist = cf.th.transient_heat_tet(
+        m, k=C.k_fn, rho_cp=C.rho_fn, f=C.f_fn, bc={"xmin": 0.0},
+        robin={"xmax": (C.h_fn, C.tinf_fn)}, neumann={"ymax": 1.5},
+        t_end=0.3, dt=0.1, T0=5.0, method="cn")
+    np.testing.assert_array_equal(times, golden["p1_tr_times"])
+    assert_close(hist, golden["p1_tr_hist"], SOL_RTOL, "p1 transient")
+    _, hist = cf.th.transient_heat_tet(
+        m, robin={s: (25.0, 20.0) for s in C.FACES}, t_end=0.2, dt=0.1,
+        T0=C.t_nodal(m.n_nodes), method="be")
+    assert_close(hist, golden["p1_tr2_hist"], SOL_RTOL, "p1 robin transient")
+
+
+def test_tet10_scalar(cf, golden):
+    m = _box(C.TET10_BOX, cf.mesh.box_mesh_tet10)
+    A, b = cf.t10.assemble_tet10(m, k=C.k_fn, f=C.f_fn)
+    assert_csr_equal(A, golden_csr(golden, "t10_K"))
+    assert_close(b, golden["t10_F"], 1e-12, "t10 rhs")
+    assert_csr_equal(cf.t10.assemble_mass_tet10(m, rho_cp=C.rho_fn),
+                     golden_csr(golden, "t10_C"))
+    K, F = cf.t10.assemble_boundary_terms_tet10(
+        m, neumann={"xmax": C.q_fn, "zmin": 2.0},
+        robin={"ymax": (C.h_fn, C.tinf_fn)})
+    assert_csr_equal(K, golden_csr(golden, "t10_Krobin"))
+    assert_close(F, golden["t10_Frobin"], 1e-12, "t10 robin load")
+    np.testing.assert_array_equal(cf.t10._boundary_faces10(m, "ymax"),
+                                  golden["t10_faces_ymax"])
+    np.testing.assert_array_equal(cf.e10.boundary_faces10(m, "xmin"),
+                                  golden["t10_faces10e_xmin"])
+
+
+def test_tet10_solve_and_transient(cf, golden):
+    m = _box(C.TET10_BOX, cf.mesh.box_mesh_tet10)
+    A, b = cf.t10.assemble_tet10(m, k=C.k_fn, f=C.f_fn)
+    bc10 = {"xmin": C.bc_fn, "zmax": 0.5}
+    Abc, bbc = cf.tp.apply_dirichlet(A, b, m, bc10)
+    assert_csr_equal(Abc, golden_csr(golden, "t10_Kbc"), eliminate=True)
+    assert_close(bbc, golden["t10_Fbc"], 1e-12, "t10 lifted rhs")
+    u = cf.t10.solve_tet10_poisson(m, k=C.k_fn, f=C.f_fn, bc=bc10)
+    assert_close(u, golden["t10_u"], SOL_RTOL, "t10 solution")
+    times, hist = cf.t10.transient_heat_tet10(
+        m, k=C.k_fn, rho_cp=C.rho_fn, f=1.0, bc={"zmin": 1.0},
+        neumann={"xmax": lambda x, y, z, t: 2.0 * t + x},
+        robin={"ymin": (3.0, 0.5)}, t_end=0.2, dt=0.05, T0=0.0, method="cn")
+    np.testing.assert_array_equal(times, golden["t10_tr_times"])
+    assert_close(hist, golden["t10_tr_hist"], SOL_RTOL, "t10 transient")
+
+
+def test_p1_elasticity(cf, golden):
+    m = _box(C.P1_BOX, cf.mesh.box_mesh)
+    A, b = cf.e3.assemble_elasticity_3d(
+        m, E, NU, body=(C.bx_fn, None, -7.8e4),
+        traction={"xmax": (0.0, 1e5, C.q_fn)}, T=C.t_nodal(m.n_nodes),
+        alpha=1.2e-5, T_ref=20.0)
+    assert_csr_equal(A, golden_csr(golden, "e3_K"))
+    assert_close(b, golden["e3_F"], 1e-12, "e3 rhs")
+    bcv = {"xmin": (0.0, 0.0, 0.0), "zmin": (None, None, 0.0),
+           "ymax": (None, 1e-4, None)}
+    u = cf.e3.apply_dirichlet_vec3(A, b, m, bcv)
+    assert_close(u, golden["e3_u"], SOL_RTOL, "e3 reduced solve")
+    sol = cf.e3.solve_elasticity_3d(m, E, NU, bc={"xmin": (0.0, 0.0, 0.0)},
+                                    traction={"xmax": (0.0, 0.0, -1e6)})
+    assert_close(np.stack(sol), golden["e3_sol"], SOL_RTOL, "e3 solution")
+    sig, eps = cf.e3.element_stress_strain_3d(
+        m, tuple(golden["e3_sol"]), E, NU, T=C.t_fn, alpha=1e-5, T_ref=20.0)
+    assert_close(sig, golden["e3_sig"], 1e-12, "e3 stress")
+    assert_close(eps, golden["e3_eps"], 1e-12, "e3 strain")
+
+
+def test_tet10_elasticity(cf, golden):
+    m = _box(C.TET10_BEAM, cf.mesh.box_mesh_tet10)
+    A, b = cf.e10.assemble_elasticity_tet10(
+        m, E, NU, body=(None, C.bx_fn, -7.8e4),
+        traction={"xmax": (0.0, 0.0, -1e6), "ymin": (C.q_fn, None, 0.0)},
+        T=C.t_nodal(m.n_nodes), alpha=1.2e-5, T_ref=20.0)
+    assert_csr_equal(A, golden_csr(golden, "e10_K"))
+    assert_close(b, golden["e10_F"], 1e-12, "e10 rhs")
+    _, b2 = cf.e10.assemble_elasticity_tet10(m, E, NU, T=C.t_fn, alpha=1e-5)
+    assert_close(b2, golden["e10_Fthermal_fn"], 1e-12, "e10 thermal rhs")
+    sol = cf.e10.solve_elasticity_tet10(m, E, NU, bc={"xmin": (0.0, 0.0, 0.0)},
+                                        traction={"xmax": (0.0, 0.0, -1e6)})
+    assert_close(np.stack(sol), golden["e10_sol"], 1e-9, "e10 solution")
+    sig, eps = cf.e10.element_stress_tet10(
+        m, tuple(golden["e10_sol"]), E, NU, T=C.t_nodal(m.n_nodes),
+        alpha=1e-5, T_ref=20.0)
+    assert_close(sig, golden["e10_sig"], 1e-11, "e10 stress")
+    assert_close(eps, golden["e10_eps"], 1e-11, "e10 strain")
+
+
+def test_mixed_precision_matches_fp64(cf):
+    m = cf.mesh.box_mesh_tet10(16, 2, 2, xlim=(0, 0.8), ylim=(0, 0.1),
+                               zlim=(0, 0.1))
+    kw = dict(bc={"xmin": (0.0, 0.0, 0.0)},
+              traction={"xmax": (0.0, 0.0, -1e6)})
+    u64 = np.stack(cf.e10.solve_elasticity_tet10(m, E, NU, **kw))
+    u32 = np.stack(cf.e10.solve_elasticity_tet10(m, E, NU, precision="mixed",
+                                                 rtol=1e-10, **kw))
+    err = np.linalg.norm(u32 - u64) / np.linalg.norm(u64)
+    assert err <= 1e-8, err
