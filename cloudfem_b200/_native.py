@@ -55,7 +55,8 @@ class LinSys(ctypes.Structure):
                 ("d_row_ptr", _vp), ("d_col", _vp), ("d_vals64", _vp),
                 ("d_vals32", _vp), ("d_b", _vp), ("d_x", _vp),
                 ("d_fixed", _vp), ("rtol", _f64), ("max_iter", _i32),
-                ("mode", _i32)]
+                ("mode", _i32), ("reliable_delta", _f64), ("max_stall", _i32),
+                ("history_cap", _i32), ("d_history", _vp)]
 
 
 class SolveStats(ctypes.Structure):
@@ -97,6 +98,8 @@ SIGNATURES = [
     ("cfem_dirichlet_csr", ctypes.c_int,
      [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
       ctypes.POINTER(_i64), _vp]),
+    ("cfem_mixed_matrix", ctypes.c_int,
+     [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     ("cfem_pcg_solve", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), _i32, ctypes.POINTER(SolveStats), _vp]),
 ]

@@ -1,27 +1,29 @@
 // Persistent batched Jacobi-PCG (replaces spla.spsolve / spla.factorized).
 //
-// All systems of a batch are solved by ONE cooperative launch. Rows of each
-// system are cut into fixed chunks (aligned at the system's row 0) that the
-// warps of the grid process; every step the grid runs one phase of every
-// unfinished system and meets at a bounded grid barrier:
+// All systems of a batch are solved by ONE cooperative launch (after one
+// ordinary INIT launch). Rows of each system are cut into small chunks
+// (8 block rows for 3x3 blocks, 16 rows for scalars, aligned at the
+// system's row 0); the warps of the grid take chunks round-robin. Every
+// step the grid runs one phase of every unfinished system and meets at a
+// bounded two-level grid barrier:
 //
 //   INIT  r = b - A x (FP64 matrix), ||b_lift||, Jacobi inverse, z = M r
-//   A     p = z + beta p_old (computed on the fly for neighbours, so the
+//   A     p = z + beta p_old (evaluated on the fly for neighbours, so the
 //         update needs no extra barrier), q = A p, p.q
 //   B     x += alpha p (FP64), r -= alpha q, z = M r, r.z, r.r
 //   R     true residual r = b - A x in FP64 replaces the recursive one
-//         (reliable update: when the mixed-precision residual fell by 10x,
-//         and always before convergence is declared)
+//         (reliable update: when the mixed-precision residual fell by
+//         `reliable_delta`, and always before convergence is declared)
 //
-// Each chunk reduces its part of the dot products warp-locally; the last
-// chunk of a system to finish (atomic ticket) sums all chunk partials of
-// that system in a fixed order and advances its state. Results therefore
-// depend only on the system itself: bitwise identical alone or in a batch.
+// Dot products: each chunk reduces warp-locally; chunk partials are summed
+// per tile of 32 chunks by the tile's last finisher, tile partials by the
+// system's last tile (atomic tickets). The summation tree depends only on
+// the system, so each result is bitwise the same alone or in any batch.
 //
 // CFEM_SOLVE_FP64 keeps all vectors and the matrix in FP64 (the plain
-// path). CFEM_SOLVE_MIXED runs A, B in FP32 (FP32 matrix copy, FP32 r, z, p,
-// q) and keeps FP64 only for the solution x, the true residual and the
-// final convergence norm.
+// path). CFEM_SOLVE_MIXED runs A and B in FP32 (FP32 matrix copy and FP32
+// r, z, p, q) and keeps FP64 only for x, the true residual and the final
+// convergence norm.
 #include "cfem_common.cuh"
 
 #include <math.h>
@@ -31,17 +33,26 @@ namespace cfem {
 
 enum { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_R = 3, PH_ZERO = 4, PH_DONE = 5 };
 
-constexpr int SOLVE_THREADS = 256;
-constexpr int LANES = 8;                 // lanes per matrix row
-constexpr int CHUNK_ROWS = 64;           // block rows per chunk
-constexpr double RELIABLE_DELTA2 = 1e-2; // replace r when ||r|| < 0.1 ||r_ref||
+constexpr int SOLVE_THREADS = 512;
+constexpr int LANES = 8;                   // lanes per block row
+constexpr int RPP = 32 / LANES;            // block rows per warp pass
+constexpr int TILE = 32;                   // chunks per reduction tile
+constexpr double RELIABLE_DELTA = 0.1;
 constexpr int MAX_STALL = 8;
+// The FP64 residual r_i = b_i - sum_j a_ij x_j carries a rounding error of
+// a few eps * sum_j |a_ij x_j|; a residual at that level cannot be reduced
+// or even measured further, so it counts as converged.
+constexpr double FLOOR_C = 16.0 * 2.220446049250313e-16;
 constexpr unsigned long long BARRIER_TIMEOUT_NS = 4000000000ull;  // 4 s
+constexpr int BAR_GROUP = 16;              // blocks per first-level counter
+constexpr int BAR_MAX_GROUPS = 64;
+
+__host__ __device__ inline int chunk_rows(int bs) { return bs == 3 ? 8 : 16; }
 
 struct SysDev {
     int64_t n;
-    int32_t bs, precond, mode, nchunks;
-    int32_t chunk0, max_iter;
+    int32_t bs, precond, mode, max_iter;
+    int32_t nchunks, ntiles, chunk0, crows;
     const int32_t *rp;
     const int32_t *ci;
     const double *v64;
@@ -50,8 +61,12 @@ struct SysDev {
     double *x;
     const uint8_t *fixed;
     void *r, *z, *p0, *p1, *q, *dinv;
-    double *partial;
-    double rtol2;
+    double *partial;      // nchunks * 4
+    double *tpartial;     // ntiles * 4
+    unsigned int *tcnt;   // ntiles tickets
+    double rtol2, delta2;
+    int32_t max_stall, hist_cap;
+    double *hist;
 };
 
 struct SysState {
@@ -61,11 +76,15 @@ struct SysState {
     int32_t pad;
 };
 
+// Counters live on separate 128-byte lines.
 struct GridBar {
-    unsigned int count;
     unsigned int gen;
     int err;
     int active;
+    unsigned int pad0[29];
+    unsigned int top;
+    unsigned int pad1[31];
+    unsigned int grp[BAR_MAX_GROUPS][32];
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -74,21 +93,31 @@ __device__ __forceinline__ unsigned long long globaltimer() {
     return t;
 }
 
-// Bounded software grid barrier; all blocks are co-resident (cooperative
-// launch). Returns false when a block gave up waiting (error flag set).
-__device__ bool grid_sync(GridBar *bar, unsigned nblocks) {
+// Bounded two-level software grid barrier over co-resident blocks
+// (cooperative launch). Returns false when a block gave up waiting.
+__device__ bool grid_sync(GridBar *bar) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *vgen = &bar->gen;
         volatile int *verr = &bar->err;
+        const unsigned nb = gridDim.x;
+        const unsigned grp = blockIdx.x / BAR_GROUP;
+        const unsigned ngrp = (nb + BAR_GROUP - 1) / BAR_GROUP;
+        const unsigned gsize = min((unsigned)BAR_GROUP, nb - grp * BAR_GROUP);
         unsigned g = *vgen;
         __threadfence();
-        unsigned arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
+        bool released = false;
+        if (atomicAdd(&bar->grp[grp][0], 1u) == gsize - 1) {
+            atomicExch(&bar->grp[grp][0], 0u);
             __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
+            if (atomicAdd(&bar->top, 1u) == ngrp - 1) {
+                atomicExch(&bar->top, 0u);
+                __threadfence();
+                atomicAdd(&bar->gen, 1u);
+                released = true;
+            }
+        }
+        if (!released) {
             unsigned long long t0 = globaltimer();
             unsigned spins = 0;
             while (*vgen == g) {
@@ -97,7 +126,7 @@ __device__ bool grid_sync(GridBar *bar, unsigned nblocks) {
                     atomicExch(&bar->err, 1);
                     break;
                 }
-                __nanosleep(20);
+                __nanosleep(32);
             }
         }
         __threadfence();
@@ -107,7 +136,6 @@ __device__ bool grid_sync(GridBar *bar, unsigned nblocks) {
 }
 
 template <typename T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
-
 __device__ __forceinline__ double vcg(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ int vcgi(const int32_t *p) { return __ldcg(p); }
 
@@ -158,28 +186,42 @@ __device__ __forceinline__ bool block_inverse(const double a[9], const bool fx[3
     return true;
 }
 
-// z = M r for one block row (M = point or block Jacobi inverse).
+// z_c = M r for the dof this lane owns (lane = (row - r0) * BS + c). The
+// three residuals of a block row are exchanged by shuffles, so every lane
+// of the warp must call this.
 template <typename T, int BS>
-__device__ __forceinline__ void apply_prec(const SysDev &S, int64_t row,
-                                           const T r[BS], T z[BS]) {
+__device__ __forceinline__ T apply_prec_lane(const SysDev &S, int64_t row, int c,
+                                             int lane, T rv, bool valid) {
     const T *dinv = (const T *)S.dinv;
     if (BS == 3 && S.precond == CFEM_PRECOND_BLOCK) {
-        const T *D = dinv + row * 9;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            z[c] = ldcg(D + c * 3) * r[0] + ldcg(D + c * 3 + 1) * r[1] +
-                   ldcg(D + c * 3 + 2) * r[2];
-    } else {
-#pragma unroll
-        for (int c = 0; c < BS; ++c) z[c] = ldcg(dinv + row * BS + c) * r[c];
+        const int base = lane - c;
+        T r0 = __shfl_sync(0xffffffffu, rv, base >= 0 ? base : 0);
+        T r1 = __shfl_sync(0xffffffffu, rv, base + 1 < 32 ? base + 1 : 31);
+        T r2 = __shfl_sync(0xffffffffu, rv, base + 2 < 32 ? base + 2 : 31);
+        if (!valid) return (T)0;
+        const T *D = dinv + row * 9 + c * 3;
+        return ldcg(D) * r0 + ldcg(D + 1) * r1 + ldcg(D + 2) * r2;
     }
+    if (!valid) return (T)0;
+    return ldcg(dinv + row * BS + c) * rv;
 }
 
 // ---------------------------------------------------------------- phase A
-template <typename T, int BS>
+// q = A p with p = z + beta p_old. Each lane group of LANES lanes works on
+// two block rows at once and unrolls U column blocks per row, so every lane
+// keeps 2U independent (index -> gather) load chains in flight.
+//
+// DIFF (mixed precision): the FP32 operator is stored in difference form
+// (cfem_mixed_matrix): off-diagonal blocks A_ij and, in the diagonal slot,
+// the FP64 row sum s_i = sum_j A_ij rounded once. Then
+//     (A p)_i = s_i p_i + sum_{j != i} A_ij (p_j - p_i),
+// which applies constant vectors (rigid translations, uniform fields)
+// exactly whatever the rounding of A_ij, so the FP32 operator does not
+// perturb the near-null space that governs the CG convergence.
+template <typename T, int BS, bool DIFF, int U>
 __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
                         int64_t r1, int lane, double part[4]) {
-    constexpr int L = LANES, RPP = 32 / LANES;
+    constexpr int B2 = BS * BS;
     const T beta = (T)vcg(&st->beta);
     const int pbuf = vcgi(&st->pbuf);
     const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
@@ -187,39 +229,78 @@ __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
     const T *z = (const T *)S.z;
     T *q = (T *)S.q;
     const T *v = MatVal<T>::get(S);
-    const int sub = lane & (L - 1);
+    const int32_t *ci = S.ci;
+    const int sub = lane & (LANES - 1), grp = lane / LANES;
     T pq = 0;
-    for (int64_t base = r0; base < r1; base += RPP) {
-        const int64_t row = base + lane / L;
-        const bool valid = row < r1;
-        T acc[BS];
+    for (int64_t base = r0; base < r1; base += 2 * RPP) {
+        int64_t row[2];
+        bool valid[2];
+        int32_t k0[2], k1[2];
+        T pi[2][BS], acc[2][BS];
 #pragma unroll
-        for (int c = 0; c < BS; ++c) acc[c] = 0;
-        if (valid) {
-            const int32_t k1 = __ldg(S.rp + row + 1);
-            for (int32_t k = __ldg(S.rp + row) + sub; k < k1; k += L) {
-                const int64_t j = __ldg(S.ci + k);
-                T pj[BS];
-#pragma unroll
-                for (int d = 0; d < BS; ++d)
-                    pj[d] = ldcg(z + j * BS + d) + beta * ldcg(pin + j * BS + d);
-                const T *vk = v + (int64_t)k * BS * BS;
-#pragma unroll
-                for (int c = 0; c < BS; ++c)
-#pragma unroll
-                    for (int d = 0; d < BS; ++d) acc[c] += __ldg(vk + c * BS + d) * pj[d];
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < BS; ++c) acc[c] = group_sum<L>(acc[c]);
-        if (valid && sub == 0) {
+        for (int h = 0; h < 2; ++h) {
+            row[h] = base + h * RPP + grp;
+            valid[h] = row[h] < r1;
+            const int64_t rr = valid[h] ? row[h] : r0;
+            k0[h] = valid[h] ? __ldg(S.rp + rr) : 0;
+            k1[h] = valid[h] ? __ldg(S.rp + rr + 1) : 0;
 #pragma unroll
             for (int c = 0; c < BS; ++c) {
-                const int64_t i = row * BS + c;
-                const T pn = ldcg(z + i) + beta * ldcg(pin + i);
-                pout[i] = pn;
-                q[i] = acc[c];
-                pq += pn * acc[c];
+                pi[h][c] = ldcg(z + rr * BS + c) + beta * ldcg(pin + rr * BS + c);
+                acc[h][c] = 0;
+            }
+        }
+        const int32_t len = max(k1[0] - k0[0], k1[1] - k0[1]);
+        for (int32_t off = sub; off < len; off += U * LANES) {
+            int64_t j[2][U];
+            T a[2][U][B2];
+            bool on[2][U];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t k = k0[h] + off + u * LANES;
+                    on[h][u] = k < k1[h];
+                    const int32_t kk = on[h][u] ? k : k0[0];
+                    j[h][u] = __ldg(ci + kk);
+#pragma unroll
+                    for (int e = 0; e < B2; ++e) {
+                        const T av = __ldg(v + (int64_t)kk * B2 + e);
+                        a[h][u][e] = on[h][u] ? av : (T)0;
+                    }
+                }
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    T pj[BS];
+#pragma unroll
+                    for (int d = 0; d < BS; ++d) {
+                        pj[d] = ldcg(z + j[h][u] * BS + d) +
+                                beta * ldcg(pin + j[h][u] * BS + d);
+                        if (DIFF) pj[d] = (j[h][u] == row[h]) ? pi[h][d] : pj[d] - pi[h][d];
+                    }
+#pragma unroll
+                    for (int c = 0; c < BS; ++c)
+#pragma unroll
+                        for (int d = 0; d < BS; ++d) acc[h][c] += a[h][u][c * BS + d] * pj[d];
+                }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int c = 0; c < BS; ++c) acc[h][c] = group_sum<LANES>(acc[h][c]);
+        if (sub == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!valid[h]) continue;
+#pragma unroll
+                for (int c = 0; c < BS; ++c) {
+                    const int64_t i = row[h] * BS + c;
+                    pout[i] = pi[h][c];
+                    q[i] = acc[h][c];
+                    pq += pi[h][c] * acc[h][c];
+                }
             }
         }
     }
@@ -237,91 +318,100 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     T *r = (T *)S.r;
     T *z = (T *)S.z;
     const T *q = (const T *)S.q;
-    T rz = 0, rr = 0;
-    for (int64_t row = r0 + lane; row < r1; row += 32) {
-        T rv[BS], zv[BS];
-        bool fx[BS];
-#pragma unroll
-        for (int c = 0; c < BS; ++c) {
-            const int64_t i = row * BS + c;
-            fx[c] = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
+    const int64_t i = r0 * BS + lane;
+    const bool valid = i < r1 * BS;
+    const int64_t row = r0 + lane / BS;
+    const int c = lane - (lane / BS) * BS;
+    bool fx = false;
+    T rv = 0;
+    if (valid) {
+        fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
+        rv = ldcg(r + i);
+        if (!fx) {
             const T pi = ldcg(p + i);
-            rv[c] = ldcg(r + i);
-            if (!fx[c]) {
-                S.x[i] = ldcg(S.x + i) + alpha64 * (double)pi;
-                rv[c] -= alpha * ldcg(q + i);
-            }
+            S.x[i] = ldcg(S.x + i) + alpha64 * (double)pi;
+            rv -= alpha * ldcg(q + i);
         }
-        apply_prec<T, BS>(S, row, rv, zv);
-#pragma unroll
-        for (int c = 0; c < BS; ++c) {
-            const int64_t i = row * BS + c;
-            if (fx[c]) zv[c] = 0;
-            r[i] = rv[c];
-            z[i] = zv[c];
-            rz += rv[c] * zv[c];
-            rr += rv[c] * rv[c];
-        }
+    }
+    T zv = apply_prec_lane<T, BS>(S, row, c, lane, rv, valid);
+    T rz = 0, rr = 0;
+    if (valid) {
+        if (fx) zv = 0;
+        r[i] = rv;
+        z[i] = zv;
+        rz = rv * zv;
+        rr = rv * rv;
     }
     part[0] += (double)rz;
     part[1] += (double)rr;
 }
 
 // ------------------------------------------------------- phase R / INIT
-// True residual in FP64. INIT also forms ||b_lift|| and the Jacobi inverse.
+// True residual in FP64; INIT also forms ||b_lift|| and the Jacobi inverse.
+template <bool INIT, int BS>
+__device__ __forceinline__ void acc_R(const double *__restrict__ v,
+                                      const int32_t *__restrict__ ci, int32_t k,
+                                      int64_t row, const double *x,
+                                      const uint8_t *fixed, double acc[BS],
+                                      double aab[BS], double accf[BS],
+                                      double dg[BS * BS]) {
+    const int64_t j = __ldg(ci + k);
+    const double *vk = v + (int64_t)k * BS * BS;
+    double xj[BS];
+    bool fj[BS];
+#pragma unroll
+    for (int d = 0; d < BS; ++d) {
+        xj[d] = ldcg(x + j * BS + d);
+        fj[d] = INIT && fixed ? (__ldg(fixed + j * BS + d) != 0) : false;
+    }
+#pragma unroll
+    for (int c = 0; c < BS; ++c)
+#pragma unroll
+        for (int d = 0; d < BS; ++d) {
+            const double a = __ldg(vk + c * BS + d);
+            const double ax = a * xj[d];
+            acc[c] += ax;
+            aab[c] += fabs(ax);
+            if (INIT && fj[d]) accf[c] += ax;
+            if (INIT && j == row) dg[c * BS + d] = a;
+        }
+}
+
 template <typename T, int BS, bool INIT>
 __device__ void phase_R(const SysDev &S, int64_t r0, int64_t r1, int lane,
                         double part[4], int *bad) {
-    constexpr int L = LANES, RPP = 32 / LANES;
-    const int sub = lane & (L - 1);
+    const int sub = lane & (LANES - 1), grp = lane / LANES;
     T *r = (T *)S.r;
     T *z = (T *)S.z;
     T *dinv = (T *)S.dinv;
-    double rr = 0.0, bb = 0.0;
+    double rr = 0.0, bb = 0.0, aa = 0.0;
     T rz = 0;
     for (int64_t base = r0; base < r1; base += RPP) {
-        const int64_t row = base + lane / L;
+        const int64_t row = base + grp;
         const bool valid = row < r1;
-        double acc[BS], accf[BS], dg[BS * BS];
+        double acc[BS], accf[BS], aab[BS], dg[BS * BS];
 #pragma unroll
-        for (int c = 0; c < BS; ++c) acc[c] = accf[c] = 0.0;
+        for (int c = 0; c < BS; ++c) acc[c] = accf[c] = aab[c] = 0.0;
 #pragma unroll
         for (int c = 0; c < BS * BS; ++c) dg[c] = 0.0;
         if (valid) {
             const int32_t k1 = __ldg(S.rp + row + 1);
-            for (int32_t k = __ldg(S.rp + row) + sub; k < k1; k += L) {
-                const int64_t j = __ldg(S.ci + k);
-                const double *vk = S.v64 + (int64_t)k * BS * BS;
-                double xj[BS];
-                bool fj[BS];
-#pragma unroll
-                for (int d = 0; d < BS; ++d) {
-                    xj[d] = ldcg(S.x + j * BS + d);
-                    fj[d] = INIT && S.fixed ? (__ldg(S.fixed + j * BS + d) != 0) : false;
-                }
-#pragma unroll
-                for (int c = 0; c < BS; ++c)
-#pragma unroll
-                    for (int d = 0; d < BS; ++d) {
-                        const double a = __ldg(vk + c * BS + d);
-                        acc[c] += a * xj[d];
-                        if (INIT && fj[d]) accf[c] += a * xj[d];
-                        if (INIT && j == row) dg[c * BS + d] = a;
-                    }
-            }
+            for (int32_t k = __ldg(S.rp + row) + sub; k < k1; k += LANES)
+                acc_R<INIT, BS>(S.v64, S.ci, k, row, S.x, S.fixed, acc, aab, accf, dg);
         }
 #pragma unroll
         for (int c = 0; c < BS; ++c) {
-            acc[c] = group_sum<L>(acc[c]);
-            if (INIT) accf[c] = group_sum<L>(accf[c]);
+            acc[c] = group_sum<LANES>(acc[c]);
+            aab[c] = group_sum<LANES>(aab[c]);
+            if (INIT) accf[c] = group_sum<LANES>(accf[c]);
         }
         if (INIT) {
 #pragma unroll
-            for (int c = 0; c < BS * BS; ++c) dg[c] = group_sum<L>(dg[c]);
+            for (int c = 0; c < BS * BS; ++c) dg[c] = group_sum<LANES>(dg[c]);
         }
         if (valid && sub == 0) {
             bool fx[BS];
-            T rv[BS], zv[BS];
+            T rv[BS];
 #pragma unroll
             for (int c = 0; c < BS; ++c) {
                 const int64_t i = row * BS + c;
@@ -333,7 +423,9 @@ __device__ void phase_R(const SysDev &S, int64_t r0, int64_t r1, int lane,
                     bb += bl * bl;
                 }
                 rr += rt * rt;
+                if (!fx[c]) aa += aab[c] * aab[c];
                 rv[c] = (T)rt;
+                r[i] = rv[c];
             }
             if (INIT) {
                 if (BS == 3 && S.precond == CFEM_PRECOND_BLOCK) {
@@ -358,20 +450,27 @@ __device__ void phase_R(const SysDev &S, int64_t r0, int64_t r1, int lane,
                     }
                 }
             }
-            apply_prec<T, BS>(S, row, rv, zv);
+            // z = M r (row-local: this lane wrote or reads this row's dinv)
+            const T *D = (const T *)S.dinv;
 #pragma unroll
             for (int c = 0; c < BS; ++c) {
-                const int64_t i = row * BS + c;
-                if (fx[c]) zv[c] = 0;
-                r[i] = rv[c];
-                z[i] = zv[c];
-                rz += rv[c] * zv[c];
+                T zv;
+                if (BS == 3 && S.precond == CFEM_PRECOND_BLOCK)
+                    zv = ldcg(D + row * 9 + c * 3) * rv[0] +
+                         ldcg(D + row * 9 + c * 3 + 1) * rv[BS > 1 ? 1 : 0] +
+                         ldcg(D + row * 9 + c * 3 + 2) * rv[BS > 2 ? 2 : 0];
+                else
+                    zv = ldcg(D + row * BS + c) * rv[c];
+                if (fx[c]) zv = 0;
+                z[row * BS + c] = zv;
+                rz += rv[c] * zv;
             }
         }
     }
     part[0] += rr;
     part[1] += bb;
     part[2] += (double)rz;
+    part[3] += aa;
 }
 
 template <int BS>
@@ -380,33 +479,9 @@ __device__ void phase_zero(const SysDev &S, int64_t r0, int64_t r1, int lane) {
         if (!(S.fixed && __ldg(S.fixed + i))) S.x[i] = 0.0;
 }
 
-// Last-chunk bookkeeping: fixed-order sum of the system's chunk partials,
-// then the state transition.
-__device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
-                             int lc, int ph, double part[4], int lane,
-                             int bad) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
-    int last = 0;
-    if (lane == 0) {
-#pragma unroll
-        for (int v = 0; v < 4; ++v) S.partial[(int64_t)lc * 4 + v] = part[v];
-        if (bad) atomicExch(&st->status, CFEM_ERR_BREAKDOWN);
-        __threadfence();
-        unsigned old = atomicAdd(&st->cnt, 1u);
-        last = (old == (unsigned)S.nchunks - 1) ? 1 : 0;
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (!last) return;
-    __threadfence();
-    double tot[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int c = lane; c < S.nchunks; c += 32)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) tot[v] += vcg(S.partial + (int64_t)c * 4 + v);
-#pragma unroll
-    for (int v = 0; v < 4; ++v) tot[v] = warp_sum(tot[v]);
-    if (lane != 0) return;
-    st->cnt = 0;
+// State transition of a system once all its chunk sums are in.
+__device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
+                        const double tot[4]) {
     const double rtol2 = S.rtol2;
     int next = PH_DONE;
     const int status_now = *(volatile int32_t *)&st->status;
@@ -414,13 +489,14 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
         next = PH_DONE;   // a bad Jacobi block was found
     } else if (ph == PH_INIT) {
         const double rr = tot[0], bb = tot[1], rz = tot[2];
+        const double floor2 = FLOOR_C * FLOOR_C * tot[3];
         st->bb = bb;
         if (!isfinite(rr) || !isfinite(bb) || !isfinite(rz)) {
             st->status = CFEM_ERR_BREAKDOWN;
         } else if (bb == 0.0) {
             st->relres = 0.0;
             next = PH_ZERO;
-        } else if (rr <= rtol2 * bb) {
+        } else if (rr <= rtol2 * bb || rr <= floor2) {
             st->relres = sqrt(rr / bb);
         } else {
             st->rz = rz;
@@ -446,7 +522,7 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
         if (!isfinite(rz) || !isfinite(rr)) {
             st->status = CFEM_ERR_BREAKDOWN;
         } else if (rr <= rtol2 * bb ||
-                   (S.mode == CFEM_SOLVE_MIXED && rr < RELIABLE_DELTA2 * st->rmax2)) {
+                   (S.mode == CFEM_SOLVE_MIXED && rr < S.delta2 * st->rmax2)) {
             next = PH_R;
         } else if (st->iter >= S.max_iter) {
             st->status = CFEM_ERR_NOT_CONVERGED;
@@ -458,11 +534,16 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
         }
     } else if (ph == PH_R) {
         const double rr = tot[0], rz = tot[2], bb = st->bb;
+        const double floor2 = FLOOR_C * FLOOR_C * tot[3];
+        if (st->nres < S.hist_cap) {
+            S.hist[2 * st->nres] = (double)st->iter;
+            S.hist[2 * st->nres + 1] = sqrt(rr / bb);
+        }
         st->nres += 1;
         st->relres = sqrt(rr / bb);
         if (!isfinite(rr) || !isfinite(rz)) {
             st->status = CFEM_ERR_BREAKDOWN;
-        } else if (rr <= rtol2 * bb) {
+        } else if (rr <= rtol2 * bb || rr <= floor2) {
             // converged on the FP64 true residual
         } else if (st->iter >= S.max_iter) {
             st->status = CFEM_ERR_NOT_CONVERGED;
@@ -473,7 +554,7 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
             } else {
                 st->stall += 1;
             }
-            if (st->stall >= MAX_STALL) {
+            if (st->stall >= S.max_stall) {
                 st->status = CFEM_ERR_NOT_CONVERGED;
             } else {
                 st->beta = rz / st->rz;
@@ -489,62 +570,177 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
     if (next == PH_DONE) atomicSub(&bar->active, 1);
 }
 
-template <typename T, int BS>
+// Chunk partial -> tile partial -> system total, each level summed in a
+// fixed order by its last finisher.
+__device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
+                             int lc, int ph, double part[4], int lane, int bad) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
+    const int tile = lc / TILE;
+    const int tsize = min(TILE, S.nchunks - tile * TILE);
+    int last = 0;
+    if (lane == 0) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) S.partial[(int64_t)lc * 4 + v] = part[v];
+        if (bad) atomicExch(&st->status, CFEM_ERR_BREAKDOWN);
+        __threadfence();
+        last = (atomicAdd(&S.tcnt[tile], 1u) == (unsigned)tsize - 1) ? 1 : 0;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    if (lane < tsize) {
+        const int64_t c = (int64_t)tile * TILE + lane;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) t[v] = vcg(S.partial + c * 4 + v);
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) t[v] = warp_sum(t[v]);
+    int last_sys = 0;
+    if (lane == 0) {
+        S.tcnt[tile] = 0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) S.tpartial[(int64_t)tile * 4 + v] = t[v];
+        __threadfence();
+        last_sys = (atomicAdd(&st->cnt, 1u) == (unsigned)S.ntiles - 1) ? 1 : 0;
+    }
+    last_sys = __shfl_sync(0xffffffffu, last_sys, 0);
+    if (!last_sys) return;
+    __threadfence();
+    double tot[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = lane; c < S.ntiles; c += 32)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) tot[v] += vcg(S.tpartial + (int64_t)c * 4 + v);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) tot[v] = warp_sum(tot[v]);
+    if (lane != 0) return;
+    st->cnt = 0;
+    advance(S, st, bar, ph, tot);
+}
+
+template <typename T, int BS, bool INIT>
 __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
                           int lc, int lane) {
-    const int64_t r0 = (int64_t)lc * CHUNK_ROWS;
-    const int64_t r1 = min(S.n, r0 + CHUNK_ROWS);
+    const int64_t r0 = (int64_t)lc * S.crows;
+    const int64_t r1 = min(S.n, r0 + S.crows);
     double part[4] = {0.0, 0.0, 0.0, 0.0};
     int bad = 0;
-    switch (ph) {
-        case PH_INIT: {
-            int flag = 0;
-            phase_R<T, BS, true>(S, r0, r1, lane, part, &flag);
-            bad = __any_sync(0xffffffffu, flag != 0);
-            break;
+    if (INIT) {
+        int flag = 0;
+        phase_R<T, BS, true>(S, r0, r1, lane, part, &flag);
+        bad = __any_sync(0xffffffffu, flag != 0);
+    } else {
+        switch (ph) {
+            case PH_A:
+                if (sizeof(T) == 4) phase_A<T, BS, true, 2>(S, st, r0, r1, lane, part);
+                else phase_A<T, BS, false, 1>(S, st, r0, r1, lane, part);
+                break;
+            case PH_B: phase_B<T, BS>(S, st, r0, r1, lane, part); break;
+            case PH_R: phase_R<T, BS, false>(S, r0, r1, lane, part, &bad); break;
+            default: phase_zero<BS>(S, r0, r1, lane); break;
         }
-        case PH_A: phase_A<T, BS>(S, st, r0, r1, lane, part); break;
-        case PH_B: phase_B<T, BS>(S, st, r0, r1, lane, part); break;
-        case PH_R: {
-            int flag = 0;
-            phase_R<T, BS, false>(S, r0, r1, lane, part, &flag);
-            break;
-        }
-        default: phase_zero<BS>(S, r0, r1, lane); break;
     }
     finish_chunk(S, st, bar, lc, ph, part, lane, bad);
 }
 
-__global__ void __launch_bounds__(SOLVE_THREADS)
+template <bool INIT>
+__device__ __forceinline__ void dispatch(const SysDev *__restrict__ sys,
+                                         SysState *st, GridBar *bar,
+                                         const int32_t *__restrict__ chunk_sys,
+                                         int c, int lane) {
+    const int s = __ldg(chunk_sys + c);
+    const SysDev &S = sys[s];
+    const int ph = INIT ? PH_INIT : *(volatile int32_t *)&st[s].phase;
+    if (ph == PH_DONE) return;
+    const int lc = c - S.chunk0;
+    if (S.mode == CFEM_SOLVE_MIXED) {
+        if (S.bs == 3) run_chunk<float, 3, INIT>(S, &st[s], bar, ph, lc, lane);
+        else run_chunk<float, 1, INIT>(S, &st[s], bar, ph, lc, lane);
+    } else {
+        if (S.bs == 3) run_chunk<double, 3, INIT>(S, &st[s], bar, ph, lc, lane);
+        else run_chunk<double, 1, INIT>(S, &st[s], bar, ph, lc, lane);
+    }
+}
+
+// INIT: one ordinary launch, one warp per chunk.
+__global__ void __launch_bounds__(256)
+k_pcg_init(const SysDev *__restrict__ sys, SysState *st,
+           const int32_t *__restrict__ chunk_sys, int n_chunks, GridBar *bar) {
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= n_chunks) return;
+    dispatch<true>(sys, st, bar, chunk_sys, c, threadIdx.x & 31);
+}
+
+__global__ void __launch_bounds__(SOLVE_THREADS, 1)
 k_pcg_persistent(const SysDev *__restrict__ sys, SysState *st,
                  const int32_t *__restrict__ chunk_sys, int n_chunks,
                  GridBar *bar, int max_steps) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
+    if (*(volatile int *)&bar->active <= 0) return;
     for (int step = 0; step < max_steps; ++step) {
-        for (int c = gw; c < n_chunks; c += nw) {
-            const int s = __ldg(chunk_sys + c);
-            const SysDev &S = sys[s];
-            const int ph = *(volatile int32_t *)&st[s].phase;
-            if (ph == PH_DONE) continue;
-            const int lc = c - S.chunk0;
-            if (S.mode == CFEM_SOLVE_MIXED) {
-                if (S.bs == 3) run_chunk<float, 3>(S, &st[s], bar, ph, lc, lane);
-                else run_chunk<float, 1>(S, &st[s], bar, ph, lc, lane);
-            } else {
-                if (S.bs == 3) run_chunk<double, 3>(S, &st[s], bar, ph, lc, lane);
-                else run_chunk<double, 1>(S, &st[s], bar, ph, lc, lane);
-            }
-        }
-        if (!grid_sync(bar, gridDim.x)) return;
+        for (int c = gw; c < n_chunks; c += nw)
+            dispatch<false>(sys, st, bar, chunk_sys, c, lane);
+        if (!grid_sync(bar)) return;
         if (*(volatile int *)&bar->active <= 0) return;
+    }
+}
+
+// FP32 difference-form operator: off-diagonal blocks rounded, the diagonal
+// slot holding the rounded FP64 block row sum (see phase_A).
+template <int BS>
+__global__ void k_mixed_matrix(int64_t n, const int32_t *__restrict__ rp,
+                               const int32_t *__restrict__ ci,
+                               const double *__restrict__ v64,
+                               float *__restrict__ v32) {
+    constexpr int B2 = BS * BS;
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double sum[B2];
+#pragma unroll
+    for (int e = 0; e < B2; ++e) sum[e] = 0.0;
+    int32_t kd = -1;
+    for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+        if (ci[k] == r) kd = k;
+#pragma unroll
+        for (int e = 0; e < B2; ++e) {
+            const double a = v64[(int64_t)k * B2 + e];
+            sum[e] += a;
+            v32[(int64_t)k * B2 + e] = (float)a;
+        }
+    }
+    if (kd >= 0) {
+#pragma unroll
+        for (int e = 0; e < B2; ++e) v32[(int64_t)kd * B2 + e] = (float)sum[e];
     }
 }
 
 }  // namespace cfem
 
 using namespace cfem;
+
+extern "C" int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
+                                 const int32_t *d_row_ptr, const int32_t *d_col,
+                                 const double *d_vals64, float *d_vals32,
+                                 void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_row_ptr && d_col && d_vals64 && d_vals32 && n_rows >= 0 &&
+                   (bs == 1 || bs == 3),
+               CFEM_ERR_INVALID, "cfem_mixed_matrix: bad args");
+    if (n_rows == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (bs == 1)
+        CFEM_LAUNCH(k_mixed_matrix<1>, grid_for(n_rows, 128), 128, 0, s, n_rows,
+                    d_row_ptr, d_col, d_vals64, d_vals32);
+    else
+        CFEM_LAUNCH(k_mixed_matrix<3>, grid_for(n_rows, 128), 128, 0, s, n_rows,
+                    d_row_ptr, d_col, d_vals64, d_vals32);
+    return CFEM_OK;
+    CFEM_API_END
+}
 
 extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
                               int32_t n_systems, cfem_solve_stats *stats,
@@ -578,7 +774,9 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.bs = L.bs;
         S.precond = (L.bs == 3) ? L.precond : CFEM_PRECOND_JACOBI;
         S.mode = L.mode;
-        S.nchunks = (int32_t)((L.n_rows + CHUNK_ROWS - 1) / CHUNK_ROWS);
+        S.crows = chunk_rows(L.bs);
+        S.nchunks = (int32_t)((L.n_rows + S.crows - 1) / S.crows);
+        S.ntiles = (S.nchunks + TILE - 1) / TILE;
         S.chunk0 = (int32_t)chunk_sys.size();
         S.max_iter = L.max_iter;
         S.rp = L.d_row_ptr;
@@ -589,11 +787,19 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.x = L.d_x;
         S.fixed = L.d_fixed;
         S.rtol2 = L.rtol * L.rtol;
+        const double dl = L.reliable_delta > 0.0 ? L.reliable_delta : RELIABLE_DELTA;
+        S.delta2 = dl * dl;
+        S.max_stall = L.max_stall > 0 ? L.max_stall : MAX_STALL;
+        S.hist_cap = L.d_history ? L.history_cap : 0;
+        S.hist = L.d_history;
         for (int c = 0; c < S.nchunks; ++c) chunk_sys.push_back(i);
         const size_t ts = (L.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
         const size_t nd = (size_t)L.n_rows * L.bs;
         const size_t nprec = (S.precond == CFEM_PRECOND_BLOCK) ? (size_t)L.n_rows * 9 : nd;
-        bytes += 5 * align(nd * ts) + align(nprec * ts) + align(S.nchunks * 4 * sizeof(double));
+        bytes += 5 * align(nd * ts) + align(nprec * ts) +
+                 align(S.nchunks * 4 * sizeof(double)) +
+                 align(S.ntiles * 4 * sizeof(double)) +
+                 align(S.ntiles * sizeof(unsigned));
         if (L.max_iter > max_iter) max_iter = L.max_iter;
     }
     const int n_chunks = (int)chunk_sys.size();
@@ -616,43 +822,47 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.q = take(nd * ts);
         S.dinv = take(nprec * ts);
         S.partial = (double *)take(S.nchunks * 4 * sizeof(double));
+        S.tpartial = (double *)take(S.ntiles * 4 * sizeof(double));
+        S.tcnt = (unsigned *)take(S.ntiles * sizeof(unsigned));
     }
     SysDev *d_sys = (SysDev *)take(n_systems * sizeof(SysDev));
     SysState *d_st = (SysState *)take(n_systems * sizeof(SysState));
     int32_t *d_chunks = (int32_t *)take(n_chunks * sizeof(int32_t));
     GridBar *d_bar = (GridBar *)take(sizeof(GridBar));
-    GridBar hbar{0u, 0u, 0, n_systems};
+    const int h_active = n_systems;
     CFEM_CUDA(cudaMemcpyAsync(d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
     CFEM_CUDA(cudaMemcpyAsync(d_chunks, chunk_sys.data(),
                               n_chunks * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    CFEM_CUDA(cudaMemcpyAsync(d_bar, &hbar, sizeof(GridBar),
+    CFEM_CUDA(cudaMemcpyAsync(&d_bar->active, &h_active, sizeof(int),
                               cudaMemcpyHostToDevice, s));
 
     int per_sm = 0;
     CFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &per_sm, k_pcg_persistent, SOLVE_THREADS, 0));
     CFEM_CHECK(per_sm > 0, CFEM_ERR_CUDA, "solver kernel cannot be resident");
-    if (per_sm > 4) per_sm = 4;
     int grid = ctx->num_sms * per_sm;
-    const int warps_needed = (n_chunks + 0);
-    const int max_blocks_useful = (warps_needed * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
-    if (grid > max_blocks_useful) grid = max_blocks_useful < 1 ? 1 : max_blocks_useful;
+    const int useful = (n_chunks * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
+    if (grid > useful) grid = useful < 1 ? 1 : useful;
+    if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     int max_steps = 3 * max_iter + 16;
-    void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
-                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     CFEM_CUDA(cudaEventCreate(&ev0));
     CFEM_CUDA(cudaEventCreate(&ev1));
     CFEM_CUDA(cudaEventRecord(ev0, s));
+    CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, s,
+                d_sys, d_st, d_chunks, n_chunks, d_bar);
+    void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
+                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
     CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
                                           dim3(SOLVE_THREADS), args, 0, s));
     CFEM_CUDA(cudaEventRecord(ev1, s));
     g_launches.fetch_add(1, std::memory_order_relaxed);
     std::vector<SysState> hst(n_systems);
+    int h_err = 0;
     CFEM_CUDA(cudaMemcpyAsync(hst.data(), d_st, n_systems * sizeof(SysState),
                               cudaMemcpyDeviceToHost, s));
-    CFEM_CUDA(cudaMemcpyAsync(&hbar, d_bar, sizeof(GridBar),
+    CFEM_CUDA(cudaMemcpyAsync(&h_err, &d_bar->err, sizeof(int),
                               cudaMemcpyDeviceToHost, s));
     tmp_free(ws, s);
     CFEM_CUDA(cudaStreamSynchronize(s));
@@ -671,7 +881,7 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         stats[i].bnorm = sqrt(hst[i].bb);
         stats[i].kernel_ms = (double)kms;
     }
-    CFEM_CHECK(hbar.err == 0, CFEM_ERR_TIMEOUT,
+    CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
     return CFEM_OK;
     CFEM_API_END

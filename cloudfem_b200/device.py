@@ -367,28 +367,41 @@ class BlockSystem:
         self.keep = keep
 
     def ensure_fp32(self):
+        """FP32 difference-form operator for the mixed solver."""
         torch = _torch()
         if self.vals32 is None:
             n = self.vals64.numel()
             self.vals32 = torch.empty(n, dtype=torch.float32,
                                       device=self.vals64.device)
-            N.check(self.rt.lib.cfem_to_fp32(
-                self.rt.ctx, n, ptr(self.vals64), ptr(self.vals32),
+
+            def p(v):
+                return v if isinstance(v, N._vp) else ptr(v)
+            N.check(self.rt.lib.cfem_mixed_matrix(
+                self.rt.ctx, self.n_rows, self.bs, p(self.row_ptr),
+                p(self.col), ptr(self.vals64), ptr(self.vals32),
                 self.rt.stream()))
         return self.vals32
 
-    def linsys(self, mode, rtol, max_iter):
+    def linsys(self, mode, rtol, max_iter, reliable_delta=0.0, max_stall=0,
+               history=None):
         def p(v):
             return v if isinstance(v, N._vp) else ptr(v)
         v32 = self.ensure_fp32() if mode == N.SOLVE_MIXED else None
+        cap = 0 if history is None else history.numel() // 2
         return N.LinSys(self.n_rows, self.bs, self.precond, p(self.row_ptr),
                         p(self.col), ptr(self.vals64), ptr(v32), ptr(self.b),
                         ptr(self.x), ptr(self.fixed), float(rtol),
-                        int(max_iter), int(mode))
+                        int(max_iter), int(mode), float(reliable_delta),
+                        int(max_stall), int(cap), ptr(history))
 
 
-def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None):
-    """Solve a batch of BlockSystems in one persistent launch."""
+def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None,
+        reliable_delta=0.0, max_stall=0, history=None):
+    """Solve a batch of BlockSystems in one persistent launch.
+
+    history: optional list (one device f64 tensor of 2*k entries per
+    system) receiving (iteration, relres) at each FP64 residual.
+    """
     if not systems:
         return []
     rt = systems[0].rt
@@ -396,7 +409,8 @@ def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None):
     for i, s in enumerate(systems):
         mi = max_iter if max_iter is not None else max(
             1000, 20 * int(np.sqrt(s.n_rows * s.bs)) + 2000)
-        arr[i] = s.linsys(mode, rtol, mi)
+        arr[i] = s.linsys(mode, rtol, mi, reliable_delta, max_stall,
+                          None if history is None else history[i])
     stats = (N.SolveStats * len(systems))()
     N.check(rt.lib.cfem_pcg_solve(rt.ctx, arr, len(systems), stats,
                                   rt.stream()))

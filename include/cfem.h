@@ -94,13 +94,20 @@ typedef struct cfem_linsys {
     const int32_t *d_row_ptr;
     const int32_t *d_col;
     const double *d_vals64;  /* FP64 values (required)                      */
-    const float *d_vals32;   /* FP32 copy (CFEM_SOLVE_MIXED), else NULL     */
+    const float *d_vals32;   /* CFEM_SOLVE_MIXED: FP32 difference-form copy
+                                from cfem_mixed_matrix; else NULL           */
     const double *d_b;       /* right-hand side, n_rows*bs                  */
     double *d_x;             /* in: guess + Dirichlet values; out: solution */
     const uint8_t *d_fixed;  /* n_rows*bs mask, or NULL                     */
     double rtol;             /* ||b - A x||_free <= rtol * ||b_lift||_free  */
     int32_t max_iter;
     int32_t mode;            /* CFEM_SOLVE_*                                */
+    double reliable_delta;   /* mixed: replace r when it fell by this factor
+                                since the last replacement (0 -> 0.1)       */
+    int32_t max_stall;       /* true-residual replacements without a 4x
+                                gain before giving up (0 -> 8)              */
+    int32_t history_cap;     /* entries of d_history (0 = none)             */
+    double *d_history;       /* (iteration, relres) at every FP64 residual  */
 } cfem_linsys;
 
 typedef struct cfem_solve_stats {
@@ -218,6 +225,16 @@ CFEM_API int cfem_dirichlet_csr(cfem_ctx *ctx, int64_t n, const int32_t *d_indpt
                        const double *d_fixed_val, int32_t *d_out_indptr,
                        int32_t *d_out_indices, double *d_out_vals,
                        double *d_rhs_out, int64_t *nnz_out, void *stream);
+
+/* FP32 operator for CFEM_SOLVE_MIXED in difference form: off-diagonal
+ * blocks rounded to FP32 and, in each diagonal slot, the FP64 block row
+ * sum s_i = sum_j A_ij rounded once. The solver applies it as
+ * s_i p_i + sum_{j!=i} A_ij (p_j - p_i), which keeps constant vectors
+ * (rigid translations) exact under FP32 rounding. Same layout as d_vals64. */
+CFEM_API int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
+                               const int32_t *d_row_ptr, const int32_t *d_col,
+                               const double *d_vals64, float *d_vals32,
+                               void *stream);
 
 /* ---- solver -------------------------------------------------------------
  * Jacobi-preconditioned CG on a batch of independent systems in ONE

@@ -29,13 +29,28 @@ def golden_csr(golden, name):
                           golden[name + "__indptr"]), shape=shape)
 
 
+def _drop_zeros(A, tol):
+    """Remove entries with |v| <= tol * max|v| (exact zeros included).
+
+    The reference's Dirichlet step stores its cleared columns as explicit
+    zeros, and on Kuhn meshes some P1 couplings cancel to exactly 0.0 in the
+    reference's LAPACK arithmetic but to ~1e-17 in any other order of
+    operations, so post-BC structures are compared without (near-)zeros.
+    """
+    A = A.tocsr().copy()
+    scale = float(np.abs(A.data).max(initial=0.0))
+    A.data[np.abs(A.data) <= tol * scale] = 0.0
+    A.eliminate_zeros()
+    return A
+
+
 def assert_csr_equal(A, B, rtol=1e-12, eliminate=False):
     """Bit-exact structure and values within rtol of the largest entry."""
     A = A.tocsr().copy()
     B = B.tocsr().copy()
     if eliminate:
-        A.eliminate_zeros()
-        B.eliminate_zeros()
+        A = _drop_zeros(A, 1e-13)
+        B = _drop_zeros(B, 1e-13)
     assert A.shape == B.shape
     np.testing.assert_array_equal(np.asarray(A.indptr, np.int64),
                                   np.asarray(B.indptr, np.int64))
