@@ -116,20 +116,22 @@ def _free_dofs(mesh):
     return 3 * mesh.n_nodes - 3 * len(mesh.boundaries["xmin"])
 
 
-def pcg_bytes(n_nodes, nnzb, iters, updates):
-    """Algorithmic HBM bytes of one mixed-precision (bs = 3) solve launch.
+def pcg_bytes(n_nodes, nnzb, iters, updates, precision="mixed"):
+    """Algorithmic HBM bytes of one solve launch (3x3 blocks, s = 4 B for
+    the mixed path's FP32 vectors and matrix, 8 B for the FP64 path).
 
-    Phase A per iteration: FP32 3x3 blocks + column index (40 B / block),
-    row pointers, read z and p, write p and q (4 x 12 B / node).
-    Phase B: read p, q, r, dinv (36 B), fixed mask (3 B), x (24 B), write
-    x, r, z: 12*3 + 36 + 3 + 24 + 24 + 12*2 = 147 B / node.
-    Phase R (reliable update, plus INIT once): FP64 blocks + index
+    Phase A per iteration: blocks + column index (9 s + 4 B / block), row
+    pointers, read z and p, write p and q (4 x 3 s B / node).
+    Phase B: read p, q, r (9 s), block-Jacobi inverse (9 s), fixed mask
+    (3 B), x (24 B), write x (24 B), r, z (6 s) per node.
+    Phase R (true residual; plus INIT once): FP64 blocks + index
     (76 B / block), row pointers, read x, b (48 B), fixed mask (3 B), write
-    r, z (24 B).
+    r, z (6 s).
     """
-    a = nnzb * 40 + 4 * (n_nodes + 1) + 48 * n_nodes
-    b = 147 * n_nodes
-    r = nnzb * 76 + 4 * (n_nodes + 1) + 75 * n_nodes
+    sz = 4 if precision == "mixed" else 8
+    a = nnzb * (9 * sz + 4) + 4 * (n_nodes + 1) + 12 * sz * n_nodes
+    b = (24 * sz + 51) * n_nodes
+    r = nnzb * 76 + 4 * (n_nodes + 1) + (51 + 6 * sz) * n_nodes
     return iters * (a + b) + (updates + 1) * r
 
 
@@ -163,13 +165,20 @@ def run_ours(args, rank, world, local_rank):
     dm = DeviceMesh(mesh, local_rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
-    # FP64 plain reference solution (accuracy gate) and its speed.
+    # FP64 plain reference solution (accuracy gate) and one solve in the
+    # other precision, reported beside the timed one.
+    _device_step(dm, mesh, "fp64")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     x64, info64 = _device_step(dm, mesh, "fp64")
     torch.cuda.synchronize()
     fp64_s = time.perf_counter() - t0
     u64 = x64.clone()
+    t0 = time.perf_counter()
+    xm, infom = _device_step(dm, mesh, "mixed")
+    torch.cuda.synchronize()
+    mixed_s = time.perf_counter() - t0
+    mixed_err = float(torch.linalg.norm(xm - u64) / torch.linalg.norm(u64))
 
     for _ in range(args.warmup):
         _device_step(dm, mesh, args.precision)
@@ -229,7 +238,7 @@ def run_ours(args, rank, world, local_rank):
     pat = dm.pattern
     last = infos[-1]
     bytes_launch = pcg_bytes(mesh.n_nodes, pat.nnz, last.iterations,
-                             last.residual_updates)
+                             last.residual_updates, args.precision)
     peak, peak_kind = _peaks()
     achieved = bytes_launch / (last.kernel_ms * 1e-3) / 1e9
     h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
@@ -259,6 +268,11 @@ def run_ours(args, rank, world, local_rank):
             "fp64_plain": {"iterations": info64.iterations,
                            "dof_per_s": free / fp64_s,
                            "kernel_ms": info64.kernel_ms},
+            "mixed": {"iterations": infom.iterations,
+                      "residual_updates": infom.residual_updates,
+                      "dof_per_s": free / mixed_s,
+                      "kernel_ms": infom.kernel_ms,
+                      "rel_err_vs_fp64_plain": mixed_err},
             "l2": "256 MiB buffer written between timed steps",
             "parallelism": f"replicas x{world}",
         },
@@ -327,7 +341,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -70,7 +70,7 @@ struct SysDev {
 };
 
 struct SysState {
-    double rz, alpha, beta, bb, rmax2, best, relres;
+    double rz, alpha, beta, bb, rmax2, best, relres, zeta;
     int32_t phase, iter, status, nres, stall, pbuf;
     unsigned int cnt;
     int32_t pad;
@@ -87,6 +87,12 @@ struct GridBar {
     unsigned int grp[BAR_MAX_GROUPS][32];
 };
 
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -100,6 +106,7 @@ __device__ bool grid_sync(GridBar *bar) {
     if (threadIdx.x == 0) {
         volatile unsigned *vgen = &bar->gen;
         volatile int *verr = &bar->err;
+        (void)vgen;
         const unsigned nb = gridDim.x;
         const unsigned grp = blockIdx.x / BAR_GROUP;
         const unsigned ngrp = (nb + BAR_GROUP - 1) / BAR_GROUP;
@@ -120,13 +127,14 @@ __device__ bool grid_sync(GridBar *bar) {
         if (!released) {
             unsigned long long t0 = globaltimer();
             unsigned spins = 0;
-            while (*vgen == g) {
-                if (*verr) break;
-                if ((++spins & 255u) == 0 && globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
-                    atomicExch(&bar->err, 1);
-                    break;
+            while (ld_acquire(&bar->gen) == g) {
+                if ((++spins & 1023u) == 0) {
+                    if (*verr) break;
+                    if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+                        atomicExch(&bar->err, 1);
+                        break;
+                    }
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -207,7 +215,8 @@ __device__ __forceinline__ T apply_prec_lane(const SysDev &S, int64_t row, int c
 }
 
 // ---------------------------------------------------------------- phase A
-// q = A p with p = z + beta p_old. Each lane group of LANES lanes works on
+// q = A p with p = zeta z + beta p_old (zeta = 1 except right after a
+// true-residual replacement, see advance()). Each lane group of LANES lanes works on
 // two block rows at once and unrolls U column blocks per row, so every lane
 // keeps 2U independent (index -> gather) load chains in flight.
 //
@@ -223,6 +232,7 @@ __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
                         int64_t r1, int lane, double part[4]) {
     constexpr int B2 = BS * BS;
     const T beta = (T)vcg(&st->beta);
+    const T zeta = (T)vcg(&st->zeta);
     const int pbuf = vcgi(&st->pbuf);
     const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
     T *pout = (T *)(pbuf ? S.p0 : S.p1);
@@ -246,7 +256,7 @@ __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
             k1[h] = valid[h] ? __ldg(S.rp + rr + 1) : 0;
 #pragma unroll
             for (int c = 0; c < BS; ++c) {
-                pi[h][c] = ldcg(z + rr * BS + c) + beta * ldcg(pin + rr * BS + c);
+                pi[h][c] = zeta * ldcg(z + rr * BS + c) + beta * ldcg(pin + rr * BS + c);
                 acc[h][c] = 0;
             }
         }
@@ -276,7 +286,7 @@ __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
                     T pj[BS];
 #pragma unroll
                     for (int d = 0; d < BS; ++d) {
-                        pj[d] = ldcg(z + j[h][u] * BS + d) +
+                        pj[d] = zeta * ldcg(z + j[h][u] * BS + d) +
                                 beta * ldcg(pin + j[h][u] * BS + d);
                         if (DIFF) pj[d] = (j[h][u] == row[h]) ? pi[h][d] : pj[d] - pi[h][d];
                     }
@@ -378,14 +388,15 @@ __device__ __forceinline__ void acc_R(const double *__restrict__ v,
 }
 
 template <typename T, int BS, bool INIT>
-__device__ void phase_R(const SysDev &S, int64_t r0, int64_t r1, int lane,
-                        double part[4], int *bad) {
+__device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
+                        int64_t r1, int lane, double part[4], int *bad) {
     const int sub = lane & (LANES - 1), grp = lane / LANES;
     T *r = (T *)S.r;
     T *z = (T *)S.z;
     T *dinv = (T *)S.dinv;
+    const T *pc = (const T *)((INIT || vcgi(&st->pbuf) == 0) ? S.p0 : S.p1);
     double rr = 0.0, bb = 0.0, aa = 0.0;
-    T rz = 0;
+    T rz = 0, rp = 0;
     for (int64_t base = r0; base < r1; base += RPP) {
         const int64_t row = base + grp;
         const bool valid = row < r1;
@@ -464,11 +475,12 @@ __device__ void phase_R(const SysDev &S, int64_t r0, int64_t r1, int lane,
                 if (fx[c]) zv = 0;
                 z[row * BS + c] = zv;
                 rz += rv[c] * zv;
+                if (!INIT) rp += rv[c] * ldcg(pc + row * BS + c);
             }
         }
     }
     part[0] += rr;
-    part[1] += bb;
+    part[1] += INIT ? bb : (double)rp;
     part[2] += (double)rz;
     part[3] += aa;
 }
@@ -501,6 +513,7 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
         } else {
             st->rz = rz;
             st->beta = 0.0;
+            st->zeta = 1.0;
             st->rmax2 = rr;
             st->best = rr;
             st->relres = sqrt(rr / bb);
@@ -513,6 +526,7 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
         } else {
             st->alpha = st->rz / pq;
             st->pbuf ^= 1;
+            st->zeta = 1.0;
             next = PH_B;
         }
     } else if (ph == PH_B) {
@@ -533,7 +547,7 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
             next = PH_A;
         }
     } else if (ph == PH_R) {
-        const double rr = tot[0], rz = tot[2], bb = st->bb;
+        const double rr = tot[0], rp = tot[1], rz = tot[2], bb = st->bb;
         const double floor2 = FLOOR_C * FLOOR_C * tot[3];
         if (st->nres < S.hist_cap) {
             S.hist[2 * st->nres] = (double)st->iter;
@@ -557,7 +571,12 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
             if (st->stall >= S.max_stall) {
                 st->status = CFEM_ERR_NOT_CONVERGED;
             } else {
-                st->beta = rz / st->rz;
+                // The replaced residual is no longer orthogonal to the last
+                // search direction; restore r.p' = 0 with p' = p - g z,
+                // g = r.p / r.z, folded into the next p = z + beta p'.
+                const double beta = rz / st->rz;
+                st->beta = beta;
+                st->zeta = (rz != 0.0) ? 1.0 - beta * (rp / rz) : 1.0;
                 st->rz = rz;
                 st->rmax2 = rr;
                 next = PH_A;
@@ -597,6 +616,13 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
     }
 #pragma unroll
     for (int v = 0; v < 4; ++v) t[v] = warp_sum(t[v]);
+    if (S.ntiles == 1) {            // the tile is the whole system
+        if (lane == 0) {
+            S.tcnt[0] = 0;
+            advance(S, st, bar, ph, t);
+        }
+        return;
+    }
     int last_sys = 0;
     if (lane == 0) {
         S.tcnt[tile] = 0;
@@ -628,7 +654,7 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
     int bad = 0;
     if (INIT) {
         int flag = 0;
-        phase_R<T, BS, true>(S, r0, r1, lane, part, &flag);
+        phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
         bad = __any_sync(0xffffffffu, flag != 0);
     } else {
         switch (ph) {
@@ -637,7 +663,7 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
                 else phase_A<T, BS, false, 1>(S, st, r0, r1, lane, part);
                 break;
             case PH_B: phase_B<T, BS>(S, st, r0, r1, lane, part); break;
-            case PH_R: phase_R<T, BS, false>(S, r0, r1, lane, part, &bad); break;
+            case PH_R: phase_R<T, BS, false>(S, st, r0, r1, lane, part, &bad); break;
             default: phase_zero<BS>(S, r0, r1, lane); break;
         }
     }
