@@ -102,6 +102,9 @@ SIGNATURES = [
      [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     ("cfem_pcg_solve", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), _i32, ctypes.POINTER(SolveStats), _vp]),
+    ("cfem_pcg_noalloc_capacity", ctypes.c_size_t, []),
+    ("cfem_pcg_solve_noalloc", ctypes.c_int,
+     [_vp, ctypes.POINTER(LinSys), ctypes.POINTER(SolveStats), _vp]),
 ]
 
 _lib = None

@@ -27,6 +27,9 @@
 #include "cfem_common.cuh"
 
 #include <math.h>
+#include <string.h>
+
+#include <mutex>
 #include <vector>
 
 namespace cfem {
@@ -907,6 +910,171 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         stats[i].bnorm = sqrt(hst[i].bb);
         stats[i].kernel_ms = (double)kms;
     }
+    CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
+               "solver grid barrier timed out (device wait bound reached)");
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of cfem_pcg_solve for one system.
+//
+// Some callers cannot allocate device memory at solve time: an application
+// that reserves the whole HBM budget for its own pools up front (so any
+// library allocation mid-run can fail or fragment that budget), and
+// latency-bound control loops that cannot afford the implicit
+// synchronisation and unbounded latency of cudaMalloc. For them the solver
+// workspace lives in one file-scope device array of fixed size, loaded with
+// the library and held by every GPU that loads it until the process exits.
+// The same kernels as cfem_pcg_solve run on it; nothing is allocated.
+namespace cfem {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;   // 32 MiB
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device. In host code the array's
+// name is only a host-side stand-in, so the address is looked up once per
+// device with that device current and passed to the kernels.
+static void *g_noalloc_addr[64] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(int device, void **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    CFEM_CHECK(device >= 0 && device < 64, CFEM_ERR_INVALID,
+               "device %d out of range for the allocation-free solver", device);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        CFEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        CFEM_CHECK(p != nullptr, CFEM_ERR_CUDA, "scratch symbol has no address");
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return CFEM_OK;
+}
+
+}  // namespace cfem
+
+extern "C" size_t cfem_pcg_noalloc_capacity(void) { return NOALLOC_SCRATCH_BYTES; }
+
+extern "C" int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *L,
+                                      cfem_solve_stats *stats, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && L && stats, CFEM_ERR_INVALID,
+               "cfem_pcg_solve_noalloc: NULL argument");
+    CFEM_CHECK(L->bs == 1 || L->bs == 3, CFEM_ERR_INVALID,
+               "block size %d (1 or 3)", L->bs);
+    CFEM_CHECK(L->n_rows > 0 && L->d_row_ptr && L->d_col && L->d_vals64 &&
+                   L->d_b && L->d_x,
+               CFEM_ERR_INVALID, "missing arrays");
+    CFEM_CHECK(L->mode == CFEM_SOLVE_FP64 ||
+                   (L->mode == CFEM_SOLVE_MIXED && L->d_vals32),
+               CFEM_ERR_INVALID, "mixed mode needs FP32 values");
+    CFEM_CHECK(L->rtol > 0.0 && L->max_iter > 0, CFEM_ERR_INVALID,
+               "rtol and max_iter must be positive");
+    CFEM_CHECK(L->n_rows < ((int64_t)1 << 31) / 9, CFEM_ERR_INVALID,
+               "system too large");
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+
+    SysDev S;
+    memset(&S, 0, sizeof(S));
+    S.n = L->n_rows;
+    S.bs = L->bs;
+    S.precond = (L->bs == 3) ? L->precond : CFEM_PRECOND_JACOBI;
+    S.mode = L->mode;
+    S.crows = chunk_rows(L->bs);
+    S.nchunks = (int32_t)((L->n_rows + S.crows - 1) / S.crows);
+    S.ntiles = (S.nchunks + TILE - 1) / TILE;
+    S.chunk0 = 0;
+    S.max_iter = L->max_iter;
+    S.rp = L->d_row_ptr;
+    S.ci = L->d_col;
+    S.v64 = L->d_vals64;
+    S.v32 = L->d_vals32;
+    S.b = L->d_b;
+    S.x = L->d_x;
+    S.fixed = L->d_fixed;
+    S.rtol2 = L->rtol * L->rtol;
+    const double dl = L->reliable_delta > 0.0 ? L->reliable_delta : RELIABLE_DELTA;
+    S.delta2 = dl * dl;
+    S.max_stall = L->max_stall > 0 ? L->max_stall : MAX_STALL;
+    S.hist_cap = L->d_history ? L->history_cap : 0;
+    S.hist = L->d_history;
+
+    auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
+    const size_t nd = (size_t)S.n * S.bs;
+    const size_t nprec = (S.precond == CFEM_PRECOND_BLOCK) ? (size_t)S.n * 9 : nd;
+    const size_t need = 5 * align(nd * ts) + align(nprec * ts) +
+                        align(S.nchunks * 4 * sizeof(double)) +
+                        align(S.ntiles * 4 * sizeof(double)) +
+                        align(S.ntiles * sizeof(unsigned)) + align(sizeof(SysDev)) +
+                        align(sizeof(SysState)) + align(S.nchunks * sizeof(int32_t)) +
+                        align(sizeof(GridBar));
+    CFEM_CHECK(need <= NOALLOC_SCRATCH_BYTES, CFEM_ERR_INVALID,
+               "system needs %zu bytes of solver scratch; the allocation-free "
+               "entry point has a fixed %zu (use cfem_pcg_solve)",
+               need, NOALLOC_SCRATCH_BYTES);
+
+    void *base = nullptr;
+    CFEM_TRY(noalloc_scratch(ctx->device, &base));
+    char *ws = (char *)base;
+    // Every call reuses the array: clear all of it that this call uses
+    // (state, tickets, chunk table, p buffers) before the launch.
+    CFEM_CUDA(cudaMemsetAsync(ws, 0, need, s));
+    size_t off = 0;
+    auto take = [&](size_t b) { char *p = ws + off; off += align(b); return (void *)p; };
+    S.r = take(nd * ts);
+    S.z = take(nd * ts);
+    S.p0 = take(nd * ts);
+    S.p1 = take(nd * ts);
+    S.q = take(nd * ts);
+    S.dinv = take(nprec * ts);
+    S.partial = (double *)take(S.nchunks * 4 * sizeof(double));
+    S.tpartial = (double *)take(S.ntiles * 4 * sizeof(double));
+    S.tcnt = (unsigned *)take(S.ntiles * sizeof(unsigned));
+    SysDev *d_sys = (SysDev *)take(sizeof(SysDev));
+    SysState *d_st = (SysState *)take(sizeof(SysState));
+    int32_t *d_chunks = (int32_t *)take(S.nchunks * sizeof(int32_t));  // all 0
+    GridBar *d_bar = (GridBar *)take(sizeof(GridBar));
+    const int h_active = 1;
+    CFEM_CUDA(cudaMemcpyAsync(d_sys, &S, sizeof(SysDev), cudaMemcpyHostToDevice, s));
+    CFEM_CUDA(cudaMemcpyAsync(&d_bar->active, &h_active, sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+
+    int per_sm = 0;
+    CFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_pcg_persistent, SOLVE_THREADS, 0));
+    CFEM_CHECK(per_sm > 0, CFEM_ERR_CUDA, "solver kernel cannot be resident");
+    int n_chunks = S.nchunks;
+    int grid = ctx->num_sms * per_sm;
+    const int useful = (n_chunks * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
+    if (grid > useful) grid = useful < 1 ? 1 : useful;
+    if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
+    int max_steps = 3 * L->max_iter + 16;
+    CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, s,
+                d_sys, d_st, d_chunks, n_chunks, d_bar);
+    void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
+                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
+    CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
+                                          dim3(SOLVE_THREADS), args, 0, s));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    SysState hst;
+    int h_err = 0;
+    CFEM_CUDA(cudaMemcpyAsync(&hst, d_st, sizeof(SysState), cudaMemcpyDeviceToHost, s));
+    CFEM_CUDA(cudaMemcpyAsync(&h_err, &d_bar->err, sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    stats->status = hst.status;
+    if (hst.status == CFEM_OK && hst.phase != PH_DONE)
+        stats->status = CFEM_ERR_NOT_CONVERGED;
+    stats->iterations = hst.iter;
+    stats->residual_updates = hst.nres;
+    stats->pad_ = 0;
+    stats->relres = hst.relres;
+    stats->bnorm = sqrt(hst.bb);
+    stats->kernel_ms = 0.0;
     CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
     return CFEM_OK;

@@ -417,6 +417,28 @@ def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None,
     return [SolveResult(s) for s in stats]
 
 
+def pcg_noalloc(system, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None):
+    """Solve one BlockSystem without any device allocation by the library.
+
+    For callers that cannot allocate device memory at solve time (an
+    application that has reserved the whole HBM budget for its own pools,
+    or a latency-bound loop that cannot take cudaMalloc's implicit
+    synchronisation): the workspace is libcfem's fixed 32 MiB device array
+    (``cfem_pcg_noalloc_capacity()``), so larger systems raise ValueError.
+    Concurrent calls on one GPU share that array and must not overlap. The
+    FP32 operator of the mixed mode is the caller's to provide (made here
+    once by ``ensure_fp32`` if missing).
+    """
+    rt = system.rt
+    mi = max_iter if max_iter is not None else max(
+        1000, 20 * int(np.sqrt(system.n_rows * system.bs)) + 2000)
+    ls = system.linsys(mode, rtol, mi)
+    st = N.SolveStats()
+    N.check(rt.lib.cfem_pcg_solve_noalloc(rt.ctx, ctypes.byref(ls),
+                                          ctypes.byref(st), rt.stream()))
+    return SolveResult(st)
+
+
 def raise_for(result, what="solve"):
     if result.status == N.CFEM_OK:
         return

@@ -249,6 +249,25 @@ CFEM_API int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
 CFEM_API int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
                    int32_t n_systems, cfem_solve_stats *stats, void *stream);
 
+/* Allocation-free variant of cfem_pcg_solve for ONE system. It has no
+ * counterpart in the reference, which only solves on the host with SciPy.
+ * It is for callers that cannot allocate device memory while solving: an
+ * application that reserves the whole HBM budget for its own pools up front
+ * (a library allocation mid-run could fail or fragment that budget), or a
+ * latency-bound control loop that cannot take cudaMalloc's implicit
+ * synchronisation. The solver workspace is a fixed file-scope device array
+ * of cfem_pcg_noalloc_capacity() bytes (32 MiB), held by every GPU that
+ * loads the library until the process exits; systems that need more are
+ * rejected with CFEM_ERR_INVALID. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. Every call reuses the same array and clears it
+ * first: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller. stats->kernel_ms is 0 (no timing
+ * events are created). Otherwise identical to cfem_pcg_solve. Synchronises. */
+CFEM_API size_t cfem_pcg_noalloc_capacity(void);
+CFEM_API int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *system,
+                                    cfem_solve_stats *stats, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
