@@ -280,7 +280,8 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {
-            "kernel": "k_pcg_persistent",
+            "kernel": "pcg solve launch sequence (k_pcg_init + graph of "
+                      "k_gx SpMV / k_greduce / k_gb update / k_greduce)",
             "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "bytes_per_launch": bytes_launch,

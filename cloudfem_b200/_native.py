@@ -29,6 +29,7 @@ OP_P1_ELAST, OP_T10_ELAST = 5, 6
 COEF_CONST, COEF_ELEM, COEF_QP, COEF_NODAL = 0, 1, 2, 3
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK = 0, 1
+SCHED_AUTO, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
 
 STATUS_NAMES = {
     CFEM_OK: "ok", CFEM_ERR_INVALID: "invalid argument",
@@ -72,6 +73,7 @@ SIGNATURES = [
     ("cfem_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("cfem_ctx_destroy", ctypes.c_int, [_vp]),
     ("cfem_ctx_launch_count", _i64, [_vp]),
+    ("cfem_ctx_set_scheduler", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cfem_pattern_create", ctypes.c_int,
      [_vp, _vp, _i64, _i32, _i64, _vp, ctypes.POINTER(_vp)]),
     ("cfem_pattern_destroy", ctypes.c_int, [_vp]),

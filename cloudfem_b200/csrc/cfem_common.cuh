@@ -68,6 +68,10 @@ struct cfem_ctx {
     int num_sms = 0;
     int cc_major = 0, cc_minor = 0;
     int64_t launches_at_create = 0;
+    int scheduler = 0;                 // CFEM_SCHED_*
+    cudaStream_t work = nullptr;       // capture stream of the graph scheduler
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int *h_flags = nullptr;            // pinned host words (convergence polling)
 };
 
 struct cfem_pattern {

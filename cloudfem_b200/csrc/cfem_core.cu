@@ -127,13 +127,32 @@ int cfem_ctx_create(int device, cfem_ctx **out) {
     c->cc_major = prop.major;
     c->cc_minor = prop.minor;
     c->launches_at_create = g_launches.load();
+    CFEM_CUDA(cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking));
+    for (int i = 0; i < 4; ++i)
+        CFEM_CUDA(cudaEventCreateWithFlags(&c->ev[i], i < 2 ? cudaEventDisableTiming
+                                                            : cudaEventDefault));
+    CFEM_CUDA(cudaMallocHost(&c->h_flags, 4 * sizeof(int)));
     *out = c;
     return CFEM_OK;
     CFEM_API_END
 }
 
 int cfem_ctx_destroy(cfem_ctx *ctx) {
+    if (!ctx) return CFEM_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->work) cudaStreamSynchronize(ctx->work);
+    for (int i = 0; i < 4; ++i)
+        if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->work) cudaStreamDestroy(ctx->work);
+    if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     delete ctx;
+    return CFEM_OK;
+}
+
+int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler) {
+    CFEM_CHECK(ctx && scheduler >= CFEM_SCHED_AUTO && scheduler <= CFEM_SCHED_GRAPH,
+               CFEM_ERR_INVALID, "unknown scheduler %d", scheduler);
+    ctx->scheduler = scheduler;
     return CFEM_OK;
 }
 

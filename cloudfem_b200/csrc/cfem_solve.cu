@@ -29,6 +29,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -70,6 +71,11 @@ struct SysDev {
     double rtol2, delta2;
     int32_t max_stall, hist_cap;
     double *hist;
+    // graph scheduler: update-phase chunks (whole block rows, <= 32 DOFs)
+    int32_t nchunksB, pad_;
+    double *partialB;     // nchunksB * 4
+    const void *vsoa;     // working-precision block values, entry-major
+    int64_t nnzb;         // blocks of the matrix (stride of vsoa)
 };
 
 struct SysState {
@@ -100,6 +106,13 @@ __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+__device__ __forceinline__ unsigned atom_add_acqrel(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
 }
 
 // Bounded two-level software grid barrier over co-resident blocks
@@ -321,6 +334,8 @@ __device__ void phase_A(const SysDev &S, const SysState *st, int64_t r0,
 }
 
 // ---------------------------------------------------------------- phase B
+// One lane per DOF of the chunk; every load (vectors, mask, the lane's row
+// of the Jacobi inverse) is issued before any is used.
 template <typename T, int BS>
 __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
                         int64_t r1, int lane, double part[4]) {
@@ -331,22 +346,41 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     T *r = (T *)S.r;
     T *z = (T *)S.z;
     const T *q = (const T *)S.q;
+    const T *dinv = (const T *)S.dinv;
+    const bool blockj = BS == 3 && S.precond == CFEM_PRECOND_BLOCK;
     const int64_t i = r0 * BS + lane;
     const bool valid = i < r1 * BS;
-    const int64_t row = r0 + lane / BS;
-    const int c = lane - (lane / BS) * BS;
-    bool fx = false;
-    T rv = 0;
-    if (valid) {
-        fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
-        rv = ldcg(r + i);
-        if (!fx) {
-            const T pi = ldcg(p + i);
-            S.x[i] = ldcg(S.x + i) + alpha64 * (double)pi;
-            rv -= alpha * ldcg(q + i);
-        }
+    const int64_t ii = valid ? i : r0 * BS;
+    const int64_t row = ii / BS;
+    const int c = (int)(ii - row * BS);
+    const bool fx = S.fixed ? (__ldg(S.fixed + ii) != 0) : false;
+    T rv = ldcg(r + ii);
+    const T pi = ldcg(p + ii);
+    const T qi = ldcg(q + ii);
+    const double xi = ldcg(S.x + ii);
+    T d0, d1 = 0, d2 = 0;
+    if (blockj) {
+        const T *D = dinv + row * 9 + c * 3;
+        d0 = ldcg(D);
+        d1 = ldcg(D + 1);
+        d2 = ldcg(D + 2);
+    } else {
+        d0 = ldcg(dinv + ii);
     }
-    T zv = apply_prec_lane<T, BS>(S, row, c, lane, rv, valid);
+    if (valid && !fx) {
+        S.x[i] = xi + alpha64 * (double)pi;
+        rv -= alpha * qi;
+    }
+    T zv;
+    if (blockj) {
+        const int base = lane - c;
+        const T ra = __shfl_sync(0xffffffffu, rv, base >= 0 ? base : 0);
+        const T rb = __shfl_sync(0xffffffffu, rv, base + 1 < 32 ? base + 1 : 31);
+        const T rc = __shfl_sync(0xffffffffu, rv, base + 2 < 32 ? base + 2 : 31);
+        zv = d0 * ra + d1 * rb + d2 * rc;
+    } else {
+        zv = d0 * rv;
+    }
     T rz = 0, rr = 0;
     if (valid) {
         if (fx) zv = 0;
@@ -605,8 +639,7 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
 #pragma unroll
         for (int v = 0; v < 4; ++v) S.partial[(int64_t)lc * 4 + v] = part[v];
         if (bad) atomicExch(&st->status, CFEM_ERR_BREAKDOWN);
-        __threadfence();
-        last = (atomicAdd(&S.tcnt[tile], 1u) == (unsigned)tsize - 1) ? 1 : 0;
+        last = (atom_add_acqrel(&S.tcnt[tile], 1u) == (unsigned)tsize - 1) ? 1 : 0;
     }
     last = __shfl_sync(0xffffffffu, last, 0);
     if (!last) return;
@@ -631,8 +664,7 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
         S.tcnt[tile] = 0;
 #pragma unroll
         for (int v = 0; v < 4; ++v) S.tpartial[(int64_t)tile * 4 + v] = t[v];
-        __threadfence();
-        last_sys = (atomicAdd(&st->cnt, 1u) == (unsigned)S.ntiles - 1) ? 1 : 0;
+        last_sys = (atom_add_acqrel(&st->cnt, 1u) == (unsigned)S.ntiles - 1) ? 1 : 0;
     }
     last_sys = __shfl_sync(0xffffffffu, last_sys, 0);
     if (!last_sys) return;
@@ -648,24 +680,31 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
     advance(S, st, bar, ph, tot);
 }
 
-template <typename T, int BS, bool INIT>
+// Which phases a kernel handles.
+enum { RUN_INIT = 0, RUN_ALL = 1, RUN_X = 2, RUN_B = 3 };
+
+template <typename T, int BS, int RUN>
 __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
                           int lc, int lane) {
     const int64_t r0 = (int64_t)lc * S.crows;
     const int64_t r1 = min(S.n, r0 + S.crows);
     double part[4] = {0.0, 0.0, 0.0, 0.0};
     int bad = 0;
-    if (INIT) {
+    if (RUN == RUN_INIT) {
         int flag = 0;
         phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
         bad = __any_sync(0xffffffffu, flag != 0);
+    } else if (RUN == RUN_B) {
+        phase_B<T, BS>(S, st, r0, r1, lane, part);
     } else {
         switch (ph) {
             case PH_A:
                 if (sizeof(T) == 4) phase_A<T, BS, true, 2>(S, st, r0, r1, lane, part);
                 else phase_A<T, BS, false, 1>(S, st, r0, r1, lane, part);
                 break;
-            case PH_B: phase_B<T, BS>(S, st, r0, r1, lane, part); break;
+            case PH_B:
+                if (RUN == RUN_ALL) phase_B<T, BS>(S, st, r0, r1, lane, part);
+                break;
             case PH_R: phase_R<T, BS, false>(S, st, r0, r1, lane, part, &bad); break;
             default: phase_zero<BS>(S, r0, r1, lane); break;
         }
@@ -673,22 +712,24 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
     finish_chunk(S, st, bar, lc, ph, part, lane, bad);
 }
 
-template <bool INIT>
+template <int RUN>
 __device__ __forceinline__ void dispatch(const SysDev *__restrict__ sys,
                                          SysState *st, GridBar *bar,
                                          const int32_t *__restrict__ chunk_sys,
                                          int c, int lane) {
     const int s = __ldg(chunk_sys + c);
     const SysDev &S = sys[s];
-    const int ph = INIT ? PH_INIT : *(volatile int32_t *)&st[s].phase;
+    const int ph = RUN == RUN_INIT ? PH_INIT : *(volatile int32_t *)&st[s].phase;
     if (ph == PH_DONE) return;
+    if (RUN == RUN_X && ph == PH_B) return;
+    if (RUN == RUN_B && ph != PH_B) return;
     const int lc = c - S.chunk0;
     if (S.mode == CFEM_SOLVE_MIXED) {
-        if (S.bs == 3) run_chunk<float, 3, INIT>(S, &st[s], bar, ph, lc, lane);
-        else run_chunk<float, 1, INIT>(S, &st[s], bar, ph, lc, lane);
+        if (S.bs == 3) run_chunk<float, 3, RUN>(S, &st[s], bar, ph, lc, lane);
+        else run_chunk<float, 1, RUN>(S, &st[s], bar, ph, lc, lane);
     } else {
-        if (S.bs == 3) run_chunk<double, 3, INIT>(S, &st[s], bar, ph, lc, lane);
-        else run_chunk<double, 1, INIT>(S, &st[s], bar, ph, lc, lane);
+        if (S.bs == 3) run_chunk<double, 3, RUN>(S, &st[s], bar, ph, lc, lane);
+        else run_chunk<double, 1, RUN>(S, &st[s], bar, ph, lc, lane);
     }
 }
 
@@ -698,7 +739,7 @@ k_pcg_init(const SysDev *__restrict__ sys, SysState *st,
            const int32_t *__restrict__ chunk_sys, int n_chunks, GridBar *bar) {
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c >= n_chunks) return;
-    dispatch<true>(sys, st, bar, chunk_sys, c, threadIdx.x & 31);
+    dispatch<RUN_INIT>(sys, st, bar, chunk_sys, c, threadIdx.x & 31);
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS, 1)
@@ -711,7 +752,7 @@ k_pcg_persistent(const SysDev *__restrict__ sys, SysState *st,
     if (*(volatile int *)&bar->active <= 0) return;
     for (int step = 0; step < max_steps; ++step) {
         for (int c = gw; c < n_chunks; c += nw)
-            dispatch<false>(sys, st, bar, chunk_sys, c, lane);
+            dispatch<RUN_ALL>(sys, st, bar, chunk_sys, c, lane);
         if (!grid_sync(bar)) return;
         if (*(volatile int *)&bar->active <= 0) return;
     }
@@ -746,6 +787,211 @@ __global__ void k_mixed_matrix(int64_t n, const int32_t *__restrict__ rp,
     }
 }
 
+// Graph scheduler: one warp per chunk, one launch per phase group. X runs
+// the SpMV-type phases (A, R, ZERO) and B the vector update; an iteration is
+// an X launch followed by a B launch.
+template <int RUN>
+__global__ void __launch_bounds__(256, 3)
+k_pcg_step(const SysDev *__restrict__ sys, SysState *st,
+           const int32_t *__restrict__ chunk_sys, int n_chunks, GridBar *bar) {
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= n_chunks) return;
+    dispatch<RUN>(sys, st, bar, chunk_sys, c, threadIdx.x & 31);
+}
+
+
+// Lean SpMV phase for the graph scheduler: one block row per group of
+// LANES lanes, one row in flight per group, few registers so that many
+// warps are resident and hide the gather latency. Block values are read
+// from an entry-major copy (vsoa[e * nnzb + k]) so that the lanes of a
+// group read consecutive addresses for every entry e.
+template <typename T, int BS, bool DIFF>
+__device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
+                             int64_t r1, int lane, double part[4]) {
+    const T beta = (T)vcg(&st->beta);
+    const T zeta = (T)vcg(&st->zeta);
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
+    T *pout = (T *)(pbuf ? S.p0 : S.p1);
+    const T *z = (const T *)S.z;
+    T *q = (T *)S.q;
+    const T *va = (const T *)S.vsoa;
+    const int64_t ld = S.nnzb;
+    const int sub = lane & (LANES - 1), grp = lane / LANES;
+    T pq = 0;
+    for (int64_t base = r0; base < r1; base += RPP) {
+        const int64_t row = base + grp;
+        const bool valid = row < r1;
+        const int64_t rr = valid ? row : r0;
+        T pi[BS], acc[BS];
+#pragma unroll
+        for (int c = 0; c < BS; ++c) {
+            pi[c] = zeta * ldcg(z + rr * BS + c) + beta * ldcg(pin + rr * BS + c);
+            acc[c] = 0;
+        }
+        const int32_t kb = valid ? __ldg(S.rp + rr) : 0;
+        const int32_t k1 = valid ? __ldg(S.rp + rr + 1) : 0;
+        // software pipeline: the next block's index and values are loaded
+        // while the current block's gathers are in flight
+        int32_t k = kb + sub;
+        bool on = k < k1;
+        int32_t kk = on ? k : 0;
+        int64_t j = __ldg(S.ci + kk);
+        T a[BS * BS];
+#pragma unroll
+        for (int e = 0; e < BS * BS; ++e) a[e] = __ldg(va + (int64_t)e * ld + kk);
+        while (on) {
+            T pj[BS];
+#pragma unroll
+            for (int d = 0; d < BS; ++d) {
+                pj[d] = zeta * ldcg(z + j * BS + d) + beta * ldcg(pin + j * BS + d);
+                if (DIFF) pj[d] = (j == rr) ? pi[d] : pj[d] - pi[d];
+            }
+            const int32_t k2 = k + LANES;
+            const bool on2 = k2 < k1;
+            const int32_t kk2 = on2 ? k2 : 0;
+            const int64_t j2 = __ldg(S.ci + kk2);
+            T a2[BS * BS];
+#pragma unroll
+            for (int e = 0; e < BS * BS; ++e) a2[e] = __ldg(va + (int64_t)e * ld + kk2);
+#pragma unroll
+            for (int c = 0; c < BS; ++c)
+#pragma unroll
+                for (int d = 0; d < BS; ++d) acc[c] += a[c * BS + d] * pj[d];
+            j = j2;
+#pragma unroll
+            for (int e = 0; e < BS * BS; ++e) a[e] = a2[e];
+            k = k2;
+            on = on2;
+        }
+#pragma unroll
+        for (int c = 0; c < BS; ++c) acc[c] = group_sum<LANES>(acc[c]);
+        if (valid && sub == 0) {
+#pragma unroll
+            for (int c = 0; c < BS; ++c) {
+                const int64_t i = row * BS + c;
+                pout[i] = pi[c];
+                q[i] = acc[c];
+                pq += pi[c] * acc[c];
+            }
+        }
+    }
+    part[0] += (double)pq;
+}
+
+// Entry-major working-precision copy of block values (AoS -> SoA).
+template <typename TI, typename TO, int B2>
+__global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict__ out) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnzb;
+         k += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int e = 0; e < B2; ++e) out[(int64_t)e * nnzb + k] = (TO)in[k * B2 + e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Graph scheduler kernels: lean, one template instance per precision and
+// block size, so each keeps few registers and high occupancy. Chunk sums go
+// to plain per-chunk slots; k_greduce then sums every system's slots in a
+// fixed order (one block per system) and advances its state. An iteration
+// is k_gx (A, R or ZERO), k_greduce, k_gb (B), k_greduce.
+__host__ __device__ inline int brows(int bs) { return bs == 3 ? 10 : 32; }
+
+template <typename T, int BS>
+__global__ void __launch_bounds__(256, 4)
+k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
+     int n) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= n) return;
+    const int2 e = __ldg(list + wid);
+    const SysDev &S = sys[e.x];
+    const int ph = *(volatile int32_t *)&st[e.x].phase;
+    const int64_t r0 = (int64_t)e.y * S.crows;
+    const int64_t r1 = min(S.n, r0 + S.crows);
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ph == PH_A) {
+        phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
+    } else if (ph == PH_R) {
+        int bad = 0;
+        phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+    } else if (ph == PH_ZERO) {
+        phase_zero<BS>(S, r0, r1, lane);
+    } else {
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
+    if (lane == 0) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) S.partial[(int64_t)e.y * 4 + v] = part[v];
+    }
+}
+
+template <typename T, int BS>
+__global__ void __launch_bounds__(256)
+k_gb(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
+     int n) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= n) return;
+    const int2 e = __ldg(list + wid);
+    const SysDev &S = sys[e.x];
+    if (*(volatile int32_t *)&st[e.x].phase != PH_B) return;
+    const int64_t r0 = (int64_t)e.y * brows(BS);
+    const int64_t r1 = min(S.n, r0 + brows(BS));
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    phase_B<T, BS>(S, &st[e.x], r0, r1, lane, part);
+#pragma unroll
+    for (int v = 0; v < 2; ++v) part[v] = warp_sum(part[v]);
+    if (lane == 0) {
+        S.partialB[(int64_t)e.y * 4 + 0] = part[0];
+        S.partialB[(int64_t)e.y * 4 + 1] = part[1];
+    }
+}
+
+// One block per system: fixed-order sum of its chunk slots, then advance.
+constexpr int RED_THREADS = 1024;
+__global__ void __launch_bounds__(RED_THREADS)
+k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which) {
+    __shared__ double red[4][RED_THREADS / 32];
+    const int s = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const SysDev &S = sys[s];
+    const int ph = *(volatile int32_t *)&st[s].phase;
+    const bool mine = which ? (ph == PH_B) : (ph == PH_A || ph == PH_R || ph == PH_ZERO);
+    if (!mine) return;
+    const int n = which ? S.nchunksB : S.nchunks;
+    const double *P = which ? S.partialB : S.partial;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    // four independent slots per round keep the loads in flight
+    for (int c0 = t; c0 < n; c0 += 4 * RED_THREADS) {
+        double v[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + u * RED_THREADS;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[u][e] = c < n ? __ldcg(P + (int64_t)c * 4 + e) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[e] += v[u][e];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[e] = warp_sum(acc[e]);
+    if (lane == 0)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) red[e][w] = acc[e];
+    __syncthreads();
+    if (w == 0) {
+        double tot[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) tot[e] = warp_sum(lane < RED_THREADS / 32 ? red[e][lane] : 0.0);
+        if (lane == 0) advance(S, &st[s], bar, ph, tot);
+    }
+}
+
+constexpr int GRAPH_ITERS = 16;   // iterations per graph replay
 }  // namespace cfem
 
 using namespace cfem;
@@ -784,6 +1030,8 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     size_t bytes = 0;
     auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
     int max_iter = 1;
+    int64_t n_chunks_b = 0;
+    size_t soa_bytes = 0;
     for (int i = 0; i < n_systems; ++i) {
         const cfem_linsys &L = systems[i];
         CFEM_CHECK(L.bs == 1 || L.bs == 3, CFEM_ERR_INVALID,
@@ -822,18 +1070,29 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.hist_cap = L.d_history ? L.history_cap : 0;
         S.hist = L.d_history;
         for (int c = 0; c < S.nchunks; ++c) chunk_sys.push_back(i);
+        S.nchunksB = (int32_t)((L.n_rows + brows(L.bs) - 1) / brows(L.bs));
+        int32_t nnzb = 0;
+        CFEM_CUDA(cudaMemcpyAsync(&nnzb, L.d_row_ptr + L.n_rows, sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, s));
+        CFEM_CUDA(cudaStreamSynchronize(s));
+        S.nnzb = nnzb;
+        if (L.bs == 3) soa_bytes += align((size_t)nnzb * 9 * (L.mode == CFEM_SOLVE_MIXED ? 4 : 8));
         const size_t ts = (L.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
         const size_t nd = (size_t)L.n_rows * L.bs;
         const size_t nprec = (S.precond == CFEM_PRECOND_BLOCK) ? (size_t)L.n_rows * 9 : nd;
         bytes += 5 * align(nd * ts) + align(nprec * ts) +
                  align(S.nchunks * 4 * sizeof(double)) +
                  align(S.ntiles * 4 * sizeof(double)) +
-                 align(S.ntiles * sizeof(unsigned));
+                 align(S.ntiles * sizeof(unsigned)) +
+                 align(S.nchunksB * 4 * sizeof(double));
+        n_chunks_b += S.nchunksB;
         if (L.max_iter > max_iter) max_iter = L.max_iter;
     }
     const int n_chunks = (int)chunk_sys.size();
     bytes += align(n_systems * sizeof(SysDev)) + align(n_systems * sizeof(SysState)) +
-             align(n_chunks * sizeof(int32_t)) + align(sizeof(GridBar));
+             align(n_chunks * sizeof(int32_t)) + align(sizeof(GridBar)) +
+             align(n_chunks * sizeof(int2)) + align(n_chunks_b * sizeof(int2)) +
+             soa_bytes;
     char *ws = nullptr;
     CFEM_TRY(tmp_alloc(&ws, bytes, s));
     CFEM_CUDA(cudaMemsetAsync(ws, 0, bytes, s));
@@ -853,11 +1112,26 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.partial = (double *)take(S.nchunks * 4 * sizeof(double));
         S.tpartial = (double *)take(S.ntiles * 4 * sizeof(double));
         S.tcnt = (unsigned *)take(S.ntiles * sizeof(unsigned));
+        S.partialB = (double *)take(S.nchunksB * 4 * sizeof(double));
+        if (S.bs == 3) {
+            void *soa = take((size_t)S.nnzb * 9 * ts);
+            if (S.mode == CFEM_SOLVE_MIXED)
+                CFEM_LAUNCH((k_to_soa<float, float, 9>), grid_for(S.nnzb, 256), 256, 0,
+                            s, S.nnzb, S.v32, (float *)soa);
+            else
+                CFEM_LAUNCH((k_to_soa<double, double, 9>), grid_for(S.nnzb, 256), 256, 0,
+                            s, S.nnzb, S.v64, (double *)soa);
+            S.vsoa = soa;
+        } else {
+            S.vsoa = (S.mode == CFEM_SOLVE_MIXED) ? (const void *)S.v32 : (const void *)S.v64;
+        }
     }
     SysDev *d_sys = (SysDev *)take(n_systems * sizeof(SysDev));
     SysState *d_st = (SysState *)take(n_systems * sizeof(SysState));
     int32_t *d_chunks = (int32_t *)take(n_chunks * sizeof(int32_t));
     GridBar *d_bar = (GridBar *)take(sizeof(GridBar));
+    int2 *d_lista = (int2 *)take(n_chunks * sizeof(int2));
+    int2 *d_listb = (int2 *)take(n_chunks_b * sizeof(int2));
     const int h_active = n_systems;
     CFEM_CUDA(cudaMemcpyAsync(d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
@@ -872,21 +1146,108 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     CFEM_CHECK(per_sm > 0, CFEM_ERR_CUDA, "solver kernel cannot be resident");
     int grid = ctx->num_sms * per_sm;
     const int useful = (n_chunks * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
+    // One resident wave holds every chunk: the persistent kernel pays a grid
+    // barrier per phase and no launches. Otherwise the graph scheduler keeps
+    // the SMs fed with one warp per chunk per launch.
+    bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
+                      (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
     if (grid > useful) grid = useful < 1 ? 1 : useful;
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     int max_steps = 3 * max_iter + 16;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    CFEM_CUDA(cudaEventCreate(&ev0));
-    CFEM_CUDA(cudaEventCreate(&ev1));
-    CFEM_CUDA(cudaEventRecord(ev0, s));
-    CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, s,
+    cudaStream_t w = ctx->work;
+    // The work stream runs after everything queued so far on s.
+    CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
+    CFEM_CUDA(cudaStreamWaitEvent(w, ctx->ev[0], 0));
+    CFEM_CUDA(cudaEventRecord(ctx->ev[2], w));
+    CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, w,
                 d_sys, d_st, d_chunks, n_chunks, d_bar);
-    void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
-                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
-    CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
-                                          dim3(SOLVE_THREADS), args, 0, s));
-    CFEM_CUDA(cudaEventRecord(ev1, s));
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (persistent) {
+        void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
+                        (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
+        CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
+                                              dim3(SOLVE_THREADS), args, 0, w));
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    } else {
+        // Work lists per (precision, block size): {system, chunk} pairs.
+        std::vector<int2> la[4], lb[4];
+        for (int i = 0; i < n_systems; ++i) {
+            const int t = (hs[i].mode == CFEM_SOLVE_MIXED ? 2 : 0) + (hs[i].bs == 3 ? 1 : 0);
+            for (int c = 0; c < hs[i].nchunks; ++c) la[t].push_back(make_int2(i, c));
+            for (int c = 0; c < hs[i].nchunksB; ++c) lb[t].push_back(make_int2(i, c));
+        }
+        int2 *pa[4], *pb[4];
+        size_t oa = 0, ob = 0;
+        for (int t = 0; t < 4; ++t) {
+            pa[t] = d_lista + oa;
+            pb[t] = d_listb + ob;
+            if (!la[t].empty())
+                CFEM_CUDA(cudaMemcpyAsync(pa[t], la[t].data(), la[t].size() * sizeof(int2),
+                                          cudaMemcpyHostToDevice, s));
+            if (!lb[t].empty())
+                CFEM_CUDA(cudaMemcpyAsync(pb[t], lb[t].data(), lb[t].size() * sizeof(int2),
+                                          cudaMemcpyHostToDevice, s));
+            oa += la[t].size();
+            ob += lb[t].size();
+        }
+        CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
+        CFEM_CUDA(cudaStreamWaitEvent(w, ctx->ev[0], 0));
+        int per_iter = 2;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < GRAPH_ITERS; ++it) {
+            for (int t = 0; t < 4; ++t) {
+                const int n = (int)la[t].size();
+                if (!n) continue;
+                const unsigned g = grid_for((int64_t)n * 32, 256);
+                if (t == 0) k_gx<double, 1><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 1) k_gx<double, 3><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 2) k_gx<float, 1><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 3) k_gx<float, 3><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (it == 0) ++per_iter;
+            }
+            k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 0);
+            for (int t = 0; t < 4; ++t) {
+                const int n = (int)lb[t].size();
+                if (!n) continue;
+                const unsigned g = grid_for((int64_t)n * 32, 256);
+                if (t == 0) k_gb<double, 1><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 1) k_gb<double, 3><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 2) k_gb<float, 1><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 3) k_gb<float, 3><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (it == 0) ++per_iter;
+            }
+            k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 1);
+        }
+        cudaError_t ce = cudaStreamEndCapture(w, &graph);
+        CFEM_CUDA(ce);
+        CFEM_CUDA(cudaGetLastError());
+        CFEM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        // Each iteration takes one X+B pair, each true-residual replacement
+        // one more; a replay holds GRAPH_ITERS pairs. Poll the number of
+        // active systems one replay behind so the queue never drains.
+        const int max_replays = (2 * max_iter + 32) / GRAPH_ITERS + 2;
+        volatile int *flags = ctx->h_flags;
+        flags[0] = flags[1] = 1;
+        int rep = 0;
+        for (; rep < max_replays; ++rep) {
+            CFEM_CUDA(cudaGraphLaunch(exec, w));
+            g_launches.fetch_add((int64_t)per_iter * GRAPH_ITERS, std::memory_order_relaxed);
+            CFEM_CUDA(cudaMemcpyAsync((void *)&ctx->h_flags[rep & 1], &d_bar->active,
+                                      sizeof(int), cudaMemcpyDeviceToHost, w));
+            CFEM_CUDA(cudaEventRecord(ctx->ev[rep & 1], w));
+            if (rep >= 1) {
+                CFEM_CUDA(cudaEventSynchronize(ctx->ev[(rep - 1) & 1]));
+                if (flags[(rep - 1) & 1] <= 0) break;
+            }
+        }
+        CFEM_CUDA(cudaStreamSynchronize(w));
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+    }
+    CFEM_CUDA(cudaEventRecord(ctx->ev[3], w));
+    CFEM_CUDA(cudaEventRecord(ctx->ev[0], w));
+    CFEM_CUDA(cudaStreamWaitEvent(s, ctx->ev[0], 0));
     std::vector<SysState> hst(n_systems);
     int h_err = 0;
     CFEM_CUDA(cudaMemcpyAsync(hst.data(), d_st, n_systems * sizeof(SysState),
@@ -896,9 +1257,7 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     tmp_free(ws, s);
     CFEM_CUDA(cudaStreamSynchronize(s));
     float kms = 0.0f;
-    CFEM_CUDA(cudaEventElapsedTime(&kms, ev0, ev1));
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
+    CFEM_CUDA(cudaEventElapsedTime(&kms, ctx->ev[2], ctx->ev[3]));
     for (int i = 0; i < n_systems; ++i) {
         stats[i].status = hst[i].status;
         if (hst[i].status == CFEM_OK && hst[i].phase != PH_DONE)

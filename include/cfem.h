@@ -130,6 +130,16 @@ CFEM_API int cfem_version(void);
 /* Creates a context on `device` (must be compute capability 10.x). */
 CFEM_API int cfem_ctx_create(int device, cfem_ctx **out);
 CFEM_API int cfem_ctx_destroy(cfem_ctx *ctx);
+/* How cfem_pcg_solve runs its iterations:
+ * PERSISTENT - one cooperative launch, grid barrier between phases (lowest
+ *              latency when the whole batch fits in one wave of warps);
+ * GRAPH      - two kernels per iteration (SpMV phase, update phase) with a
+ *              warp per row chunk, replayed from a CUDA graph of 16
+ *              iterations; the host polls convergence once per replay;
+ * AUTO       - PERSISTENT when all row chunks fit in one resident wave,
+ *              else GRAPH (default). */
+enum { CFEM_SCHED_AUTO = 0, CFEM_SCHED_PERSISTENT = 1, CFEM_SCHED_GRAPH = 2 };
+CFEM_API int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler);
 /* Number of kernels this library launched through `ctx` so far. */
 CFEM_API int64_t cfem_ctx_launch_count(const cfem_ctx *ctx);
 
