@@ -217,9 +217,11 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
     p->n_nodes = n_nodes;
     p->n_elems = n_elems;
     p->npe = npe;
-    CFEM_CUDA(cudaMalloc(&p->row_ptr, (n_nodes + 1) * sizeof(int32_t)));
-    CFEM_CUDA(cudaMalloc(&p->diag, n_nodes * sizeof(int32_t)));
-    CFEM_CUDA(cudaMalloc(&p->contrib, (total > 0 ? total : 1) * sizeof(int32_t)));
+    // pattern arrays come from the stream-ordered pool: building and
+    // dropping patterns does not synchronise the device
+    CFEM_CUDA(cudaMallocAsync(&p->row_ptr, (n_nodes + 1) * sizeof(int32_t), s));
+    CFEM_CUDA(cudaMallocAsync(&p->diag, n_nodes * sizeof(int32_t), s));
+    CFEM_CUDA(cudaMallocAsync(&p->contrib, (total > 0 ? total : 1) * sizeof(int32_t), s));
 
     uint64_t *keys = nullptr, *keys_sorted = nullptr;
     int32_t *ids = nullptr, *head = nullptr, *pos = nullptr, *rowk = nullptr;
@@ -284,8 +286,8 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
                         "[0, %lld)", (long long)n_nodes);
         }
         nnz = (int64_t)last_pos + last_head;
-        CFEM_CUDA(cudaMalloc(&p->col, nnz * sizeof(int32_t)));
-        CFEM_CUDA(cudaMalloc(&p->seg, (nnz + 1) * sizeof(int32_t)));
+        CFEM_CUDA(cudaMallocAsync(&p->col, (nnz > 0 ? nnz : 1) * sizeof(int32_t), s));
+        CFEM_CUDA(cudaMallocAsync(&p->seg, (nnz + 1) * sizeof(int32_t), s));
         CFEM_TRY(tmp_alloc(&rowk, nnz, s));
         CFEM_LAUNCH(k_scatter_heads, g, 256, 0, s, keys_sorted, head, pos,
                     total, n_nodes, p->col, rowk, p->seg);
@@ -297,8 +299,8 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
         tmp_free(rowk, s);
         tmp_free(d_bad, s);
     } else {
-        CFEM_CUDA(cudaMalloc(&p->col, sizeof(int32_t)));
-        CFEM_CUDA(cudaMalloc(&p->seg, sizeof(int32_t)));
+        CFEM_CUDA(cudaMallocAsync(&p->col, sizeof(int32_t), s));
+        CFEM_CUDA(cudaMallocAsync(&p->seg, sizeof(int32_t), s));
         CFEM_CUDA(cudaMemsetAsync(p->row_ptr, 0, (n_nodes + 1) * sizeof(int32_t), s));
         CFEM_CUDA(cudaMemsetAsync(p->seg, 0, sizeof(int32_t), s));
     }
@@ -314,11 +316,13 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
 int cfem_pattern_destroy(cfem_pattern *p) {
     if (!p) return CFEM_OK;
     cudaSetDevice(p->device);
-    cudaFree(p->row_ptr);
-    cudaFree(p->col);
-    cudaFree(p->diag);
-    cudaFree(p->seg);
-    cudaFree(p->contrib);
+    // ordered after all work queued on the legacy stream (which waits for
+    // the blocking streams the library's callers use)
+    cudaFreeAsync(p->row_ptr, 0);
+    cudaFreeAsync(p->col, 0);
+    cudaFreeAsync(p->diag, 0);
+    cudaFreeAsync(p->seg, 0);
+    cudaFreeAsync(p->contrib, 0);
     delete p;
     return CFEM_OK;
 }

@@ -897,57 +897,75 @@ __global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict
 // is k_gx (A, R or ZERO), k_greduce, k_gb (B), k_greduce.
 __host__ __device__ inline int brows(int bs) { return bs == 3 ? 10 : 32; }
 
-template <typename T, int BS>
-__global__ void __launch_bounds__(256, 4)
-k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
-     int n) {
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= n) return;
-    const int2 e = __ldg(list + wid);
-    const SysDev &S = sys[e.x];
-    const int ph = *(volatile int32_t *)&st[e.x].phase;
-    const int64_t r0 = (int64_t)e.y * S.crows;
-    const int64_t r1 = min(S.n, r0 + S.crows);
-    double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (ph == PH_A) {
-        phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
-    } else if (ph == PH_R) {
-        int bad = 0;
-        phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
-    } else if (ph == PH_ZERO) {
-        phase_zero<BS>(S, r0, r1, lane);
-    } else {
-        return;
-    }
+// Work lists hold each system's chunks padded to whole groups of GROUP
+// entries ({-1, -1} = padding), so every block of GROUP warps works on one
+// group of one system and writes one group partial, summed in warp order.
+constexpr int GROUP = 8;
+
+__device__ __forceinline__ void group_store(double part[4], int nv, double *dst,
+                                            int lane, int w) {
+    __shared__ double red[GROUP][4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
-    if (lane == 0) {
+    if (lane == 0)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) S.partial[(int64_t)e.y * 4 + v] = part[v];
+        for (int v = 0; v < 4; ++v) red[w][v] = part[v];
+    __syncthreads();
+    if (threadIdx.x == 0 && dst) {
+        for (int v = 0; v < nv; ++v) {
+            double t = 0.0;
+#pragma unroll
+            for (int g = 0; g < GROUP; ++g) t += red[g][v];
+            dst[v] = t;
+        }
     }
 }
 
 template <typename T, int BS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(32 * GROUP, 4)
+k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
+     int n) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * S.crows;
+        const int64_t r1 = min(S.n, r0 + S.crows);
+        if (ph == PH_A) {
+            phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
+        } else if (ph == PH_R) {
+            int bad = 0;
+            phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+        } else {
+            phase_zero<BS>(S, r0, r1, lane);
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
+template <typename T, int BS>
+__global__ void __launch_bounds__(32 * GROUP)
 k_gb(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
      int n) {
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= n) return;
-    const int2 e = __ldg(list + wid);
-    const SysDev &S = sys[e.x];
-    if (*(volatile int32_t *)&st[e.x].phase != PH_B) return;
-    const int64_t r0 = (int64_t)e.y * brows(BS);
-    const int64_t r1 = min(S.n, r0 + brows(BS));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    const SysDev &S = sys[lead.x];
+    if (*(volatile int32_t *)&st[lead.x].phase != PH_B) return;
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    phase_B<T, BS>(S, &st[e.x], r0, r1, lane, part);
-#pragma unroll
-    for (int v = 0; v < 2; ++v) part[v] = warp_sum(part[v]);
-    if (lane == 0) {
-        S.partialB[(int64_t)e.y * 4 + 0] = part[0];
-        S.partialB[(int64_t)e.y * 4 + 1] = part[1];
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * brows(BS);
+        const int64_t r1 = min(S.n, r0 + brows(BS));
+        phase_B<T, BS>(S, &st[e.x], r0, r1, lane, part);
     }
+    group_store(part, 2, S.partialB + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
 // One block per system: fixed-order sum of its chunk slots, then advance.
@@ -960,7 +978,7 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     const int ph = *(volatile int32_t *)&st[s].phase;
     const bool mine = which ? (ph == PH_B) : (ph == PH_A || ph == PH_R || ph == PH_ZERO);
     if (!mine) return;
-    const int n = which ? S.nchunksB : S.nchunks;
+    const int n = which ? (S.nchunksB + GROUP - 1) / GROUP : (S.nchunks + GROUP - 1) / GROUP;
     const double *P = which ? S.partialB : S.partial;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     // four independent slots per round keep the loads in flight
@@ -1091,8 +1109,8 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     const int n_chunks = (int)chunk_sys.size();
     bytes += align(n_systems * sizeof(SysDev)) + align(n_systems * sizeof(SysState)) +
              align(n_chunks * sizeof(int32_t)) + align(sizeof(GridBar)) +
-             align(n_chunks * sizeof(int2)) + align(n_chunks_b * sizeof(int2)) +
-             soa_bytes;
+             align((n_chunks + (size_t)GROUP * n_systems) * sizeof(int2)) +
+             align((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2)) + soa_bytes;
     char *ws = nullptr;
     CFEM_TRY(tmp_alloc(&ws, bytes, s));
     CFEM_CUDA(cudaMemsetAsync(ws, 0, bytes, s));
@@ -1130,8 +1148,8 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     SysState *d_st = (SysState *)take(n_systems * sizeof(SysState));
     int32_t *d_chunks = (int32_t *)take(n_chunks * sizeof(int32_t));
     GridBar *d_bar = (GridBar *)take(sizeof(GridBar));
-    int2 *d_lista = (int2 *)take(n_chunks * sizeof(int2));
-    int2 *d_listb = (int2 *)take(n_chunks_b * sizeof(int2));
+    int2 *d_lista = (int2 *)take((n_chunks + (size_t)GROUP * n_systems) * sizeof(int2));
+    int2 *d_listb = (int2 *)take((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2));
     const int h_active = n_systems;
     CFEM_CUDA(cudaMemcpyAsync(d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
@@ -1173,7 +1191,9 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         for (int i = 0; i < n_systems; ++i) {
             const int t = (hs[i].mode == CFEM_SOLVE_MIXED ? 2 : 0) + (hs[i].bs == 3 ? 1 : 0);
             for (int c = 0; c < hs[i].nchunks; ++c) la[t].push_back(make_int2(i, c));
+            while (la[t].size() % GROUP) la[t].push_back(make_int2(-1, -1));
             for (int c = 0; c < hs[i].nchunksB; ++c) lb[t].push_back(make_int2(i, c));
+            while (lb[t].size() % GROUP) lb[t].push_back(make_int2(-1, -1));
         }
         int2 *pa[4], *pb[4];
         size_t oa = 0, ob = 0;
@@ -1199,22 +1219,22 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
             for (int t = 0; t < 4; ++t) {
                 const int n = (int)la[t].size();
                 if (!n) continue;
-                const unsigned g = grid_for((int64_t)n * 32, 256);
-                if (t == 0) k_gx<double, 1><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 1) k_gx<double, 3><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 2) k_gx<float, 1><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 3) k_gx<float, 3><<<g, 256, 0, w>>>(d_sys, d_st, pa[t], n);
+                const unsigned g = (unsigned)(n / GROUP);
+                if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
                 if (it == 0) ++per_iter;
             }
             k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 0);
             for (int t = 0; t < 4; ++t) {
                 const int n = (int)lb[t].size();
                 if (!n) continue;
-                const unsigned g = grid_for((int64_t)n * 32, 256);
-                if (t == 0) k_gb<double, 1><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 1) k_gb<double, 3><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 2) k_gb<float, 1><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 3) k_gb<float, 3><<<g, 256, 0, w>>>(d_sys, d_st, pb[t], n);
+                const unsigned g = (unsigned)(n / GROUP);
+                if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
                 if (it == 0) ++per_iter;
             }
             k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 1);
