@@ -310,12 +310,168 @@ def cpu_baseline(shape=CPU_SAMPLE):
                       f"({free} free DOFs), one solve, {dt:.1f} s"}
 
 
+# --------------------------------------------------------------------- C3
+C3_MESHES = 512
+C3_SEED = 0
+
+
+def c3_draw(count=C3_MESHES, seed=C3_SEED):
+    """Seeded batch: n ~ U{4..24}, lognormal(0, 1) conductivity per hex cell."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(4, 25, size=count)
+    ks = [rng.lognormal(0.0, 1.0, int(n) ** 3) for n in ns]
+    return ns, ks
+
+
+def c3_cell_fn(n, kc):
+    """The per-cell conductivity as the reference's callable API sees it:
+    k(x, y, z) = K[i, j, k] of the hex cell containing the point (Keast
+    points are interior, so the lookup is exact)."""
+    kc3 = kc.reshape(n, n, n)          # cell order k, j, i (box_mesh)
+
+    def k(x, y, z):
+        i = np.minimum((np.asarray(x) * n).astype(int), n - 1)
+        j = np.minimum((np.asarray(y) * n).astype(int), n - 1)
+        kk = np.minimum((np.asarray(z) * n).astype(int), n - 1)
+        return kc3[kk, j, i]
+    return k
+
+
+def c3_problems(ns, ks):
+    from cloudfem_b200.batch import HeatProblem
+    from cloudfem_b200.mesh import box_mesh_tet10
+    meshes = {int(n): box_mesh_tet10(int(n), int(n), int(n)) for n in set(ns)}
+    bc = {s: 0.0 for s in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")}
+    # 6 Kuhn tets per cell, cells in k, j, i order: element e is in cell e // 6
+    return [HeatProblem(meshes[int(n)], k=np.repeat(kc, 6), f=1.0, bc=bc)
+            for n, kc in zip(ns, ks)]
+
+
+def run_c3(args, rank, world, local_rank):
+    import torch
+
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.batch import BatchSolver, solve_batch
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rt = N.runtime(local_rank)
+    ns, ks = c3_draw()
+    problems = c3_problems(ns, ks)
+    solver = BatchSolver(local_rank)
+    batch = solver.prepare(problems)
+    free = batch.free_dofs
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    rtol = 1e-10
+
+    def step(precision, tol=rtol):
+        batch.assemble()
+        return batch.solve(precision, rtol=tol)
+
+    # FP64 answer of the same batch (accuracy gate, tighter tolerance)
+    step("fp64", 1e-12)
+    x64 = [it["x"].clone() for it in batch.items]
+    # plain FP64 path: one problem per assembly+solve call, on a prefix
+    plain_n = 32
+    sub = problems[:plain_n]
+    solve_batch(sub[:2], precision="fp64", rtol=1e-10, solver=solver)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for pb in sub:
+        solve_batch([pb], precision="fp64", rtol=1e-10, solver=solver)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    plain_free = sum(batch.items[i]["free"] for i in range(plain_n))
+
+    for _ in range(args.warmup):
+        step(args.precision)
+    torch.cuda.synchronize()
+    times, launches0 = [], rt.launches()
+    with Clocks(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = step(args.precision)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = rt.launches() - launches0
+    err = max(float(torch.linalg.norm(it["x"] - x) / torch.linalg.norm(x))
+              for it, x in zip(batch.items, x64))
+    iters = [r.iterations for r in res]
+
+    # end to end: host coefficient arrays in, solutions out (meshes and
+    # their patterns stay resident in the solver, as in a serving process)
+    e2e = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve_batch(problems, precision=args.precision, rtol=rtol, solver=solver)
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ms = float(np.sum(times))
+    e2e_ms = float(np.sum(e2e))
+    if rank != 0:
+        return None
+    h2d = sum(pb.k.nbytes for pb in problems)
+    d2h = sum(it["dm"].n_nodes * 8 for it in batch.items)
+    out = {
+        "metric": METRIC,
+        "value": world * free * args.steps / (ms * 1e-3),
+        "unit": "DOF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 PCG + f64 residual/update" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded unit-cube Tet10 meshes, lognormal k per cell)",
+        "config": {
+            "workload": "batched_tet10_heat_512_meshes_n4to24",
+            "meshes": len(problems), "free_dofs": int(free),
+            "precision": args.precision, "rtol": rtol,
+            "iterations_max": int(max(iters)), "iterations_mean": float(np.mean(iters)),
+            "rel_err_vs_fp64_max": err,
+            "plain_fp64_per_mesh": {"meshes": plain_n,
+                                    "dof_per_s": plain_free / plain_s},
+            "l2": "256 MiB buffer written between timed steps",
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {"value": world * free * args.steps / (e2e_ms * 1e-3), "unit": "DOF/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "meshes and patterns resident; coefficients and solutions cross"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_c3(ns, ks)
+    return out
+
+
+def cpu_baseline_c3(ns, ks, cap_n=7, count=12):
+    """Oracle (NumPy + SuperLU) on the first `count` draws with n <= cap_n."""
+    from oracle import cfem_oracle as O
+    bc = {s: 0.0 for s in O.FACE_NAMES}
+    picked = [(int(n), kc) for n, kc in zip(ns, ks) if n <= cap_n][:count]
+    free, t0 = 0, time.perf_counter()
+    for n, kc in picked:
+        m = O.box_mesh_tet10(n, n, n)
+        O.solve_tet10_poisson(m, k=c3_cell_fn(n, kc), f=1.0, bc=bc)
+        free += (2 * n - 1) ** 3
+    dt = time.perf_counter() - t0
+    return {"value": free / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"{len(picked)} of the seeded meshes with n <= {cap_n} "
+                      f"({free} free DOFs), one solve each"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
     per = []
+    if args.workload == "c3":
+        draw = c3_draw()
     for i in range(args.warmup + args.steps):
-        c = cpu_baseline()
+        c = cpu_baseline_c3(*draw) if args.workload == "c3" else cpu_baseline()
         if i >= args.warmup:
             per.append(c)
     value = float(np.mean([c["value"] for c in per]))
@@ -328,7 +484,9 @@ def run_reference(args, rank):
         "ms_per_step": float(np.mean([c["seconds"] for c in per])) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "tet10_elasticity_beam_80x10x10",
+        "config": {"workload": ("batched_tet10_heat_512_meshes_n4to24"
+                                if args.workload == "c3" else
+                                "tet10_elasticity_beam_80x10x10"),
                    "sample": c["sample"]},
         "cpu_baseline": c,
         "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0,
@@ -342,9 +500,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default=None, choices=["mixed", "fp64"],
+                    help="default: fp64 for c2 (faster there), mixed for c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                    help="c2: Tet10 elasticity beam (default); c3: 512 "
+                         "batched Tet10 heat meshes")
     args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "c3" else "fp64"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -359,7 +523,10 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl",
                                     timeout=datetime.timedelta(seconds=300))
-        out = run_ours(args, rank, world, local_rank)
+        if args.workload == "c3":
+            out = run_c3(args, rank, world, local_rank)
+        else:
+            out = run_ours(args, rank, world, local_rank)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()

@@ -51,6 +51,12 @@ class Coef(ctypes.Structure):
                 ("pad_", _i32)]
 
 
+class AssemblyJob(ctypes.Structure):
+    _fields_ = [("pattern", _vp), ("d_nodes", _vp), ("d_elems", _vp),
+                ("coef", Coef), ("load", Coef), ("d_vals", _vp),
+                ("d_rhs", _vp)]
+
+
 class LinSys(ctypes.Structure):
     _fields_ = [("n_rows", _i64), ("bs", _i32), ("precond", _i32),
                 ("d_row_ptr", _vp), ("d_col", _vp), ("d_vals64", _vp),
@@ -86,6 +92,8 @@ SIGNATURES = [
     ("cfem_assemble", ctypes.c_int,
      [_vp, _vp, _i32, _vp, _vp, ctypes.POINTER(Coef), ctypes.POINTER(Coef),
       _vp, _vp, _i32, _vp]),
+    ("cfem_assemble_batch", ctypes.c_int,
+     [_vp, _i32, ctypes.POINTER(AssemblyJob), _i32, _vp]),
     ("cfem_assemble_elastic", ctypes.c_int,
      [_vp, _vp, _i32, _vp, _vp, _f64, _f64, ctypes.POINTER(Coef),
       ctypes.POINTER(Coef), _f64, _f64, _vp, _vp, _i32, _vp]),

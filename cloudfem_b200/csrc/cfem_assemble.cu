@@ -17,6 +17,7 @@
 
 #include <math.h>
 #include <mutex>
+#include <vector>
 
 namespace cfem {
 
@@ -186,12 +187,11 @@ __device__ __forceinline__ void p1_grads(const Geo &g, double G[4][3]) {
 // OP = CFEM_OP_P1_STIFF: Ke = (k V) G G^T, fe = f V / 4 (tet_poisson.py:51-66)
 // OP = CFEM_OP_P1_MASS : Ke = (rho V) (1 + d_ij)/20  (tet_heat.py:81-94)
 template <int OP>
-__global__ void __launch_bounds__(128)
-k_p1_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
-            int64_t M, Coef coef, Coef load, double *__restrict__ ke,
-            double *__restrict__ fe) {
-    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= M) return;
+__device__ __forceinline__ void p1_scalar_elem(const double *__restrict__ nodes,
+                                               const int32_t *__restrict__ elems,
+                                               int64_t e, const Coef &coef,
+                                               const Coef &load, double *ke,
+                                               double *fe) {
     int4 el = __ldg(reinterpret_cast<const int4 *>(elems) + e);
     Geo g;
     tet_geo(nodes, el.x, el.y, el.z, el.w, g);
@@ -208,8 +208,7 @@ k_p1_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
                                        G[i][2] * G[j][2]);
         if (fe) {
             double f = coef_at(load, e, 0) * g.vol / 4.0;
-            double4 f4 = make_double4(f, f, f, f);
-            reinterpret_cast<double4 *>(fe)[e] = f4;
+            *reinterpret_cast<double4 *>(fe) = make_double4(f, f, f, f);
         }
     } else {
         double rv = coef_at(coef, e, 0) * g.vol;
@@ -219,11 +218,21 @@ k_p1_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
 #pragma unroll
             for (int j = 0; j < 4; ++j) out[i * 4 + j] = (i == j) ? d : o;
     }
-    double4 *dst = reinterpret_cast<double4 *>(ke + e * 16);
+    double4 *dst = reinterpret_cast<double4 *>(ke);
 #pragma unroll
     for (int v = 0; v < 4; ++v)
         dst[v] = make_double4(out[4 * v], out[4 * v + 1], out[4 * v + 2],
                               out[4 * v + 3]);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(128)
+k_p1_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
+            int64_t M, Coef coef, Coef load, double *__restrict__ ke,
+            double *__restrict__ fe) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= M) return;
+    p1_scalar_elem<OP>(nodes, elems, e, coef, load, ke + e * 16, fe ? fe + e * 4 : nullptr);
 }
 
 // ------------------------------------------------------------- P1 elastic
@@ -303,18 +312,16 @@ __device__ __forceinline__ void t10_stage_grads(const double *__restrict__ nodes
 //                        (tet10.py:150-161)
 // OP = CFEM_OP_T10_MASS : Ke = (rho V) MASS_REF (tet10.py:241-246)
 template <int OP>
-__global__ void __launch_bounds__(32 * T10_WARPS)
-k_t10_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
-             int64_t M, Coef coef, Coef load, double *__restrict__ ke,
-             double *__restrict__ fe) {
-    __shared__ double sG[T10_WARPS][5][10][3];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t e = (int64_t)blockIdx.x * T10_WARPS + w;
-    if (e >= M) return;
+__device__ __forceinline__ void t10_scalar_elem(const double *__restrict__ nodes,
+                                                const int32_t *__restrict__ elems,
+                                                int64_t e, const Coef &coef,
+                                                const Coef &load, double *ke,
+                                                double *fe, double (*sG)[10][3],
+                                                int lane) {
     const int32_t *el = elems + e * 10;
     if (OP == CFEM_OP_T10_STIFF) {
         double vol;
-        t10_stage_grads(nodes, el, sG[w], lane, vol);
+        t10_stage_grads(nodes, el, sG, lane, vol);
         double wk[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) wk[q] = c_wq[q] * coef_at(coef, e, q);
@@ -323,24 +330,37 @@ k_t10_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems
             double s = 0.0;
 #pragma unroll
             for (int q = 0; q < 5; ++q)
-                s += wk[q] * (sG[w][q][a][0] * sG[w][q][b][0] +
-                              sG[w][q][a][1] * sG[w][q][b][1] +
-                              sG[w][q][a][2] * sG[w][q][b][2]);
-            ke[e * 100 + t] = vol * s;
+                s += wk[q] * (sG[q][a][0] * sG[q][b][0] + sG[q][a][1] * sG[q][b][1] +
+                              sG[q][a][2] * sG[q][b][2]);
+            ke[t] = vol * s;
         }
         if (fe && lane < 10) {
             double s = 0.0;
 #pragma unroll
             for (int q = 0; q < 5; ++q) s += c_N[q][lane] * (c_wq[q] * coef_at(load, e, q));
-            fe[e * 10 + lane] = vol * s;
+            fe[lane] = vol * s;
         }
+        __syncwarp();
     } else {
         Geo g;
         tet_geo(nodes, __ldg(el + 0), __ldg(el + 1), __ldg(el + 2), __ldg(el + 3), g);
         double rv = coef_at(coef, e, 0) * g.vol;
         for (int t = lane; t < 100; t += 32)
-            ke[e * 100 + t] = rv * c_mass[t / 10][t - (t / 10) * 10];
+            ke[t] = rv * c_mass[t / 10][t - (t / 10) * 10];
     }
+}
+
+template <int OP>
+__global__ void __launch_bounds__(32 * T10_WARPS)
+k_t10_scalar(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
+             int64_t M, Coef coef, Coef load, double *__restrict__ ke,
+             double *__restrict__ fe) {
+    __shared__ double sG[T10_WARPS][5][10][3];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t e = (int64_t)blockIdx.x * T10_WARPS + w;
+    if (e >= M) return;
+    t10_scalar_elem<OP>(nodes, elems, e, coef, load, ke + e * 100,
+                        fe ? fe + e * 10 : nullptr, sG[w], lane);
 }
 
 // Tet10 elasticity: block (a,b) = V sum_q w_q (lam g_a g_b^T + mu g_b g_a^T
@@ -466,6 +486,92 @@ __global__ void k_reduce_rhs(const int32_t *__restrict__ diag,
     }
 }
 
+
+// ------------------------------------------------------------- batches
+// Many independent meshes in one launch per pass: a job table gives each
+// mesh's arrays and its offsets in the concatenated element / CSR / node
+// ranges; a thread (P1), warp (Tet10) or CSR entry finds its job by binary
+// search over the offsets.
+struct AsmJob {
+    const double *nodes;
+    const int32_t *elems;
+    const int32_t *seg, *contrib, *diag;
+    double *vals, *rhs;
+    Coef coef, load;
+    int64_t e0, k0, a0;          // element, CSR entry and node offsets
+    int64_t m, nnz, n_nodes;
+};
+
+__device__ __forceinline__ int find_job(const AsmJob *jobs, int nj, int64_t g, int which) {
+    int lo = 0, hi = nj - 1;     // last job with offset <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t off = which == 0 ? jobs[mid].e0 : (which == 1 ? jobs[mid].k0 : jobs[mid].a0);
+        if (off <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(128)
+k_p1_scalar_batch(const AsmJob *__restrict__ jobs, int nj, int64_t M,
+                  double *__restrict__ ke, double *__restrict__ fe) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= M) return;
+    const AsmJob &J = jobs[find_job(jobs, nj, g, 0)];
+    p1_scalar_elem<OP>(J.nodes, J.elems, g - J.e0, J.coef, J.load, ke + g * 16,
+                       fe ? fe + g * 4 : nullptr);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(32 * T10_WARPS)
+k_t10_scalar_batch(const AsmJob *__restrict__ jobs, int nj, int64_t M,
+                   double *__restrict__ ke, double *__restrict__ fe) {
+    __shared__ double sG[T10_WARPS][5][10][3];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t g = (int64_t)blockIdx.x * T10_WARPS + w;
+    if (g >= M) return;
+    const AsmJob &J = jobs[find_job(jobs, nj, g, 0)];
+    t10_scalar_elem<OP>(J.nodes, J.elems, g - J.e0, J.coef, J.load, ke + g * 100,
+                        fe ? fe + g * 10 : nullptr, sG[w], lane);
+}
+
+__global__ void k_reduce_vals_batch(const AsmJob *__restrict__ jobs, int nj,
+                                    int64_t K, int npe, const double *__restrict__ ke) {
+    const int64_t per = (int64_t)npe * npe;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < K;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const AsmJob &J = jobs[find_job(jobs, nj, g, 1)];
+        const int64_t k = g - J.k0;
+        const double *kj = ke + J.e0 * per;
+        double s = 0.0;
+        for (int32_t t = J.seg[k]; t < J.seg[k + 1]; ++t) s += __ldg(kj + __ldg(J.contrib + t));
+        J.vals[k] = s;
+    }
+}
+
+__global__ void k_reduce_rhs_batch(const AsmJob *__restrict__ jobs, int nj,
+                                   int64_t A, int npe, const double *__restrict__ fe) {
+    const int per = npe * npe;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < A;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const AsmJob &J = jobs[find_job(jobs, nj, g, 2)];
+        const int64_t a = g - J.a0;
+        const double *fj = fe + J.e0 * npe;
+        double s = 0.0;
+        const int32_t k = J.diag[a];
+        if (k >= 0) {
+            for (int32_t t = J.seg[k]; t < J.seg[k + 1]; ++t) {
+                const int32_t id = J.contrib[t];
+                const int32_t ee = id / per, r = id - ee * per;
+                const int32_t i = r / npe, jj = r - (r / npe) * npe;
+                if (i == jj) s += fj[(int64_t)ee * npe + i];
+            }
+        }
+        J.rhs[a] = s;
+    }
+}
+
 static int check_coef(const cfem_coef *c, bool allow_qp, const char *what) {
     if (!c) return CFEM_OK;
     CFEM_CHECK(c->mode >= CFEM_COEF_CONST && c->mode <= CFEM_COEF_NODAL,
@@ -571,6 +677,112 @@ int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
     tmp_free(ke, s);
     tmp_free(fe, s);
     return st;
+    CFEM_API_END
+}
+
+
+int cfem_assemble_batch(cfem_ctx *ctx, int32_t op, const cfem_assembly_job *jobs,
+                        int32_t n_jobs, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && jobs && n_jobs > 0, CFEM_ERR_INVALID,
+               "cfem_assemble_batch: bad args");
+    const bool p1 = (op == CFEM_OP_P1_STIFF || op == CFEM_OP_P1_MASS);
+    const bool t10 = (op == CFEM_OP_T10_STIFF || op == CFEM_OP_T10_MASS);
+    CFEM_CHECK(p1 || t10, CFEM_ERR_INVALID, "cfem_assemble_batch: scalar operators only");
+    const int npe = p1 ? 4 : 10;
+    const bool stiff = (op == CFEM_OP_P1_STIFF || op == CFEM_OP_T10_STIFF);
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t per = (int64_t)npe * npe;
+    // Staging is bounded: jobs are processed in groups of at most ~256 M
+    // element-matrix entries (2 GiB).
+    const int64_t stage_cap = (int64_t)256 << 20;
+    int i0 = 0;
+    while (i0 < n_jobs) {
+        std::vector<AsmJob> hj;
+        int64_t M = 0, K = 0, A = 0;
+        int i1 = i0;
+        bool rhs = false;
+        while (i1 < n_jobs) {
+            const cfem_assembly_job &J = jobs[i1];
+            CFEM_CHECK(J.pattern && J.d_nodes && J.d_elems && J.d_vals, CFEM_ERR_INVALID,
+                       "job %d: missing arrays", i1);
+            CFEM_CHECK(J.pattern->npe == npe, CFEM_ERR_INVALID,
+                       "job %d: pattern has %d nodes per element, operator needs %d",
+                       i1, J.pattern->npe, npe);
+            CFEM_CHECK(((uintptr_t)J.d_elems & 15) == 0, CFEM_ERR_INVALID,
+                       "job %d: element array must be 16-byte aligned", i1);
+            CFEM_TRY(check_coef(&J.coef, op == CFEM_OP_T10_STIFF, "coef"));
+            CFEM_TRY(check_coef(&J.load, op == CFEM_OP_T10_STIFF, "load"));
+            const int64_t m = J.pattern->n_elems;
+            if (i1 > i0 && (M + m) * per > stage_cap) break;
+            AsmJob a;
+            a.nodes = J.d_nodes;
+            a.elems = J.d_elems;
+            a.seg = J.pattern->seg;
+            a.contrib = J.pattern->contrib;
+            a.diag = J.pattern->diag;
+            a.vals = J.d_vals;
+            a.rhs = J.d_rhs;
+            a.coef = to_coef(&J.coef);
+            a.load = to_coef(&J.load);
+            a.e0 = M;
+            a.k0 = K;
+            a.a0 = A;
+            a.m = m;
+            a.nnz = J.pattern->nnz;
+            a.n_nodes = J.pattern->n_nodes;
+            rhs = rhs || (J.d_rhs != nullptr);
+            CFEM_CHECK(!rhs || J.d_rhs, CFEM_ERR_INVALID,
+                       "job %d: either every job of a batch has a load vector or none", i1);
+            M += m;
+            K += a.nnz;
+            A += a.n_nodes;
+            hj.push_back(a);
+            ++i1;
+        }
+        const int nj = (int)hj.size();
+        AsmJob *d_jobs = nullptr;
+        double *ke = nullptr, *fe = nullptr;
+        CFEM_TRY(tmp_alloc(&d_jobs, nj, s));
+        CFEM_CUDA(cudaMemcpyAsync(d_jobs, hj.data(), nj * sizeof(AsmJob),
+                                  cudaMemcpyHostToDevice, s));
+        CFEM_TRY(tmp_alloc(&ke, M * per, s));
+        const bool want_rhs = rhs && stiff;
+        if (want_rhs) CFEM_TRY(tmp_alloc(&fe, M * npe, s));
+        if (M > 0) {
+            if (op == CFEM_OP_P1_STIFF)
+                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_STIFF>, grid_for(M, 128), 128, 0, s,
+                            d_jobs, nj, M, ke, fe);
+            else if (op == CFEM_OP_P1_MASS)
+                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_MASS>, grid_for(M, 128), 128, 0, s,
+                            d_jobs, nj, M, ke, nullptr);
+            else if (op == CFEM_OP_T10_STIFF)
+                CFEM_LAUNCH(k_t10_scalar_batch<CFEM_OP_T10_STIFF>, grid_for(M, T10_WARPS),
+                            32 * T10_WARPS, 0, s, d_jobs, nj, M, ke, fe);
+            else
+                CFEM_LAUNCH(k_t10_scalar_batch<CFEM_OP_T10_MASS>, grid_for(M, T10_WARPS),
+                            32 * T10_WARPS, 0, s, d_jobs, nj, M, ke, nullptr);
+        }
+        unsigned g = grid_for(K, 256);
+        if (g > (unsigned)ctx->num_sms * 32) g = ctx->num_sms * 32;
+        if (K > 0) CFEM_LAUNCH(k_reduce_vals_batch, g, 256, 0, s, d_jobs, nj, K, npe, ke);
+        if (rhs) {
+            if (want_rhs) {
+                g = grid_for(A, 256);
+                if (g > (unsigned)ctx->num_sms * 32) g = ctx->num_sms * 32;
+                CFEM_LAUNCH(k_reduce_rhs_batch, g, 256, 0, s, d_jobs, nj, A, npe, fe);
+            } else {
+                for (int j = 0; j < nj; ++j)
+                    CFEM_CUDA(cudaMemsetAsync(hj[j].rhs, 0, hj[j].n_nodes * sizeof(double), s));
+            }
+        }
+        tmp_free(ke, s);
+        tmp_free(fe, s);
+        tmp_free(d_jobs, s);
+        i0 = i1;
+    }
+    return CFEM_OK;
     CFEM_API_END
 }
 

@@ -179,6 +179,27 @@ CFEM_API int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
                   const cfem_coef *coef, const cfem_coef *load,
                   double *d_vals, double *d_rhs, int32_t accumulate,
                   void *stream);
+/* One mesh of a batched scalar assembly (cfem_assemble_batch). */
+typedef struct cfem_assembly_job {
+    const cfem_pattern *pattern;   /* the mesh's pattern (cfem_pattern_create) */
+    const double *d_nodes;
+    const int32_t *d_elems;
+    cfem_coef coef;                /* k or rho_cp                              */
+    cfem_coef load;                /* f (stiffness operators)                  */
+    double *d_vals;                /* nnz values, overwritten                  */
+    double *d_rhs;                 /* n_nodes, overwritten; NULL in every job
+                                      of the batch to skip                     */
+} cfem_assembly_job;
+
+/* Assembles many independent meshes with one launch per pass (elements of
+ * all meshes, then CSR entries of all meshes, then loads), the batched
+ * form of cfem_assemble for the scalar operators (tet_poisson.py:35-69,
+ * tet10.py:138-165, tet_heat.py:72-94, tet10.py:229-249). Element-matrix
+ * staging is bounded to about 2 GiB per pass group. */
+CFEM_API int cfem_assemble_batch(cfem_ctx *ctx, int32_t op,
+                                 const cfem_assembly_job *jobs, int32_t n_jobs,
+                                 void *stream);
+
 /* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
  * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),
  * thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or QP). */
