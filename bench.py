@@ -135,6 +135,26 @@ def pcg_bytes(n_nodes, nnzb, iters, updates, precision="mixed"):
     return iters * (a + b) + (updates + 1) * r
 
 
+def spmv_bytes(n_nodes, nnzb, sz):
+    """Algorithmic bytes of one SpMV-phase launch (3x3 blocks, s-byte
+    values): blocks + column index, row pointers, read z and p, write p and
+    q."""
+    return nnzb * (9 * sz + 4) + 4 * (n_nodes + 1) + 12 * sz * n_nodes
+
+
+def _profiled_traffic(name, precision):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    key = f"dram_bytes_per_launch_{precision}:"
+    with open(path) as f:
+        for line in f:
+            if line.strip().startswith(key):
+                return int(line.split(":")[1].strip().split()[0])
+    return None
+
+
 def _device_step(dm, mesh, precision):
     """Pattern + assembly + loads + masking + solve on resident inputs."""
     from cloudfem_b200 import _native as N
@@ -237,10 +257,19 @@ def run_ours(args, rank, world, local_rank):
 
     pat = dm.pattern
     last = infos[-1]
-    bytes_launch = pcg_bytes(mesh.n_nodes, pat.nnz, last.iterations,
-                             last.residual_updates, args.precision)
+    bytes_solve = pcg_bytes(mesh.n_nodes, pat.nnz, last.iterations,
+                            last.residual_updates, args.precision)
+    sz = 4 if args.precision == "mixed" else 8
+    bytes_spmv = spmv_bytes(mesh.n_nodes, pat.nnz, sz)
+    spmv_ms = float(np.mean([i.spmv_ms for i in infos if i.spmv_samples])) \
+        if any(i.spmv_samples for i in infos) else None
     peak, peak_kind = _peaks()
-    achieved = bytes_launch / (last.kernel_ms * 1e-3) / 1e9
+    if spmv_ms:
+        achieved = bytes_spmv / (spmv_ms * 1e-3) / 1e9
+    else:
+        achieved = bytes_solve / (last.kernel_ms * 1e-3) / 1e9
+    traffic = _profiled_traffic("k_gx_tet10_elasticity_80x10x10",
+                                "fp32" if args.precision == "mixed" else "fp64")
     h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
     d2h = 3 * mesh.n_nodes * 8
     out = {
@@ -280,13 +309,14 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {
-            "kernel": "pcg solve launch sequence (k_pcg_init + graph of "
-                      "k_gx SpMV / k_greduce / k_gb update / k_greduce)",
+            "kernel": "k_gx (PCG SpMV phase: q = A p, p update, p.q)",
             "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-            "bytes_per_launch": bytes_launch,
-            "kernel_ms": last.kernel_ms,
-            "traffic": None,
+            "bytes_per_launch": bytes_spmv,
+            "launch_ms": spmv_ms,
+            "traffic": traffic,
+            "solve": {"bytes": bytes_solve, "kernel_ms": last.kernel_ms,
+                      "achieved_gbs": bytes_solve / (last.kernel_ms * 1e-3) / 1e9},
         },
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

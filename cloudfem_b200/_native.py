@@ -69,7 +69,8 @@ class LinSys(ctypes.Structure):
 class SolveStats(ctypes.Structure):
     _fields_ = [("status", _i32), ("iterations", _i32),
                 ("residual_updates", _i32), ("pad_", _i32),
-                ("relres", _f64), ("bnorm", _f64), ("kernel_ms", _f64)]
+                ("relres", _f64), ("bnorm", _f64), ("kernel_ms", _f64),
+                ("spmv_ms", _f64), ("spmv_samples", _i32), ("pad2_", _i32)]
 
 
 # (name, restype, argtypes) of every symbol in include/cfem.h
@@ -79,6 +80,7 @@ SIGNATURES = [
     ("cfem_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("cfem_ctx_destroy", ctypes.c_int, [_vp]),
     ("cfem_ctx_launch_count", _i64, [_vp]),
+    ("cfem_ctx_trim", _i32, [_vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("cfem_ctx_set_scheduler", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cfem_pattern_create", ctypes.c_int,
      [_vp, _vp, _i64, _i32, _i64, _vp, ctypes.POINTER(_vp)]),
@@ -173,6 +175,13 @@ class Runtime:
 
     def launches(self):
         return int(self.lib.cfem_ctx_launch_count(self.ctx))
+
+    def trim(self, keep_bytes=0):
+        """Return the library pool's unused device memory beyond keep_bytes
+        to the driver; returns the bytes the pool still reserves."""
+        out = ctypes.c_uint64()
+        check(self.lib.cfem_ctx_trim(self.ctx, int(keep_bytes), ctypes.byref(out)))
+        return int(out.value)
 
     def __del__(self):
         try:

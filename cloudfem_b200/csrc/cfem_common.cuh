@@ -56,6 +56,7 @@ extern std::atomic<int64_t> g_launches;
 
 #define CFEM_LAUNCH(kernel, grid, block, smem, stream, ...)                 \
     do {                                                                    \
+        (void)cudaGetLastError(); /* drop stale non-sticky errors */        \
         kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);         \
         ::cfem::g_launches.fetch_add(1, std::memory_order_relaxed);         \
         CFEM_CUDA(cudaGetLastError());                                      \
@@ -71,6 +72,7 @@ struct cfem_ctx {
     int scheduler = 0;                 // CFEM_SCHED_*
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // SpMV timing
     int *h_flags = nullptr;            // pinned host words (convergence polling)
 };
 
@@ -89,12 +91,20 @@ struct cfem_pattern {
 
 namespace cfem {
 
-// Stream-ordered temporary allocation (CUDA's default memory pool).
+// The library's stream-ordered memory pool on the current device. It keeps
+// what it has mapped (release threshold: unlimited) so repeated assemblies
+// and solves reuse the same physical pages instead of unmapping them at every
+// synchronisation and mapping them again; cfem_ctx_trim hands them back.
+cudaMemPool_t device_pool();
+
+// Stream-ordered temporary allocation from device_pool().
 template <typename T>
 int tmp_alloc(T **ptr, size_t count, cudaStream_t s) {
     *ptr = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMallocAsync((void **)ptr, count * sizeof(T), s);
+    cudaMemPool_t pool = device_pool();
+    if (!pool) return fail(CFEM_ERR_CUDA, "no memory pool on the current device");
+    cudaError_t e = cudaMallocFromPoolAsync((void **)ptr, count * sizeof(T), pool, s);
     if (e != cudaSuccess) {
         return fail(e == cudaErrorMemoryAllocation ? CFEM_ERR_NOMEM
                                                    : CFEM_ERR_CUDA,

@@ -4,6 +4,8 @@
 
 #include <string.h>
 
+#include <mutex>
+
 namespace cfem {
 
 static thread_local char g_err[1024] = "";
@@ -27,6 +29,30 @@ int fail(int code, const char *fmt, ...) {
 int set_device(int device) {
     CFEM_CUDA(cudaSetDevice(device));
     return CFEM_OK;
+}
+
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t device_pool() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
 }
 
 // ---------------------------------------------------------------- kernels
@@ -121,6 +147,8 @@ int cfem_ctx_create(int device, cfem_ctx **out) {
                "libcfem is built for sm_100a; device %d is sm_%d%d (%s)",
                device, prop.major, prop.minor, prop.name);
     CFEM_TRY(upload_tables(device));
+    CFEM_CHECK(device_pool() != nullptr, CFEM_ERR_CUDA,
+               "cannot create the memory pool on device %d", device);
     cfem_ctx *c = new cfem_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
@@ -131,6 +159,8 @@ int cfem_ctx_create(int device, cfem_ctx **out) {
     for (int i = 0; i < 4; ++i)
         CFEM_CUDA(cudaEventCreateWithFlags(&c->ev[i], i < 2 ? cudaEventDisableTiming
                                                             : cudaEventDefault));
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) CFEM_CUDA(cudaEventCreate(&c->tev[i][j]));
     CFEM_CUDA(cudaMallocHost(&c->h_flags, 4 * sizeof(int)));
     *out = c;
     return CFEM_OK;
@@ -143,6 +173,9 @@ int cfem_ctx_destroy(cfem_ctx *ctx) {
     if (ctx->work) cudaStreamSynchronize(ctx->work);
     for (int i = 0; i < 4; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            if (ctx->tev[i][j]) cudaEventDestroy(ctx->tev[i][j]);
     if (ctx->work) cudaStreamDestroy(ctx->work);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     delete ctx;
@@ -154,6 +187,23 @@ int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler) {
                CFEM_ERR_INVALID, "unknown scheduler %d", scheduler);
     ctx->scheduler = scheduler;
     return CFEM_OK;
+}
+
+int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes, uint64_t *reserved_bytes) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx, CFEM_ERR_INVALID, "cfem_ctx_trim: ctx is NULL");
+    CFEM_TRY(set_device(ctx->device));
+    cudaMemPool_t pool = device_pool();
+    CFEM_CHECK(pool, CFEM_ERR_CUDA, "no memory pool on device %d", ctx->device);
+    CFEM_CUDA(cudaDeviceSynchronize());
+    CFEM_CUDA(cudaMemPoolTrimTo(pool, (size_t)keep_bytes));
+    if (reserved_bytes) {
+        uint64_t v = 0;
+        CFEM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+        *reserved_bytes = v;
+    }
+    return CFEM_OK;
+    CFEM_API_END
 }
 
 int64_t cfem_ctx_launch_count(const cfem_ctx *ctx) {

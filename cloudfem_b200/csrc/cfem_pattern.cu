@@ -219,9 +219,9 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
     p->npe = npe;
     // pattern arrays come from the stream-ordered pool: building and
     // dropping patterns does not synchronise the device
-    CFEM_CUDA(cudaMallocAsync(&p->row_ptr, (n_nodes + 1) * sizeof(int32_t), s));
-    CFEM_CUDA(cudaMallocAsync(&p->diag, n_nodes * sizeof(int32_t), s));
-    CFEM_CUDA(cudaMallocAsync(&p->contrib, (total > 0 ? total : 1) * sizeof(int32_t), s));
+    CFEM_TRY(tmp_alloc(&p->row_ptr, n_nodes + 1, s));
+    CFEM_TRY(tmp_alloc(&p->diag, n_nodes, s));
+    CFEM_TRY(tmp_alloc(&p->contrib, total, s));
 
     uint64_t *keys = nullptr, *keys_sorted = nullptr;
     int32_t *ids = nullptr, *head = nullptr, *pos = nullptr, *rowk = nullptr;
@@ -286,8 +286,8 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
                         "[0, %lld)", (long long)n_nodes);
         }
         nnz = (int64_t)last_pos + last_head;
-        CFEM_CUDA(cudaMallocAsync(&p->col, (nnz > 0 ? nnz : 1) * sizeof(int32_t), s));
-        CFEM_CUDA(cudaMallocAsync(&p->seg, (nnz + 1) * sizeof(int32_t), s));
+        CFEM_TRY(tmp_alloc(&p->col, nnz, s));
+        CFEM_TRY(tmp_alloc(&p->seg, nnz + 1, s));
         CFEM_TRY(tmp_alloc(&rowk, nnz, s));
         CFEM_LAUNCH(k_scatter_heads, g, 256, 0, s, keys_sorted, head, pos,
                     total, n_nodes, p->col, rowk, p->seg);
@@ -299,8 +299,8 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
         tmp_free(rowk, s);
         tmp_free(d_bad, s);
     } else {
-        CFEM_CUDA(cudaMallocAsync(&p->col, sizeof(int32_t), s));
-        CFEM_CUDA(cudaMallocAsync(&p->seg, sizeof(int32_t), s));
+        CFEM_TRY(tmp_alloc(&p->col, 1, s));
+        CFEM_TRY(tmp_alloc(&p->seg, 1, s));
         CFEM_CUDA(cudaMemsetAsync(p->row_ptr, 0, (n_nodes + 1) * sizeof(int32_t), s));
         CFEM_CUDA(cudaMemsetAsync(p->seg, 0, sizeof(int32_t), s));
     }

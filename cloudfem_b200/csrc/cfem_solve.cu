@@ -804,7 +804,10 @@ k_pcg_step(const SysDev *__restrict__ sys, SysState *st,
 // LANES lanes, one row in flight per group, few registers so that many
 // warps are resident and hide the gather latency. Block values are read
 // from an entry-major copy (vsoa[e * nnzb + k]) so that the lanes of a
-// group read consecutive addresses for every entry e.
+// group read consecutive addresses for every entry e. z and the previous
+// direction are read-only for the whole launch (written by earlier launches
+// only), so their gathers go through the L1/texture path: neighbouring rows
+// of a block share most of their columns.
 template <typename T, int BS, bool DIFF>
 __device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
                              int64_t r1, int lane, double part[4]) {
@@ -826,7 +829,7 @@ __device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
         T pi[BS], acc[BS];
 #pragma unroll
         for (int c = 0; c < BS; ++c) {
-            pi[c] = zeta * ldcg(z + rr * BS + c) + beta * ldcg(pin + rr * BS + c);
+            pi[c] = zeta * __ldg(z + rr * BS + c) + beta * __ldg(pin + rr * BS + c);
             acc[c] = 0;
         }
         const int32_t kb = valid ? __ldg(S.rp + rr) : 0;
@@ -844,7 +847,7 @@ __device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
             T pj[BS];
 #pragma unroll
             for (int d = 0; d < BS; ++d) {
-                pj[d] = zeta * ldcg(z + j * BS + d) + beta * ldcg(pin + j * BS + d);
+                pj[d] = zeta * __ldg(z + j * BS + d) + beta * __ldg(pin + j * BS + d);
                 if (DIFF) pj[d] = (j == rr) ? pi[d] : pj[d] - pi[d];
             }
             const int32_t k2 = k + LANES;
@@ -902,6 +905,14 @@ __host__ __device__ inline int brows(int bs) { return bs == 3 ? 10 : 32; }
 // group of one system and writes one group partial, summed in warp order.
 constexpr int GROUP = 8;
 
+// Resident blocks per SM asked of k_gx: four (64 registers) keeps the most
+// warps in flight, except for FP64 3x3 blocks whose pipelined block values
+// need more registers; there three blocks (80 registers, no spills) measured
+// 12% faster per iteration than four with spills.
+template <typename T, int BS> struct GxOcc {
+    static constexpr int blocks = (sizeof(T) == 8 && BS == 3) ? 3 : 4;
+};
+
 __device__ __forceinline__ void group_store(double part[4], int nv, double *dst,
                                             int lane, int w) {
     __shared__ double red[GROUP][4];
@@ -922,7 +933,7 @@ __device__ __forceinline__ void group_store(double part[4], int nv, double *dst,
 }
 
 template <typename T, int BS>
-__global__ void __launch_bounds__(32 * GROUP, 4)
+__global__ void __launch_bounds__(32 * GROUP, (GxOcc<T, BS>::blocks))
 k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
      int n) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1172,6 +1183,8 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     if (grid > useful) grid = useful < 1 ? 1 : useful;
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     int max_steps = 3 * max_iter + 16;
+    double spmv_ms = 0.0;
+    int spmv_samples = 0;
     cudaStream_t w = ctx->work;
     // The work stream runs after everything queued so far on s.
     CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
@@ -1212,37 +1225,45 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
         CFEM_CUDA(cudaStreamWaitEvent(w, ctx->ev[0], 0));
         int per_iter = 2;
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
-        for (int it = 0; it < GRAPH_ITERS; ++it) {
-            for (int t = 0; t < 4; ++t) {
-                const int n = (int)la[t].size();
-                if (!n) continue;
-                const unsigned g = (unsigned)(n / GROUP);
-                if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                if (it == 0) ++per_iter;
+        // Two instantiations of the same iteration sequence, replayed in
+        // turn; each times the SpMV launch of its first iteration with its
+        // own pair of events, so a replay's pair is read only after that
+        // replay finished while the other one runs.
+        cudaGraph_t graph[2] = {nullptr, nullptr};
+        cudaGraphExec_t exec[2] = {nullptr, nullptr};
+        for (int gi = 0; gi < 2; ++gi) {
+            CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
+            for (int it = 0; it < GRAPH_ITERS; ++it) {
+                if (it == 0) CFEM_CUDA(cudaEventRecordWithFlags(ctx->tev[gi][0], w, cudaEventRecordExternal));
+                for (int t = 0; t < 4; ++t) {
+                    const int n = (int)la[t].size();
+                    if (!n) continue;
+                    const unsigned g = (unsigned)(n / GROUP);
+                    if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                    if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                    if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                    if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
+                    if (it == 0 && gi == 0) ++per_iter;
+                }
+                if (it == 0) CFEM_CUDA(cudaEventRecordWithFlags(ctx->tev[gi][1], w, cudaEventRecordExternal));
+                k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 0);
+                for (int t = 0; t < 4; ++t) {
+                    const int n = (int)lb[t].size();
+                    if (!n) continue;
+                    const unsigned g = (unsigned)(n / GROUP);
+                    if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (it == 0 && gi == 0) ++per_iter;
+                }
+                k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 1);
             }
-            k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 0);
-            for (int t = 0; t < 4; ++t) {
-                const int n = (int)lb[t].size();
-                if (!n) continue;
-                const unsigned g = (unsigned)(n / GROUP);
-                if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                if (it == 0) ++per_iter;
-            }
-            k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 1);
+            cudaError_t ce = cudaStreamEndCapture(w, &graph[gi]);
+            CFEM_CUDA(ce);
+            CFEM_CUDA(cudaGetLastError());
+            CFEM_CUDA(cudaGraphInstantiate(&exec[gi], graph[gi], 0));
         }
-        cudaError_t ce = cudaStreamEndCapture(w, &graph);
-        CFEM_CUDA(ce);
-        CFEM_CUDA(cudaGetLastError());
-        CFEM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         // Each iteration takes one X+B pair, each true-residual replacement
         // one more; a replay holds GRAPH_ITERS pairs. Poll the number of
         // active systems one replay behind so the queue never drains.
@@ -1251,19 +1272,32 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         flags[0] = flags[1] = 1;
         int rep = 0;
         for (; rep < max_replays; ++rep) {
-            CFEM_CUDA(cudaGraphLaunch(exec, w));
+            CFEM_CUDA(cudaGraphLaunch(exec[rep & 1], w));
             g_launches.fetch_add((int64_t)per_iter * GRAPH_ITERS, std::memory_order_relaxed);
             CFEM_CUDA(cudaMemcpyAsync((void *)&ctx->h_flags[rep & 1], &d_bar->active,
                                       sizeof(int), cudaMemcpyDeviceToHost, w));
             CFEM_CUDA(cudaEventRecord(ctx->ev[rep & 1], w));
             if (rep >= 1) {
-                CFEM_CUDA(cudaEventSynchronize(ctx->ev[(rep - 1) & 1]));
-                if (flags[(rep - 1) & 1] <= 0) break;
+                const int prev = (rep - 1) & 1;
+                CFEM_CUDA(cudaEventSynchronize(ctx->ev[prev]));
+                float sms = 0.0f;
+                if (cudaEventElapsedTime(&sms, ctx->tev[prev][0], ctx->tev[prev][1]) ==
+                        cudaSuccess) {
+                    if (flags[prev] > 0) {
+                        spmv_ms += sms;
+                        ++spmv_samples;
+                    }
+                } else {
+                    (void)cudaGetLastError();   // timing is best effort
+                }
+                if (flags[prev] <= 0) break;
             }
         }
         CFEM_CUDA(cudaStreamSynchronize(w));
-        cudaGraphExecDestroy(exec);
-        cudaGraphDestroy(graph);
+        for (int gi = 0; gi < 2; ++gi) {
+            cudaGraphExecDestroy(exec[gi]);
+            cudaGraphDestroy(graph[gi]);
+        }
     }
     CFEM_CUDA(cudaEventRecord(ctx->ev[3], w));
     CFEM_CUDA(cudaEventRecord(ctx->ev[0], w));
@@ -1288,6 +1322,9 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         stats[i].relres = hst[i].relres;
         stats[i].bnorm = sqrt(hst[i].bb);
         stats[i].kernel_ms = (double)kms;
+        stats[i].spmv_ms = spmv_samples ? spmv_ms / spmv_samples : 0.0;
+        stats[i].spmv_samples = spmv_samples;
+        stats[i].pad2_ = 0;
     }
     CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
@@ -1454,6 +1491,9 @@ extern "C" int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *L,
     stats->relres = hst.relres;
     stats->bnorm = sqrt(hst.bb);
     stats->kernel_ms = 0.0;
+    stats->spmv_ms = 0.0;
+    stats->spmv_samples = 0;
+    stats->pad2_ = 0;
     CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
     return CFEM_OK;

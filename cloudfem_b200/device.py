@@ -340,6 +340,8 @@ class SolveResult:
         self.relres = float(stats.relres)
         self.bnorm = float(stats.bnorm)
         self.kernel_ms = float(stats.kernel_ms)
+        self.spmv_ms = float(stats.spmv_ms)
+        self.spmv_samples = int(stats.spmv_samples)
 
     def __repr__(self):
         return (f"SolveResult(status={N.STATUS_NAMES.get(self.status)}, "

@@ -117,8 +117,13 @@ typedef struct cfem_solve_stats {
     int32_t pad_;
     double relres;           /* final ||r||/||b_lift|| (FP64, true residual)*/
     double bnorm;
-    double kernel_ms;        /* device time of the persistent launch (the
-                                same value in every record of a batch)     */
+    double kernel_ms;        /* device time of the whole solve (the same
+                                value in every record of a batch)          */
+    double spmv_ms;          /* graph scheduler: mean device time of one
+                                SpMV-phase launch (CUDA events inside the
+                                replayed graphs), else 0                    */
+    int32_t spmv_samples;    /* launches averaged into spmv_ms              */
+    int32_t pad2_;
 } cfem_solve_stats;
 
 typedef struct cfem_ctx cfem_ctx;
@@ -140,6 +145,14 @@ CFEM_API int cfem_ctx_destroy(cfem_ctx *ctx);
  *              else GRAPH (default). */
 enum { CFEM_SCHED_AUTO = 0, CFEM_SCHED_PERSISTENT = 1, CFEM_SCHED_GRAPH = 2 };
 CFEM_API int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler);
+/* The library's device memory (patterns, solver workspaces, sort buffers)
+ * comes from one stream-ordered pool per GPU that keeps what it has mapped,
+ * so repeated assemblies and solves do not map and unmap pages. This waits
+ * for the device, returns all but `keep_bytes` of the pool's unused memory
+ * to the driver and reports the bytes still reserved (NULL: not wanted).
+ * No counterpart in the reference (SciPy allocates host memory per call). */
+CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
+                           uint64_t *reserved_bytes);
 /* Number of kernels this library launched through `ctx` so far. */
 CFEM_API int64_t cfem_ctx_launch_count(const cfem_ctx *ctx);
 

@@ -118,3 +118,18 @@ def test_bad_connectivity_is_rejected(torch):
     m = TetMesh(np.zeros((4, 3)), np.array([[0, 1, 2, 9]]))
     with pytest.raises(ValueError):
         DeviceMesh(m)
+
+
+def test_pool_trim_keeps_results(torch):
+    """Handing the library pool's memory back to the driver between solves
+    changes nothing in the next solve."""
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.fem.tet_poisson import solve_tet_poisson
+    from cloudfem_b200.mesh import box_mesh
+    m = box_mesh(10, 9, 8)
+    bc = {s: 0.0 for s in C.FACES}
+    u1 = solve_tet_poisson(m, k=1.0, f=1.0, bc=bc)
+    rt = N.runtime()
+    assert rt.trim(0) >= 0
+    u2 = solve_tet_poisson(m, k=1.0, f=1.0, bc=bc)
+    assert np.array_equal(u1, u2)

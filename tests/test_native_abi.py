@@ -51,4 +51,4 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.Coef) == 24
     # cfem_linsys: 8+4+4 + 7 ptrs + 8 + 4 + 4
     assert ctypes.sizeof(_native.LinSys) == 16 + 7 * 8 + 16 + 8 + 8 + 8
-    assert ctypes.sizeof(_native.SolveStats) == 40
+    assert ctypes.sizeof(_native.SolveStats) == 56
