@@ -386,7 +386,7 @@ def run_c3(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
-    ns, ks = c3_draw()
+    ns, ks = c3_draw(args.meshes)
     problems = c3_problems(ns, ks)
     solver = BatchSolver(local_rank)
     batch = solver.prepare(problems)
@@ -402,7 +402,7 @@ def run_c3(args, rank, world, local_rank):
     step("fp64", 1e-12)
     x64 = [it["x"].clone() for it in batch.items]
     # plain FP64 path: one problem per assembly+solve call, on a prefix
-    plain_n = 32
+    plain_n = min(32, len(problems))
     sub = problems[:plain_n]
     solve_batch(sub[:2], precision="fp64", rtol=1e-10, solver=solver)
     torch.cuda.synchronize()
@@ -431,6 +431,14 @@ def run_c3(args, rank, world, local_rank):
     err = max(float(torch.linalg.norm(it["x"] - x) / torch.linalg.norm(x))
               for it, x in zip(batch.items, x64))
     iters = [r.iterations for r in res]
+    # SpMV roofline: k_gx over every system of the batch (scalar CSR: values
+    # and column indices, row pointers, gathered p read once, q written)
+    sz = 4 if args.precision == "mixed" else 8
+    nnz_all = sum(it["dm"].pattern.nnz for it in batch.items)
+    n_all = sum(it["dm"].n_nodes for it in batch.items)
+    spmv_b = nnz_all * (sz + 4) + 4 * (n_all + len(batch.items)) + 2 * sz * n_all
+    spmv_ms = float(np.mean([r.spmv_ms for r in res[:1] if r.spmv_samples] or [0.0]))
+    peak, peak_kind = _peaks()
 
     # end to end: host coefficient arrays in, solutions out (meshes and
     # their patterns stay resident in the solver, as in a serving process)
@@ -456,7 +464,7 @@ def run_c3(args, rank, world, local_rank):
         "dtype": "f32 PCG + f64 residual/update" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded unit-cube Tet10 meshes, lognormal k per cell)",
         "config": {
-            "workload": "batched_tet10_heat_512_meshes_n4to24",
+            "workload": f"batched_tet10_heat_{len(problems)}_meshes_n4to24",
             "meshes": len(problems), "free_dofs": int(free),
             "precision": args.precision, "rtol": rtol,
             "iterations_max": int(max(iters)), "iterations_mean": float(np.mean(iters)),
@@ -472,6 +480,16 @@ def run_c3(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if spmv_ms > 0:
+        ach = spmv_b / (spmv_ms * 1e-3) / 1e9
+        out["roofline"] = {
+            "kernel": "k_gx (batched PCG SpMV phase over all systems: q = A p, p update, p.q)",
+            "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
+            "launch_ms": spmv_ms,
+            "traffic": _profiled_traffic("k_gx_batched_tet10_heat",
+                                         "fp32" if args.precision == "mixed" else "fp64"),
+        }
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_c3(ns, ks)
     return out
@@ -536,6 +554,9 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
                     help="c2: Tet10 elasticity beam (default); c3: 512 "
                          "batched Tet10 heat meshes")
+    ap.add_argument("--meshes", type=int, default=C3_MESHES,
+                    help="c3: number of meshes of the seeded draw (a smaller "
+                         "batch of the same kind, e.g. for profiling)")
     args = ap.parse_args()
     if args.precision is None:
         args.precision = "mixed" if args.workload == "c3" else "fp64"

@@ -72,10 +72,15 @@ struct SysDev {
     int32_t max_stall, hist_cap;
     double *hist;
     // graph scheduler: update-phase chunks (whole block rows, <= 32 DOFs)
-    int32_t nchunksB, pad_;
+    int32_t nchunksB;
+    int32_t vec4;         // bs 1, graph scheduler: ci4 / va4 present
     double *partialB;     // nchunksB * 4
     const void *vsoa;     // working-precision block values, entry-major
     int64_t nnzb;         // blocks of the matrix (stride of vsoa)
+    // bs 1, graph scheduler: rows padded to whole units of 4 entries, row i
+    // starting at unit (rp[i] + 3 i + 3) / 4 (padding: column i, value 0)
+    const int32_t *ci4;
+    const void *va4;
 };
 
 struct SysState {
@@ -804,10 +809,11 @@ k_pcg_step(const SysDev *__restrict__ sys, SysState *st,
 // LANES lanes, one row in flight per group, few registers so that many
 // warps are resident and hide the gather latency. Block values are read
 // from an entry-major copy (vsoa[e * nnzb + k]) so that the lanes of a
-// group read consecutive addresses for every entry e. z and the previous
-// direction are read-only for the whole launch (written by earlier launches
-// only), so their gathers go through the L1/texture path: neighbouring rows
-// of a block share most of their columns.
+// group read consecutive addresses for every entry e. The new direction
+// p = zeta z + beta p_old is formed at every gathered entry (z and p_old are
+// read-only for the whole launch, so their gathers go through the L1/texture
+// path; neighbouring rows of a block share most of their columns) and
+// written for the block's own rows.
 template <typename T, int BS, bool DIFF>
 __device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
                              int64_t r1, int lane, double part[4]) {
@@ -882,6 +888,111 @@ __device__ void phase_A_lean(const SysDev &S, const SysState *st, int64_t r0,
     part[0] += (double)pq;
 }
 
+// Scalar rows (bs 1) from the unit-padded copy: each lane of a group of 8
+// reads whole units of four entries (one 16-byte column load and one (FP32)
+// or two (FP64) 16-byte value loads), so a row of up to 32 entries takes one
+// step with no per-entry masking; each group keeps H rows in flight. Lanes
+// without a unit use column = own row and coefficient 0.
+template <typename T, bool DIFF, int H>
+__device__ void phase_A_vec1(const SysDev &S, const SysState *st, int64_t r0,
+                             int64_t r1, int lane, double part[4]) {
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
+    T *q = (T *)S.q;
+    const T *va = (const T *)S.va4;
+    const int32_t *ci = S.ci4;
+    const int sub = lane & 7, grp = lane >> 3;
+    T pq = 0;
+    for (int64_t base = r0; base < r1; base += 4 * H) {
+        int64_t row[H], rr[H], u[H], uend[H];
+        bool valid[H];
+        T pi[H], acc[H];
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            row[h] = base + grp + 4 * h;
+            valid[h] = row[h] < r1;
+            rr[h] = valid[h] ? row[h] : r0;
+            pi[h] = __ldg(pv + rr[h]);
+            acc[h] = 0;
+            const int64_t kb = valid[h] ? __ldg(S.rp + rr[h]) : 0;
+            const int64_t k1 = valid[h] ? __ldg(S.rp + rr[h] + 1) : 0;
+            const int64_t u0 = (kb + 3 * rr[h] + 3) >> 2;
+            u[h] = u0 + sub;
+            uend[h] = u0 + ((k1 - kb + 3) >> 2);
+        }
+        while (true) {
+            bool more = false;
+#pragma unroll
+            for (int h = 0; h < H; ++h) more |= u[h] < uend[h];
+            if (!more) break;
+            int32_t c[H][4];
+            T a[H][4];
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+                if (u[h] < uend[h]) {
+                    const int4 cc = __ldg((const int4 *)ci + u[h]);
+                    c[h][0] = cc.x; c[h][1] = cc.y; c[h][2] = cc.z; c[h][3] = cc.w;
+                    if (sizeof(T) == 4) {
+                        const float4 vv = __ldg((const float4 *)va + u[h]);
+                        a[h][0] = (T)vv.x; a[h][1] = (T)vv.y; a[h][2] = (T)vv.z; a[h][3] = (T)vv.w;
+                    } else {
+                        const double2 v0 = __ldg((const double2 *)va + 2 * u[h]);
+                        const double2 v1 = __ldg((const double2 *)va + 2 * u[h] + 1);
+                        a[h][0] = (T)v0.x; a[h][1] = (T)v0.y; a[h][2] = (T)v1.x; a[h][3] = (T)v1.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        c[h][e] = (int32_t)rr[h];
+                        a[h][e] = 0;
+                    }
+                }
+            }
+            T pj[H][4];
+#pragma unroll
+            for (int h = 0; h < H; ++h)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) pj[h][e] = __ldg(pv + c[h][e]);
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    T v = pj[h][e];
+                    if (DIFF) v = (c[h][e] == rr[h]) ? pi[h] : v - pi[h];
+                    acc[h] += a[h][e] * v;
+                }
+                u[h] += 8;
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            acc[h] = group_sum<8>(acc[h]);
+            if (valid[h] && sub == 0) {
+                q[row[h]] = acc[h];
+                pq += pi[h] * acc[h];
+            }
+        }
+    }
+    part[0] += (double)pq;
+}
+
+// Unit-padded copy of a scalar CSR matrix for phase_A_vec1.
+template <typename T>
+__global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
+                       const int32_t *__restrict__ ci, const T *__restrict__ v,
+                       int32_t *__restrict__ ci4, T *__restrict__ v4) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t kb = rp[i], len = rp[i + 1] - kb;
+        const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
+        const int64_t m = ((len + 3) >> 2) * 4;
+        for (int64_t t = 0; t < m; ++t) {
+            ci4[o + t] = t < len ? ci[kb + t] : (int32_t)i;
+            v4[o + t] = t < len ? v[kb + t] : (T)0;
+        }
+    }
+}
+
 // Entry-major working-precision copy of block values (AoS -> SoA).
 template <typename TI, typename TO, int B2>
 __global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict__ out) {
@@ -898,7 +1009,81 @@ __global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict
 // to plain per-chunk slots; k_greduce then sums every system's slots in a
 // fixed order (one block per system) and advances its state. An iteration
 // is k_gx (A, R or ZERO), k_greduce, k_gb (B), k_greduce.
-__host__ __device__ inline int brows(int bs) { return bs == 3 ? 10 : 32; }
+// Update-phase chunk: BPASS passes of one warp over whole block rows (10
+// rows of 3 DOFs or 32 scalar rows per pass), all loads of a chunk issued
+// before its arithmetic.
+constexpr int BPASS = 4;
+__host__ __device__ inline int brows(int bs) { return BPASS * (bs == 3 ? 10 : 32); }
+
+template <typename T, int BS>
+__device__ void phase_B_multi(const SysDev &S, const SysState *st, int64_t r0,
+                              int64_t r1, int lane, double part[4]) {
+    constexpr int RP = BS == 3 ? 10 : 32;      // rows per pass
+    const T alpha = (T)vcg(&st->alpha);
+    const double alpha64 = vcg(&st->alpha);
+    const int pbuf = vcgi(&st->pbuf);
+    const T *p = (const T *)(pbuf ? S.p1 : S.p0);
+    T *r = (T *)S.r;
+    T *z = (T *)S.z;
+    const T *q = (const T *)S.q;
+    const T *dinv = (const T *)S.dinv;
+    const bool blockj = BS == 3 && S.precond == CFEM_PRECOND_BLOCK;
+    int64_t iv[BPASS], ii[BPASS];
+    bool valid[BPASS], fx[BPASS];
+    int cc[BPASS];
+    T rv[BPASS], pi[BPASS], qi[BPASS], d0[BPASS], d1[BPASS], d2[BPASS];
+    double xi[BPASS];
+#pragma unroll
+    for (int k = 0; k < BPASS; ++k) {
+        iv[k] = (r0 + (int64_t)k * RP) * BS + lane;
+        valid[k] = lane < RP * BS && iv[k] < r1 * BS;
+        ii[k] = valid[k] ? iv[k] : r0 * BS;
+        const int64_t row = ii[k] / BS;
+        cc[k] = (int)(ii[k] - row * BS);
+        fx[k] = S.fixed ? (__ldg(S.fixed + ii[k]) != 0) : false;
+        rv[k] = ldcg(r + ii[k]);
+        pi[k] = ldcg(p + ii[k]);
+        qi[k] = ldcg(q + ii[k]);
+        xi[k] = ldcg(S.x + ii[k]);
+        d1[k] = 0;
+        d2[k] = 0;
+        if (blockj) {
+            const T *D = dinv + row * 9 + cc[k] * 3;
+            d0[k] = ldcg(D);
+            d1[k] = ldcg(D + 1);
+            d2[k] = ldcg(D + 2);
+        } else {
+            d0[k] = ldcg(dinv + ii[k]);
+        }
+    }
+    T rz = 0, rr = 0;
+#pragma unroll
+    for (int k = 0; k < BPASS; ++k) {
+        if (valid[k] && !fx[k]) {
+            S.x[iv[k]] = xi[k] + alpha64 * (double)pi[k];
+            rv[k] -= alpha * qi[k];
+        }
+        T zv;
+        if (blockj) {
+            const int base = lane - cc[k];
+            const T ra = __shfl_sync(0xffffffffu, rv[k], base >= 0 ? base : 0);
+            const T rb = __shfl_sync(0xffffffffu, rv[k], base + 1 < 32 ? base + 1 : 31);
+            const T rc = __shfl_sync(0xffffffffu, rv[k], base + 2 < 32 ? base + 2 : 31);
+            zv = d0[k] * ra + d1[k] * rb + d2[k] * rc;
+        } else {
+            zv = d0[k] * rv[k];
+        }
+        if (valid[k]) {
+            if (fx[k]) zv = 0;
+            r[iv[k]] = rv[k];
+            z[iv[k]] = zv;
+            rz += rv[k] * zv;
+            rr += rv[k] * rv[k];
+        }
+    }
+    part[0] += (double)rz;
+    part[1] += (double)rr;
+}
 
 // Work lists hold each system's chunks padded to whole groups of GROUP
 // entries ({-1, -1} = padding), so every block of GROUP warps works on one
@@ -910,7 +1095,7 @@ constexpr int GROUP = 8;
 // need more registers; there three blocks (80 registers, no spills) measured
 // 12% faster per iteration than four with spills.
 template <typename T, int BS> struct GxOcc {
-    static constexpr int blocks = (sizeof(T) == 8 && BS == 3) ? 3 : 4;
+    static constexpr int blocks = (sizeof(T) == 8 || BS == 1) ? 3 : 4;
 };
 
 __device__ __forceinline__ void group_store(double part[4], int nv, double *dst,
@@ -949,7 +1134,10 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list
         const int64_t r0 = (int64_t)e.y * S.crows;
         const int64_t r1 = min(S.n, r0 + S.crows);
         if (ph == PH_A) {
-            phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
+            if (BS == 1 && S.vec4)
+                phase_A_vec1<T, sizeof(T) == 4, sizeof(T) == 4 ? 2 : 1>(S, &st[e.x], r0, r1, lane, part);
+            else
+                phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
             phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
@@ -974,9 +1162,49 @@ k_gb(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list
     if (e.x >= 0) {
         const int64_t r0 = (int64_t)e.y * brows(BS);
         const int64_t r1 = min(S.n, r0 + brows(BS));
-        phase_B<T, BS>(S, &st[e.x], r0, r1, lane, part);
+        phase_B_multi<T, BS>(S, &st[e.x], r0, r1, lane, part);
     }
     group_store(part, 2, S.partialB + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
+// Direction update of the A phase, p = zeta z + beta p_old, over the rows of
+// the update-phase chunks of scalar systems. A separate streaming launch
+// before k_gx so that the scalar SpMV gathers one precomputed vector instead
+// of forming p from z and p_old at every gathered entry (half the gathers and
+// their arithmetic). 3x3-block systems form p inside k_gx: there the extra
+// launch costs more than it saves.
+template <typename T, int BS>
+__global__ void __launch_bounds__(32 * GROUP)
+k_gp(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
+     int n) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    if (e.x < 0) return;
+    const SysDev &S = sys[e.x];
+    const SysState *sst = &st[e.x];
+    if (*(volatile const int32_t *)&sst->phase != PH_A) return;
+    const T beta = (T)vcg(&sst->beta);
+    const T zeta = (T)vcg(&sst->zeta);
+    const int pbuf = vcgi(&sst->pbuf);
+    const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
+    T *pout = (T *)(pbuf ? S.p0 : S.p1);
+    const T *z = (const T *)S.z;
+    const int64_t i0 = (int64_t)e.y * brows(BS) * BS;
+    const int64_t i1 = min(S.n * BS, i0 + (int64_t)brows(BS) * BS);
+    constexpr int NV = (BS == 3 ? 30 : 32) * BPASS / 32 + 1;
+    T zz[NV], pp[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const int64_t i = i0 + lane + 32 * k;
+        zz[k] = i < i1 ? __ldcs(z + i) : (T)0;
+        pp[k] = i < i1 ? __ldcs(pin + i) : (T)0;
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const int64_t i = i0 + lane + 32 * k;
+        if (i < i1) pout[i] = zeta * zz[k] + beta * pp[k];
+    }
 }
 
 // One block per system: fixed-order sum of its chunk slots, then advance.
@@ -1118,10 +1346,30 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         if (L.max_iter > max_iter) max_iter = L.max_iter;
     }
     const int n_chunks = (int)chunk_sys.size();
+    int per_sm = 0;
+    CFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_pcg_persistent, SOLVE_THREADS, 0));
+    CFEM_CHECK(per_sm > 0, CFEM_ERR_CUDA, "solver kernel cannot be resident");
+    int grid = ctx->num_sms * per_sm;
+    const int useful = (n_chunks * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
+    // One resident wave holds every chunk: the persistent kernel pays a grid
+    // barrier per phase and no launches. Otherwise the graph scheduler keeps
+    // the SMs fed with one warp per chunk per launch.
+    bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
+                      (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
+    // Scalar systems on the graph scheduler read a unit-padded copy.
+    size_t pad_bytes = 0;
+    if (!persistent)
+        for (int i = 0; i < n_systems; ++i)
+            if (hs[i].bs == 1) {
+                const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
+                pad_bytes += align(ne * 4) + align(ne * (hs[i].mode == CFEM_SOLVE_MIXED ? 4 : 8));
+            }
     bytes += align(n_systems * sizeof(SysDev)) + align(n_systems * sizeof(SysState)) +
              align(n_chunks * sizeof(int32_t)) + align(sizeof(GridBar)) +
              align((n_chunks + (size_t)GROUP * n_systems) * sizeof(int2)) +
-             align((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2)) + soa_bytes;
+             align((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2)) + soa_bytes +
+             pad_bytes;
     char *ws = nullptr;
     CFEM_TRY(tmp_alloc(&ws, bytes, s));
     CFEM_CUDA(cudaMemsetAsync(ws, 0, bytes, s));
@@ -1153,6 +1401,21 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
             S.vsoa = soa;
         } else {
             S.vsoa = (S.mode == CFEM_SOLVE_MIXED) ? (const void *)S.v32 : (const void *)S.v64;
+            if (!persistent) {
+                const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
+                int32_t *ci4 = (int32_t *)take(ne * 4);
+                void *va4 = take(ne * ts);
+                const unsigned g = std::min(grid_for(S.n, 256), (unsigned)ctx->num_sms * 16);
+                if (S.mode == CFEM_SOLVE_MIXED)
+                    CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
+                                ci4, (float *)va4);
+                else
+                    CFEM_LAUNCH(k_pad4<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
+                                ci4, (double *)va4);
+                S.ci4 = ci4;
+                S.va4 = va4;
+                S.vec4 = 1;
+            }
         }
     }
     SysDev *d_sys = (SysDev *)take(n_systems * sizeof(SysDev));
@@ -1169,17 +1432,6 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     CFEM_CUDA(cudaMemcpyAsync(&d_bar->active, &h_active, sizeof(int),
                               cudaMemcpyHostToDevice, s));
 
-    int per_sm = 0;
-    CFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_pcg_persistent, SOLVE_THREADS, 0));
-    CFEM_CHECK(per_sm > 0, CFEM_ERR_CUDA, "solver kernel cannot be resident");
-    int grid = ctx->num_sms * per_sm;
-    const int useful = (n_chunks * 32 + SOLVE_THREADS - 1) / SOLVE_THREADS;
-    // One resident wave holds every chunk: the persistent kernel pays a grid
-    // barrier per phase and no launches. Otherwise the graph scheduler keeps
-    // the SMs fed with one warp per chunk per launch.
-    bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
-                      (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
     if (grid > useful) grid = useful < 1 ? 1 : useful;
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     int max_steps = 3 * max_iter + 16;
@@ -1234,6 +1486,14 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         for (int gi = 0; gi < 2; ++gi) {
             CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
             for (int it = 0; it < GRAPH_ITERS; ++it) {
+                for (int t = 0; t < 4; t += 2) {   // scalar types only
+                    const int n = (int)lb[t].size();
+                    if (!n) continue;
+                    const unsigned g = (unsigned)(n / GROUP);
+                    if (t == 0) k_gp<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (t == 2) k_gp<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
+                    if (it == 0 && gi == 0) ++per_iter;
+                }
                 if (it == 0) CFEM_CUDA(cudaEventRecordWithFlags(ctx->tev[gi][0], w, cudaEventRecordExternal));
                 for (int t = 0; t < 4; ++t) {
                     const int n = (int)la[t].size();

@@ -133,3 +133,43 @@ def test_pool_trim_keeps_results(torch):
     assert rt.trim(0) >= 0
     u2 = solve_tet_poisson(m, k=1.0, f=1.0, bc=bc)
     assert np.array_equal(u1, u2)
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("bs", [1, 3])
+def test_graph_scheduler_matches_persistent(torch, bs, mode):
+    """The two schedulers (one persistent launch; graphs of per-phase
+    launches with their own SpMV kernels) solve the same system to the same
+    answer, for scalar and 3x3-block rows, in both precisions."""
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import BlockSystem, DeviceMesh, fixed_mask, pcg
+    from cloudfem_b200.mesh import box_mesh_tet10
+    if bs == 1:
+        dm, sysm = _poisson_system(torch, 7, seed=3)
+        mask, x0 = sysm.fixed, sysm.x.clone()
+        make = lambda x: BlockSystem(dm.rt, dm.n_nodes, 1, dm.pattern.row_ptr,  # noqa: E731
+                                     dm.pattern.col, sysm.vals64, sysm.b, x, mask)
+    else:
+        m = box_mesh_tet10(12, 3, 3, xlim=(0, 2), ylim=(0, .5), zlim=(0, .5))
+        dm = DeviceMesh(m)
+        vals, rhs = dm.assemble_elastic(N.OP_T10_ELAST, 210e9, 0.3,
+                                        body=(0.0, 0.0, -7.8e4))
+        idx = np.concatenate([3 * m.boundaries["xmin"] + c for c in range(3)])
+        mask, x0 = fixed_mask(dm.rt, 3 * m.n_nodes, idx, np.zeros(len(idx)))
+        make = lambda x: BlockSystem(dm.rt, dm.n_nodes, 3, dm.pattern.row_ptr,  # noqa: E731
+                                     dm.pattern.col, vals, rhs, x, mask)
+    md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
+    rtol = 1e-12 if mode == "fp64" else 1e-10
+    out = {}
+    try:
+        for sched in (N.SCHED_PERSISTENT, N.SCHED_GRAPH):
+            N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, sched))
+            x = x0.clone()
+            r = pcg([make(x)], md, rtol, 20000)[0]
+            assert r.status == N.CFEM_OK, r
+            out[sched] = x.cpu().numpy()
+    finally:
+        N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, N.SCHED_AUTO))
+    a, b = out[N.SCHED_PERSISTENT], out[N.SCHED_GRAPH]
+    tol = 1e-10 if mode == "fp64" else 1e-8
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
