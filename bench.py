@@ -43,6 +43,15 @@ RTOL = 1e-10
 L2_FLUSH_BYTES = 256 << 20
 
 
+def _set_scheduler(rt, name):
+    """Solver scheduler of the run (auto unless asked; polled graphs make
+    every solver launch visible to per-launch profilers)."""
+    from cloudfem_b200 import _native as N
+    code = {"auto": N.SCHED_AUTO, "persistent": N.SCHED_PERSISTENT,
+            "graph": N.SCHED_GRAPH, "polled": N.SCHED_GRAPH_POLLED}[name]
+    N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, code))
+
+
 def _peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -180,6 +189,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
+    _set_scheduler(rt, args.scheduler)
     mesh = _beam(FULL)
     free = _free_dofs(mesh)
     dm = DeviceMesh(mesh, local_rank)
@@ -386,6 +396,7 @@ def run_c3(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
+    _set_scheduler(rt, args.scheduler)
     ns, ks = c3_draw(args.meshes)
     problems = c3_problems(ns, ks)
     solver = BatchSolver(local_rank)
@@ -512,6 +523,174 @@ def cpu_baseline_c3(ns, ks, cap_n=7, count=12):
                       f"({free} free DOFs), one solve each"}
 
 
+# ---------------------------------------------------------------- C4
+C4_N = 128
+C4_STEPS = 200
+C4_PARAMS = dict(k=45.0, rho_cp=3.6e6, t0=20.0, h=25.0, t_inf=20.0,
+                 q0=1e7, sigma=0.1, dt=1.0)
+C4_FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+
+
+def c4_source(x, y, z):
+    """Gaussian heat source of peak q0 at the box centre."""
+    p = C4_PARAMS
+    r2 = (np.asarray(x) - 0.5) ** 2 + (np.asarray(y) - 0.5) ** 2 + (np.asarray(z) - 0.5) ** 2
+    return p["q0"] * np.exp(-r2 / (2.0 * p["sigma"] ** 2))
+
+
+def c4_robin():
+    return {f: (C4_PARAMS["h"], C4_PARAMS["t_inf"]) for f in C4_FACES}
+
+
+def _c4_device_march(dm, mesh, precision, n_steps, rtol):
+    """Pattern + K, C, F and Robin terms + theta march on resident inputs;
+    returns the final field on the device and the per-step solve records."""
+    import torch
+
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200._driver import last_solve_info, theta_march
+    from cloudfem_b200.fem.tet_heat import _terms, add_csr_into
+    p = C4_PARAMS
+    dm._pattern = None
+    K, F = dm.assemble(N.OP_P1_STIFF, coef=p["k"], load=c4_source)
+    K_add, F_add = _terms(dm, mesh, None, c4_robin())
+    add_csr_into(dm, K, K_add)
+    F = F + torch.from_numpy(F_add).to(dm.rt.device)
+    C, _ = dm.assemble(N.OP_P1_MASS, coef=p["rho_cp"])
+    empty = np.zeros(0, dtype=np.int64)
+    _, T = theta_march(dm, K, C, F, empty, np.zeros(0), n_steps * p["dt"],
+                       n_steps, p["t0"], 0.5, precision, rtol,
+                       keep_history=False)
+    return T, last_solve_info()
+
+
+def run_c4(args, rank, world, local_rank):
+    import torch
+
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import DeviceMesh
+    from cloudfem_b200.fem.tet_heat import transient_heat_tet
+    from cloudfem_b200.mesh import box_mesh
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rt = N.runtime(local_rank)
+    _set_scheduler(rt, args.scheduler)
+    n = args.c4_n
+    n_steps = args.c4_steps
+    mesh = box_mesh(n, n, n)
+    dm = DeviceMesh(mesh, local_rank)
+    free = mesh.n_nodes                       # Robin everywhere: no fixed DOF
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    rtol = 1e-10 if args.precision == "mixed" else 1e-12
+
+    # accuracy gate: the first 20 steps in both precisions
+    gate = min(20, n_steps)
+    T64, _ = _c4_device_march(dm, mesh, "fp64", gate, 1e-12)
+    T64 = T64.clone()
+    Tm, _ = _c4_device_march(dm, mesh, args.precision, gate, rtol)
+    gate_err = float(torch.linalg.norm(Tm - T64) / torch.linalg.norm(T64))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _c4_device_march(dm, mesh, "fp64", gate, 1e-12)
+    torch.cuda.synchronize()
+    fp64_s = time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        _c4_device_march(dm, mesh, args.precision, min(10, n_steps), rtol)
+    torch.cuda.synchronize()
+    times, l0 = [], rt.launches()
+    with Clocks(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            T, infos = _c4_device_march(dm, mesh, args.precision, n_steps, rtol)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = rt.launches() - l0
+    its = [r.iterations for r in infos]
+    spmv = [r.spmv_ms for r in infos if r.spmv_samples]
+
+    # end to end through the public API: host mesh in, host history out
+    e2e = []
+    for _ in range(max(1, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        transient_heat_tet(mesh, k=C4_PARAMS["k"], rho_cp=C4_PARAMS["rho_cp"],
+                           f=c4_source, robin=c4_robin(),
+                           t_end=n_steps * C4_PARAMS["dt"], dt=C4_PARAMS["dt"],
+                           T0=C4_PARAMS["t0"], method="cn",
+                           precision=args.precision, rtol=rtol)
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    if rank != 0:
+        return None
+    ms = float(np.sum(times))
+    dof_steps = free * n_steps
+    pat = dm.pattern
+    sz = 4 if args.precision == "mixed" else 8
+    spmv_b = pat.nnz * (sz + 4) + 4 * (mesh.n_nodes + 1) + 2 * sz * mesh.n_nodes
+    peak, peak_kind = _peaks()
+    out = {
+        "metric": METRIC,
+        "value": world * dof_steps * args.steps / (ms * 1e-3),
+        "unit": "DOF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 PCG + f64 residual/update" if args.precision == "mixed" else "f64",
+        "data": "synthetic (structured Kuhn P1 box, analytic Gaussian source)",
+        "config": {
+            "workload": f"transient_p1_heat_cn_box_{n}cubed_{n_steps}_steps",
+            "nodes": int(mesh.n_nodes), "elements": int(len(mesh.elements)),
+            "nnz": int(pat.nnz), "time_steps": n_steps, "free_dofs": int(free),
+            "precision": args.precision, "rtol_per_step": rtol,
+            "cg_iterations_per_step_mean": float(np.mean(its)),
+            "cg_iterations_per_step_max": int(max(its)),
+            "rel_err_vs_fp64_after_20_steps": gate_err,
+            "fp64_plain_20_steps": {"dof_per_s": free * gate / fp64_s},
+            "l2": "256 MiB buffer written between timed steps",
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {"value": world * dof_steps / (float(np.mean(e2e)) * 1e-3),
+                "unit": "DOF/s",
+                "h2d_bytes_per_step": int(mesh.nodes.nbytes + mesh.elements.nbytes),
+                "d2h_bytes_per_step": int((n_steps + 1) * mesh.n_nodes * 8),
+                "note": "transient_heat_tet: host mesh in, full host history out"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if spmv:
+        ach = spmv_b / (float(np.mean(spmv)) * 1e-3) / 1e9
+        out["roofline"] = {
+            "kernel": "k_gx (scalar PCG SpMV phase: q = A p, p.q)",
+            "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
+            "launch_ms": float(np.mean(spmv)), "traffic": None,
+        }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_c4()
+    return out
+
+
+def cpu_baseline_c4(n=32, n_steps=20):
+    """Oracle (NumPy assembly + SciPy LU, factorised once) on a small box."""
+    from oracle import cfem_oracle as O
+    p = C4_PARAMS
+    t0 = time.perf_counter()
+    m = O.box_mesh(n, n, n)
+    O.transient_heat_p1(m, k=p["k"], rho_cp=p["rho_cp"], f=c4_source,
+                        robin=c4_robin(), t_end=n_steps * p["dt"], dt=p["dt"],
+                        T0=p["t0"], method="cn")
+    dt = time.perf_counter() - t0
+    free = (n + 1) ** 3
+    return {"value": free * n_steps / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"box {n}^3 ({free} nodes), {n_steps} CN steps incl. assembly"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
@@ -519,7 +698,12 @@ def run_reference(args, rank):
     if args.workload == "c3":
         draw = c3_draw()
     for i in range(args.warmup + args.steps):
-        c = cpu_baseline_c3(*draw) if args.workload == "c3" else cpu_baseline()
+        if args.workload == "c3":
+            c = cpu_baseline_c3(*draw)
+        elif args.workload == "c4":
+            c = cpu_baseline_c4()
+        else:
+            c = cpu_baseline()
         if i >= args.warmup:
             per.append(c)
     value = float(np.mean([c["value"] for c in per]))
@@ -532,9 +716,9 @@ def run_reference(args, rank):
         "ms_per_step": float(np.mean([c["seconds"] for c in per])) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": ("batched_tet10_heat_512_meshes_n4to24"
-                                if args.workload == "c3" else
-                                "tet10_elasticity_beam_80x10x10"),
+        "config": {"workload": {"c3": "batched_tet10_heat_512_meshes_n4to24",
+                                "c4": f"transient_p1_heat_cn_box_{C4_N}cubed_{C4_STEPS}_steps",
+                                }.get(args.workload, "tet10_elasticity_beam_80x10x10"),
                    "sample": c["sample"]},
         "cpu_baseline": c,
         "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0,
@@ -551,15 +735,24 @@ def main():
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"],
                     help="default: fp64 for c2 (faster there), mixed for c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
                     help="c2: Tet10 elasticity beam (default); c3: 512 "
-                         "batched Tet10 heat meshes")
+                         "batched Tet10 heat meshes; c4: transient P1 heat, "
+                         "128^3 box, 200 Crank-Nicolson steps")
+    ap.add_argument("--scheduler", default="auto",
+                    choices=["auto", "persistent", "graph", "polled"],
+                    help="solver scheduler (polled: host-polled graph replays, "
+                         "for per-launch profiling)")
+    ap.add_argument("--c4-n", type=int, default=C4_N,
+                    help="c4: cells per box edge")
+    ap.add_argument("--c4-steps", type=int, default=C4_STEPS,
+                    help="c4: time steps per bench step")
     ap.add_argument("--meshes", type=int, default=C3_MESHES,
                     help="c3: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
     args = ap.parse_args()
     if args.precision is None:
-        args.precision = "mixed" if args.workload == "c3" else "fp64"
+        args.precision = "fp64" if args.workload == "c2" else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -576,6 +769,8 @@ def main():
                                     timeout=datetime.timedelta(seconds=300))
         if args.workload == "c3":
             out = run_c3(args, rank, world, local_rank)
+        elif args.workload == "c4":
+            out = run_c4(args, rank, world, local_rank)
         else:
             out = run_ours(args, rank, world, local_rank)
         if world > 1:

@@ -18,7 +18,7 @@ import warnings
 import numpy as np
 
 from . import _native as N
-from .device import BlockSystem, fixed_mask, pcg, raise_for
+from .device import BlockSystem, PcgPlan, fixed_mask, pcg, raise_for
 
 PRECISION = {"fp64": N.SOLVE_FP64, "mixed": N.SOLVE_MIXED}
 DEFAULT_RTOL = {"fp64": 1e-13, "mixed": 1e-10}
@@ -93,10 +93,12 @@ def n_steps_of(t_end, dt):
 
 
 def theta_march(dm, K, C, F, fixed_idx, fixed_val, t_end, n_steps, T0, theta,
-                precision="fp64", rtol=None, max_iter=None, load_fn=None):
+                precision="fp64", rtol=None, max_iter=None, load_fn=None,
+                keep_history=True):
     """(C + theta h K) T+ = (C - (1-theta) h K) T + h F, one device solve
     per step with the previous field as the initial guess
-    (tet_heat.py:239-274, tet10.py:509-548)."""
+    (tet_heat.py:239-274, tet10.py:509-548). With keep_history=False the
+    fields stay on the device and (times, final device field) is returned."""
     import torch
     rt = dm.rt
     lib, ctx = rt.lib, rt.ctx
@@ -119,20 +121,28 @@ def theta_march(dm, K, C, F, fixed_idx, fixed_val, t_end, n_steps, T0, theta,
     mask, T = fixed_mask(rt, n, fixed_idx, fixed_val, T)
     b = torch.empty(n, dtype=torch.float64, device=rt.device)
     sysA = BlockSystem(rt, n, 1, pat.row_ptr, pat.col, A, b, T, mask)
-    hist = np.empty((n_steps + 1, n))
-    hist[0] = T.cpu().numpy()
+    # one solve plan for the whole march (the reference factorises A_sys
+    # once, tet_heat.py:254): every step reuses its working copies and graphs
+    plan = PcgPlan([sysA], mode, rtol, max_iter)
+    hist = np.empty((n_steps + 1, n)) if keep_history else None
+    if keep_history:
+        hist[0] = T.cpu().numpy()
     infos = []
-    for step in range(n_steps):
-        Fs = F if load_fn is None else load_fn(step, h)
-        N.check(lib.cfem_spmv(ctx, n, 1, pat.row_ptr, pat.col, N.ptr(R), 1.0,
-                              N.ptr(T), 0.0, N.ptr(b), rt.stream()))
-        N.check(lib.cfem_axpby(ctx, n, 1.0, N.ptr(b), h, N.ptr(Fs), N.ptr(b),
-                               rt.stream()))
-        res = pcg([sysA], mode, rtol, max_iter)
-        accept(res[0], rtol, f"time step {step + 1}")
-        infos.append(res[0])
-        hist[step + 1] = T.cpu().numpy()
+    try:
+        for step in range(n_steps):
+            Fs = F if load_fn is None else load_fn(step, h)
+            N.check(lib.cfem_spmv(ctx, n, 1, pat.row_ptr, pat.col, N.ptr(R), 1.0,
+                                  N.ptr(T), 0.0, N.ptr(b), rt.stream()))
+            N.check(lib.cfem_axpby(ctx, n, 1.0, N.ptr(b), h, N.ptr(Fs), N.ptr(b),
+                                   rt.stream()))
+            res = plan.solve()
+            accept(res[0], rtol, f"time step {step + 1}")
+            infos.append(res[0])
+            if keep_history:
+                hist[step + 1] = T.cpu().numpy()
+    finally:
+        plan.close()
     _record(infos)
     times = np.cumsum(np.concatenate([[0.0], np.full(n_steps, h)]))
     times[-1] = t_end
-    return times, hist
+    return times, (hist if keep_history else T)

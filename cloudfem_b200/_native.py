@@ -29,7 +29,7 @@ OP_P1_ELAST, OP_T10_ELAST = 5, 6
 COEF_CONST, COEF_ELEM, COEF_QP, COEF_NODAL = 0, 1, 2, 3
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK = 0, 1
-SCHED_AUTO, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
+SCHED_AUTO, SCHED_PERSISTENT, SCHED_GRAPH, SCHED_GRAPH_POLLED = 0, 1, 2, 3
 
 STATUS_NAMES = {
     CFEM_OK: "ok", CFEM_ERR_INVALID: "invalid argument",
@@ -114,6 +114,11 @@ SIGNATURES = [
      [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     ("cfem_pcg_solve", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), _i32, ctypes.POINTER(SolveStats), _vp]),
+    ("cfem_pcg_plan_create", ctypes.c_int,
+     [_vp, ctypes.POINTER(LinSys), ctypes.c_int32, _vp, ctypes.POINTER(_vp)]),
+    ("cfem_pcg_plan_refresh", ctypes.c_int, [_vp, _vp]),
+    ("cfem_pcg_plan_solve", ctypes.c_int, [_vp, ctypes.POINTER(SolveStats), _vp]),
+    ("cfem_pcg_plan_destroy", ctypes.c_int, [_vp]),
     ("cfem_pcg_noalloc_capacity", ctypes.c_size_t, []),
     ("cfem_pcg_solve_noalloc", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), ctypes.POINTER(SolveStats), _vp]),

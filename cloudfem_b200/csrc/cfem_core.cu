@@ -183,7 +183,7 @@ int cfem_ctx_destroy(cfem_ctx *ctx) {
 }
 
 int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler) {
-    CFEM_CHECK(ctx && scheduler >= CFEM_SCHED_AUTO && scheduler <= CFEM_SCHED_GRAPH,
+    CFEM_CHECK(ctx && scheduler >= CFEM_SCHED_AUTO && scheduler <= CFEM_SCHED_GRAPH_POLLED,
                CFEM_ERR_INVALID, "unknown scheduler %d", scheduler);
     ctx->scheduler = scheduler;
     return CFEM_OK;

@@ -81,6 +81,7 @@ struct SysDev {
     // starting at unit (rp[i] + 3 i + 3) / 4 (padding: column i, value 0)
     const int32_t *ci4;
     const void *va4;
+    const double *va4d;   // FP64 values in the same layout (== va4 in FP64 mode)
 };
 
 struct SysState {
@@ -95,7 +96,8 @@ struct GridBar {
     unsigned int gen;
     int err;
     int active;
-    unsigned int pad0[29];
+    unsigned int rounds;    // loop bodies run (graph scheduler)
+    unsigned int pad0[28];
     unsigned int top;
     unsigned int pad1[31];
     unsigned int grp[BAR_MAX_GROUPS][32];
@@ -527,6 +529,116 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
     part[3] += aa;
 }
 
+// True residual (FP64) of scalar rows from the unit-padded copy, the same
+// sums and epilogue as phase_R<T, 1, INIT>: each lane of a group of 8 reads
+// whole units of four entries; padding entries (column = own row, value 0)
+// add nothing and are told apart from the real diagonal by position.
+template <typename T, bool INIT>
+__device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
+                             int64_t r1, int lane, double part[4], int *bad) {
+    constexpr int H = 2;
+    const int sub = lane & 7, grp = lane >> 3;
+    T *r = (T *)S.r;
+    T *z = (T *)S.z;
+    T *dinv = (T *)S.dinv;
+    const T *pc = (const T *)((INIT || vcgi(&st->pbuf) == 0) ? S.p0 : S.p1);
+    const int32_t *ci = S.ci4;
+    const double *va = S.va4d;
+    double rr = 0.0, bb = 0.0, aa = 0.0;
+    T rz = 0, rp = 0;
+    for (int64_t base = r0; base < r1; base += 4 * H) {
+        int64_t row[H], u[H], u0[H], uend[H], len[H];
+        bool valid[H];
+        double acc[H], aab[H], accf[H], dg[H];
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            row[h] = base + grp + 4 * h;
+            valid[h] = row[h] < r1;
+            const int64_t rr_ = valid[h] ? row[h] : r0;
+            const int64_t kb = valid[h] ? __ldg(S.rp + rr_) : 0;
+            const int64_t k1 = valid[h] ? __ldg(S.rp + rr_ + 1) : 0;
+            len[h] = k1 - kb;
+            u0[h] = (kb + 3 * rr_ + 3) >> 2;
+            u[h] = u0[h] + sub;
+            uend[h] = u0[h] + ((len[h] + 3) >> 2);
+            acc[h] = aab[h] = accf[h] = dg[h] = 0.0;
+        }
+        while (true) {
+            bool more = false;
+#pragma unroll
+            for (int h = 0; h < H; ++h) more |= u[h] < uend[h];
+            if (!more) break;
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+                if (u[h] < uend[h]) {
+                    const int4 cc = __ldg((const int4 *)ci + u[h]);
+                    const double2 v0 = __ldg((const double2 *)va + 2 * u[h]);
+                    const double2 v1 = __ldg((const double2 *)va + 2 * u[h] + 1);
+                    const int32_t c[4] = {cc.x, cc.y, cc.z, cc.w};
+                    const double a[4] = {v0.x, v0.y, v1.x, v1.y};
+                    double xj[4];
+                    bool fj[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        xj[e] = ldcg(S.x + c[e]);
+                        fj[e] = INIT && S.fixed ? (__ldg(S.fixed + c[e]) != 0) : false;
+                    }
+                    const int64_t pos = (u[h] - u0[h]) * 4;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const double ax = a[e] * xj[e];
+                        acc[h] += ax;
+                        aab[h] += fabs(ax);
+                        if (INIT && fj[e]) accf[h] += ax;
+                        if (INIT && c[e] == row[h] && pos + e < len[h]) dg[h] = a[e];
+                    }
+                }
+                u[h] += 8;
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            acc[h] = group_sum<8>(acc[h]);
+            aab[h] = group_sum<8>(aab[h]);
+            if (INIT) {
+                accf[h] = group_sum<8>(accf[h]);
+                dg[h] = group_sum<8>(dg[h]);
+            }
+            if (valid[h] && sub == 0) {
+                const int64_t i = row[h];
+                const bool fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
+                const double bi = __ldg(S.b + i);
+                const double rt = fx ? 0.0 : bi - acc[h];
+                if (INIT && !fx) {
+                    const double bl = bi - accf[h];
+                    bb += bl * bl;
+                }
+                rr += rt * rt;
+                if (!fx) aa += aab[h] * aab[h];
+                const T rv = (T)rt;
+                r[i] = rv;
+                if (INIT) {
+                    double iv = 0.0;
+                    if (!fx) {
+                        if (!(dg[h] > 0.0) || !isfinite(dg[h])) *bad = 1;
+                        else iv = 1.0 / dg[h];
+                    }
+                    dinv[i] = (T)iv;
+                }
+                T zv = ldcg((const T *)S.dinv + i) * rv;   // this lane's row
+                if (fx) zv = 0;
+                z[i] = zv;
+                rz += rv * zv;
+                if (!INIT) rp += rv * ldcg(pc + i);
+            }
+        }
+    }
+    part[0] += rr;
+    part[1] += INIT ? bb : (double)rp;
+    part[2] += (double)rz;
+    part[3] += aa;
+}
+
 template <int BS>
 __device__ void phase_zero(const SysDev &S, int64_t r0, int64_t r1, int lane) {
     for (int64_t i = r0 * BS + lane; i < r1 * BS; i += 32)
@@ -697,7 +809,10 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
     int bad = 0;
     if (RUN == RUN_INIT) {
         int flag = 0;
-        phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
+        if (BS == 1 && S.vec4)
+            phase_R_vec1<T, true>(S, st, r0, r1, lane, part, &flag);
+        else
+            phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
         bad = __any_sync(0xffffffffu, flag != 0);
     } else if (RUN == RUN_B) {
         phase_B<T, BS>(S, st, r0, r1, lane, part);
@@ -976,17 +1091,19 @@ __device__ void phase_A_vec1(const SysDev &S, const SysState *st, int64_t r0,
     part[0] += (double)pq;
 }
 
-// Unit-padded copy of a scalar CSR matrix for phase_A_vec1.
+// Unit-padded copy of a scalar CSR matrix for phase_A_vec1 / phase_R_vec1:
+// one warp per row, lanes writing consecutive entries.
 template <typename T>
 __global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
                        const int32_t *__restrict__ ci, const T *__restrict__ v,
                        int32_t *__restrict__ ci4, T *__restrict__ v4) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
         const int64_t kb = rp[i], len = rp[i + 1] - kb;
         const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
         const int64_t m = ((len + 3) >> 2) * 4;
-        for (int64_t t = 0; t < m; ++t) {
+        for (int64_t t = lane; t < m; t += 32) {
             ci4[o + t] = t < len ? ci[kb + t] : (int32_t)i;
             v4[o + t] = t < len ? v[kb + t] : (T)0;
         }
@@ -1119,12 +1236,13 @@ __device__ __forceinline__ void group_store(double part[4], int nv, double *dst,
 
 template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP, (GxOcc<T, BS>::blocks))
-k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
-     int n) {
+k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
+     const int2 *__restrict__ list, int n) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
     const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
     const SysDev &S = sys[lead.x];
     const int ph = *(volatile int32_t *)&st[lead.x].phase;
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
@@ -1140,7 +1258,10 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list
                 phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
-            phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            if (BS == 1 && S.vec4)
+                phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            else
+                phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<BS>(S, r0, r1, lane);
         }
@@ -1150,12 +1271,13 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list
 
 template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
-k_gb(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
-     int n) {
+k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
+     const int2 *__restrict__ list, int n) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
     const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
     const SysDev &S = sys[lead.x];
     if (*(volatile int32_t *)&st[lead.x].phase != PH_B) return;
     double part[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1175,11 +1297,12 @@ k_gb(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list
 // launch costs more than it saves.
 template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
-k_gp(const SysDev *__restrict__ sys, SysState *st, const int2 *__restrict__ list,
-     int n) {
+k_gp(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
+     const int2 *__restrict__ list, int n) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
     if (e.x < 0) return;
     const SysDev &S = sys[e.x];
     const SysState *sst = &st[e.x];
@@ -1248,7 +1371,28 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     }
 }
 
-constexpr int GRAPH_ITERS = 16;   // iterations per graph replay
+constexpr int GRAPH_ITERS = 2;    // iterations per body of the solve loop
+constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
+
+// Start of a graph-scheduled solve: every system active, no barrier error.
+__global__ void k_plan_start(GridBar *bar, int n_systems) {
+    if (threadIdx.x == 0) {
+        bar->active = n_systems;
+        bar->err = 0;
+        bar->rounds = 0;
+    }
+}
+
+// Loop condition of a graph-scheduled solve: another body while a system is
+// active and the round bound (from the largest max_iter) is not reached.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, GridBar *bar, unsigned max_rounds) {
+    if (threadIdx.x == 0) {
+        const unsigned r = bar->rounds + 1;
+        bar->rounds = r;
+        const int act = *(volatile int *)&bar->active;
+        cudaGraphSetConditional(h, (act > 0 && r < max_rounds) ? 1u : 0u);
+    }
+}
 }  // namespace cfem
 
 using namespace cfem;
@@ -1274,21 +1418,119 @@ extern "C" int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
     CFEM_API_END
 }
 
-extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
-                              int32_t n_systems, cfem_solve_stats *stats,
-                              void *stream) {
-    CFEM_API_BEGIN
-    CFEM_CHECK(ctx && systems && stats && n_systems > 0, CFEM_ERR_INVALID,
-               "cfem_pcg_solve: bad args");
-    CFEM_TRY(set_device(ctx->device));
-    cudaStream_t s = (cudaStream_t)stream;
-    std::vector<SysDev> hs(n_systems);
+// ---------------------------------------------------------------------------
+// Solve plans. A plan holds everything a batch of systems needs on the
+// device between solves: the system table, the work lists, the entry-major
+// (3x3) or unit-padded (scalar) working copies of the matrix values, the
+// solver vectors and the captured iteration graphs, plus its own stream,
+// events and pinned polling words (plans of one context can run from
+// different host threads and overlap on the device). A solve resets the
+// solver state, runs k_pcg_init and then the persistent kernel or graph
+// replays until every system has finished.
+struct cfem_pcg_plan {
+    cfem_ctx *ctx = nullptr;
+    int device = 0;
+    int n_systems = 0;
+    int n_chunks = 0;
+    int max_iter = 1;
+    bool persistent = true;
+    int grid = 1;
+    int per_iter = 0;
+    std::vector<cfem::SysDev> hs;
+    char *ws_copy = nullptr;      // system table, lists, working matrix copies
+    char *ws_state = nullptr;     // vectors, partials, states, barrier
+    size_t state_bytes = 0;
+    cfem::SysDev *d_sys = nullptr;
+    cfem::SysState *d_st = nullptr;
+    int32_t *d_chunks = nullptr;
+    cfem::GridBar *d_bar = nullptr;
+    cudaStream_t w = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int *h_flags = nullptr;
+    cudaStream_t w2 = nullptr;    // captures the loop body
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    // host-polled variant (CFEM_SCHED_GRAPH_POLLED): two instantiations of
+    // POLL_ITERS iterations replayed in turn
+    bool polled = false;
+    cudaGraph_t pgraph[2] = {nullptr, nullptr};
+    cudaGraphExec_t pexec[2] = {nullptr, nullptr};
+};
+
+namespace cfem {
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// (Re)build the working copies of the matrix values on stream s.
+static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
+    for (int i = 0; i < P->n_systems; ++i) {
+        SysDev &S = P->hs[i];
+        if (S.bs == 3) {
+            if (S.mode == CFEM_SOLVE_MIXED)
+                CFEM_LAUNCH((k_to_soa<float, float, 9>), grid_for(S.nnzb, 256), 256, 0,
+                            s, S.nnzb, S.v32, (float *)S.vsoa);
+            else
+                CFEM_LAUNCH((k_to_soa<double, double, 9>), grid_for(S.nnzb, 256), 256, 0,
+                            s, S.nnzb, S.v64, (double *)S.vsoa);
+        } else if (S.vec4) {
+            const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
+            if (S.mode == CFEM_SOLVE_MIXED)
+                CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
+                            (int32_t *)S.ci4, (float *)S.va4);
+            CFEM_LAUNCH(k_pad4<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
+                        (int32_t *)S.ci4, (double *)S.va4d);
+        }
+    }
+    return CFEM_OK;
+}
+
+static void plan_free(cfem_pcg_plan *P) {
+    if (!P) return;
+    cudaSetDevice(P->device);
+    if (P->w) cudaStreamSynchronize(P->w);
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    for (int gi = 0; gi < 2; ++gi) {
+        if (P->pexec[gi]) cudaGraphExecDestroy(P->pexec[gi]);
+        if (P->pgraph[gi]) cudaGraphDestroy(P->pgraph[gi]);
+    }
+    if (P->w) {
+        if (P->ws_copy) cudaFreeAsync(P->ws_copy, P->w);
+        if (P->ws_state) cudaFreeAsync(P->ws_state, P->w);
+        cudaStreamSynchronize(P->w);
+    }
+    for (int i = 0; i < 4; ++i)
+        if (P->ev[i]) cudaEventDestroy(P->ev[i]);
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            if (P->tev[i][j]) cudaEventDestroy(P->tev[i][j]);
+    if (P->h_flags) cudaFreeHost(P->h_flags);
+    if (P->w2) cudaStreamDestroy(P->w2);
+    if (P->w) cudaStreamDestroy(P->w);
+    (void)cudaGetLastError();
+    delete P;
+}
+
+static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
+                      cudaStream_t s, cfem_pcg_plan *P) {
+    P->ctx = ctx;
+    P->device = ctx->device;
+    P->n_systems = n_systems;
+    CFEM_CUDA(cudaStreamCreateWithFlags(&P->w, cudaStreamNonBlocking));
+    CFEM_CUDA(cudaStreamCreateWithFlags(&P->w2, cudaStreamNonBlocking));
+    for (int i = 0; i < 4; ++i)
+        CFEM_CUDA(cudaEventCreateWithFlags(&P->ev[i], i < 2 ? cudaEventDisableTiming
+                                                            : cudaEventDefault));
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) CFEM_CUDA(cudaEventCreate(&P->tev[i][j]));
+    CFEM_CUDA(cudaMallocHost(&P->h_flags, 4 * sizeof(int)));
+    std::vector<SysDev> &hs = P->hs;
+    hs.assign(n_systems, SysDev{});
     std::vector<int32_t> chunk_sys;
-    size_t bytes = 0;
-    auto align = [](size_t v) { return (v + 255) & ~(size_t)255; };
     int max_iter = 1;
     int64_t n_chunks_b = 0;
-    size_t soa_bytes = 0;
+    std::vector<int32_t> nnzbs(n_systems, 0);
     for (int i = 0; i < n_systems; ++i) {
         const cfem_linsys &L = systems[i];
         CFEM_CHECK(L.bs == 1 || L.bs == 3, CFEM_ERR_INVALID,
@@ -1303,6 +1545,13 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
                    "system %d: rtol and max_iter must be positive", i);
         CFEM_CHECK(L.n_rows < ((int64_t)1 << 31) / 9, CFEM_ERR_INVALID,
                    "system %d too large", i);
+        CFEM_CUDA(cudaMemcpyAsync(&nnzbs[i], L.d_row_ptr + L.n_rows, sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, s));
+    }
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    size_t state_bytes = 0, copy_bytes = 0;
+    for (int i = 0; i < n_systems; ++i) {
+        const cfem_linsys &L = systems[i];
         SysDev &S = hs[i];
         S.n = L.n_rows;
         S.bs = L.bs;
@@ -1328,24 +1577,22 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
         S.hist = L.d_history;
         for (int c = 0; c < S.nchunks; ++c) chunk_sys.push_back(i);
         S.nchunksB = (int32_t)((L.n_rows + brows(L.bs) - 1) / brows(L.bs));
-        int32_t nnzb = 0;
-        CFEM_CUDA(cudaMemcpyAsync(&nnzb, L.d_row_ptr + L.n_rows, sizeof(int32_t),
-                                  cudaMemcpyDeviceToHost, s));
-        CFEM_CUDA(cudaStreamSynchronize(s));
-        S.nnzb = nnzb;
-        if (L.bs == 3) soa_bytes += align((size_t)nnzb * 9 * (L.mode == CFEM_SOLVE_MIXED ? 4 : 8));
+        S.nnzb = nnzbs[i];
         const size_t ts = (L.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
         const size_t nd = (size_t)L.n_rows * L.bs;
         const size_t nprec = (S.precond == CFEM_PRECOND_BLOCK) ? (size_t)L.n_rows * 9 : nd;
-        bytes += 5 * align(nd * ts) + align(nprec * ts) +
-                 align(S.nchunks * 4 * sizeof(double)) +
-                 align(S.ntiles * 4 * sizeof(double)) +
-                 align(S.ntiles * sizeof(unsigned)) +
-                 align(S.nchunksB * 4 * sizeof(double));
+        state_bytes += 5 * align256(nd * ts) + align256(nprec * ts) +
+                       align256(S.nchunks * 4 * sizeof(double)) +
+                       align256(S.ntiles * 4 * sizeof(double)) +
+                       align256(S.ntiles * sizeof(unsigned)) +
+                       align256(S.nchunksB * 4 * sizeof(double));
+        if (L.bs == 3) copy_bytes += align256((size_t)S.nnzb * 9 * ts);
         n_chunks_b += S.nchunksB;
         if (L.max_iter > max_iter) max_iter = L.max_iter;
     }
     const int n_chunks = (int)chunk_sys.size();
+    P->n_chunks = n_chunks;
+    P->max_iter = max_iter;
     int per_sm = 0;
     CFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &per_sm, k_pcg_persistent, SOLVE_THREADS, 0));
@@ -1355,223 +1602,292 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     // One resident wave holds every chunk: the persistent kernel pays a grid
     // barrier per phase and no launches. Otherwise the graph scheduler keeps
     // the SMs fed with one warp per chunk per launch.
-    bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
-                      (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
+    const bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
+                            (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
+    if (grid > useful) grid = useful < 1 ? 1 : useful;
+    if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
+    P->persistent = persistent;
+    P->grid = grid;
     // Scalar systems on the graph scheduler read a unit-padded copy.
-    size_t pad_bytes = 0;
     if (!persistent)
         for (int i = 0; i < n_systems; ++i)
             if (hs[i].bs == 1) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
-                pad_bytes += align(ne * 4) + align(ne * (hs[i].mode == CFEM_SOLVE_MIXED ? 4 : 8));
+                copy_bytes += align256(ne * 4) + align256(ne * 8) +
+                              (hs[i].mode == CFEM_SOLVE_MIXED ? align256(ne * 4) : 0);
             }
-    bytes += align(n_systems * sizeof(SysDev)) + align(n_systems * sizeof(SysState)) +
-             align(n_chunks * sizeof(int32_t)) + align(sizeof(GridBar)) +
-             align((n_chunks + (size_t)GROUP * n_systems) * sizeof(int2)) +
-             align((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2)) + soa_bytes +
-             pad_bytes;
-    char *ws = nullptr;
-    CFEM_TRY(tmp_alloc(&ws, bytes, s));
-    CFEM_CUDA(cudaMemsetAsync(ws, 0, bytes, s));
-    size_t off = 0;
-    auto take = [&](size_t b) { char *p = ws + off; off += align(b); return (void *)p; };
+    const size_t list_a = n_chunks + (size_t)GROUP * n_systems;
+    const size_t list_b = n_chunks_b + (size_t)GROUP * n_systems;
+    copy_bytes += align256(n_systems * sizeof(SysDev)) + align256(n_chunks * sizeof(int32_t)) +
+                  align256(list_a * sizeof(int2)) + align256(list_b * sizeof(int2));
+    state_bytes += align256(n_systems * sizeof(SysState)) + align256(sizeof(GridBar));
+    CFEM_TRY(tmp_alloc(&P->ws_copy, copy_bytes, s));
+    CFEM_TRY(tmp_alloc(&P->ws_state, state_bytes, s));
+    P->state_bytes = state_bytes;
+    size_t oc = 0, os = 0;
+    auto take_c = [&](size_t b) { char *p = P->ws_copy + oc; oc += align256(b); return (void *)p; };
+    auto take_s = [&](size_t b) { char *p = P->ws_state + os; os += align256(b); return (void *)p; };
     for (int i = 0; i < n_systems; ++i) {
         SysDev &S = hs[i];
         const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
         const size_t nd = (size_t)S.n * S.bs;
         const size_t nprec = (S.precond == CFEM_PRECOND_BLOCK) ? (size_t)S.n * 9 : nd;
-        S.r = take(nd * ts);
-        S.z = take(nd * ts);
-        S.p0 = take(nd * ts);
-        S.p1 = take(nd * ts);
-        S.q = take(nd * ts);
-        S.dinv = take(nprec * ts);
-        S.partial = (double *)take(S.nchunks * 4 * sizeof(double));
-        S.tpartial = (double *)take(S.ntiles * 4 * sizeof(double));
-        S.tcnt = (unsigned *)take(S.ntiles * sizeof(unsigned));
-        S.partialB = (double *)take(S.nchunksB * 4 * sizeof(double));
+        S.r = take_s(nd * ts);
+        S.z = take_s(nd * ts);
+        S.p0 = take_s(nd * ts);
+        S.p1 = take_s(nd * ts);
+        S.q = take_s(nd * ts);
+        S.dinv = take_s(nprec * ts);
+        S.partial = (double *)take_s(S.nchunks * 4 * sizeof(double));
+        S.tpartial = (double *)take_s(S.ntiles * 4 * sizeof(double));
+        S.tcnt = (unsigned *)take_s(S.ntiles * sizeof(unsigned));
+        S.partialB = (double *)take_s(S.nchunksB * 4 * sizeof(double));
         if (S.bs == 3) {
-            void *soa = take((size_t)S.nnzb * 9 * ts);
-            if (S.mode == CFEM_SOLVE_MIXED)
-                CFEM_LAUNCH((k_to_soa<float, float, 9>), grid_for(S.nnzb, 256), 256, 0,
-                            s, S.nnzb, S.v32, (float *)soa);
-            else
-                CFEM_LAUNCH((k_to_soa<double, double, 9>), grid_for(S.nnzb, 256), 256, 0,
-                            s, S.nnzb, S.v64, (double *)soa);
-            S.vsoa = soa;
+            S.vsoa = take_c((size_t)S.nnzb * 9 * ts);
         } else {
             S.vsoa = (S.mode == CFEM_SOLVE_MIXED) ? (const void *)S.v32 : (const void *)S.v64;
             if (!persistent) {
                 const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
-                int32_t *ci4 = (int32_t *)take(ne * 4);
-                void *va4 = take(ne * ts);
-                const unsigned g = std::min(grid_for(S.n, 256), (unsigned)ctx->num_sms * 16);
-                if (S.mode == CFEM_SOLVE_MIXED)
-                    CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
-                                ci4, (float *)va4);
-                else
-                    CFEM_LAUNCH(k_pad4<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
-                                ci4, (double *)va4);
-                S.ci4 = ci4;
-                S.va4 = va4;
+                S.ci4 = (const int32_t *)take_c(ne * 4);
+                S.va4d = (const double *)take_c(ne * 8);
+                S.va4 = (S.mode == CFEM_SOLVE_MIXED) ? take_c(ne * 4) : (const void *)S.va4d;
                 S.vec4 = 1;
             }
         }
     }
-    SysDev *d_sys = (SysDev *)take(n_systems * sizeof(SysDev));
-    SysState *d_st = (SysState *)take(n_systems * sizeof(SysState));
-    int32_t *d_chunks = (int32_t *)take(n_chunks * sizeof(int32_t));
-    GridBar *d_bar = (GridBar *)take(sizeof(GridBar));
-    int2 *d_lista = (int2 *)take((n_chunks + (size_t)GROUP * n_systems) * sizeof(int2));
-    int2 *d_listb = (int2 *)take((n_chunks_b + (size_t)GROUP * n_systems) * sizeof(int2));
-    const int h_active = n_systems;
-    CFEM_CUDA(cudaMemcpyAsync(d_sys, hs.data(), n_systems * sizeof(SysDev),
+    P->d_st = (SysState *)take_s(n_systems * sizeof(SysState));
+    P->d_bar = (GridBar *)take_s(sizeof(GridBar));
+    P->d_sys = (SysDev *)take_c(n_systems * sizeof(SysDev));
+    P->d_chunks = (int32_t *)take_c(n_chunks * sizeof(int32_t));
+    int2 *d_lista = (int2 *)take_c(list_a * sizeof(int2));
+    int2 *d_listb = (int2 *)take_c(list_b * sizeof(int2));
+    CFEM_TRY(plan_copies(P, s));
+    CFEM_CUDA(cudaMemcpyAsync(P->d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
-    CFEM_CUDA(cudaMemcpyAsync(d_chunks, chunk_sys.data(),
+    CFEM_CUDA(cudaMemcpyAsync(P->d_chunks, chunk_sys.data(),
                               n_chunks * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    CFEM_CUDA(cudaMemcpyAsync(&d_bar->active, &h_active, sizeof(int),
-                              cudaMemcpyHostToDevice, s));
-
-    if (grid > useful) grid = useful < 1 ? 1 : useful;
-    if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
-    int max_steps = 3 * max_iter + 16;
-    double spmv_ms = 0.0;
-    int spmv_samples = 0;
-    cudaStream_t w = ctx->work;
-    // The work stream runs after everything queued so far on s.
-    CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
-    CFEM_CUDA(cudaStreamWaitEvent(w, ctx->ev[0], 0));
-    CFEM_CUDA(cudaEventRecord(ctx->ev[2], w));
-    CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, w,
-                d_sys, d_st, d_chunks, n_chunks, d_bar);
     if (persistent) {
-        void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
-                        (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
-        CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
-                                              dim3(SOLVE_THREADS), args, 0, w));
-        g_launches.fetch_add(1, std::memory_order_relaxed);
-    } else {
-        // Work lists per (precision, block size): {system, chunk} pairs.
-        std::vector<int2> la[4], lb[4];
-        for (int i = 0; i < n_systems; ++i) {
-            const int t = (hs[i].mode == CFEM_SOLVE_MIXED ? 2 : 0) + (hs[i].bs == 3 ? 1 : 0);
-            for (int c = 0; c < hs[i].nchunks; ++c) la[t].push_back(make_int2(i, c));
-            while (la[t].size() % GROUP) la[t].push_back(make_int2(-1, -1));
-            for (int c = 0; c < hs[i].nchunksB; ++c) lb[t].push_back(make_int2(i, c));
-            while (lb[t].size() % GROUP) lb[t].push_back(make_int2(-1, -1));
+        // host staging must stay valid until the copies ran
+        CFEM_CUDA(cudaStreamSynchronize(s));
+        return CFEM_OK;
+    }
+    // Work lists per (precision, block size): {system, chunk} pairs.
+    std::vector<int2> la[4], lb[4];
+    for (int i = 0; i < n_systems; ++i) {
+        const int t = (hs[i].mode == CFEM_SOLVE_MIXED ? 2 : 0) + (hs[i].bs == 3 ? 1 : 0);
+        for (int c = 0; c < hs[i].nchunks; ++c) la[t].push_back(make_int2(i, c));
+        while (la[t].size() % GROUP) la[t].push_back(make_int2(-1, -1));
+        for (int c = 0; c < hs[i].nchunksB; ++c) lb[t].push_back(make_int2(i, c));
+        while (lb[t].size() % GROUP) lb[t].push_back(make_int2(-1, -1));
+    }
+    int2 *pa[4], *pb[4];
+    size_t oa = 0, ob = 0;
+    for (int t = 0; t < 4; ++t) {
+        pa[t] = d_lista + oa;
+        pb[t] = d_listb + ob;
+        if (!la[t].empty())
+            CFEM_CUDA(cudaMemcpyAsync(pa[t], la[t].data(), la[t].size() * sizeof(int2),
+                                      cudaMemcpyHostToDevice, s));
+        if (!lb[t].empty())
+            CFEM_CUDA(cudaMemcpyAsync(pb[t], lb[t].data(), lb[t].size() * sizeof(int2),
+                                      cudaMemcpyHostToDevice, s));
+        oa += la[t].size();
+        ob += lb[t].size();
+    }
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    cudaStream_t w = P->w;
+    SysDev *d_sys = P->d_sys;
+    SysState *d_st = P->d_st;
+    GridBar *d_bar = P->d_bar;
+    int per_iter = 2;
+    // One iteration: direction (scalar systems), SpMV, reduction, update,
+    // reduction. The SpMV of the first iteration is bracketed by the
+    // timing events when tev is given.
+    auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
+        for (int t = 0; t < 4; t += 2) {   // scalar types only
+            const int n = (int)lb[t].size();
+            if (!n) continue;
+            const unsigned g = (unsigned)(n / GROUP);
+            if (t == 0) k_gp<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (t == 2) k_gp<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (count) ++per_iter;
         }
-        int2 *pa[4], *pb[4];
-        size_t oa = 0, ob = 0;
+        if (t0) CFEM_CUDA(cudaEventRecordWithFlags(t0, cs, cudaEventRecordExternal));
         for (int t = 0; t < 4; ++t) {
-            pa[t] = d_lista + oa;
-            pb[t] = d_listb + ob;
-            if (!la[t].empty())
-                CFEM_CUDA(cudaMemcpyAsync(pa[t], la[t].data(), la[t].size() * sizeof(int2),
-                                          cudaMemcpyHostToDevice, s));
-            if (!lb[t].empty())
-                CFEM_CUDA(cudaMemcpyAsync(pb[t], lb[t].data(), lb[t].size() * sizeof(int2),
-                                          cudaMemcpyHostToDevice, s));
-            oa += la[t].size();
-            ob += lb[t].size();
+            const int n = (int)la[t].size();
+            if (!n) continue;
+            const unsigned g = (unsigned)(n / GROUP);
+            if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
+            if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
+            if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
+            if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
+            if (count) ++per_iter;
         }
-        CFEM_CUDA(cudaEventRecord(ctx->ev[0], s));
-        CFEM_CUDA(cudaStreamWaitEvent(w, ctx->ev[0], 0));
-        int per_iter = 2;
-        // Two instantiations of the same iteration sequence, replayed in
-        // turn; each times the SpMV launch of its first iteration with its
-        // own pair of events, so a replay's pair is read only after that
-        // replay finished while the other one runs.
-        cudaGraph_t graph[2] = {nullptr, nullptr};
-        cudaGraphExec_t exec[2] = {nullptr, nullptr};
+        if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));
+        k_greduce<<<n_systems, RED_THREADS, 0, cs>>>(d_sys, d_st, d_bar, 0);
+        for (int t = 0; t < 4; ++t) {
+            const int n = (int)lb[t].size();
+            if (!n) continue;
+            const unsigned g = (unsigned)(n / GROUP);
+            if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (count) ++per_iter;
+        }
+        k_greduce<<<n_systems, RED_THREADS, 0, cs>>>(d_sys, d_st, d_bar, 1);
+        return CFEM_OK;
+    };
+    // The whole solve is one graph: reset of the solver state, k_pcg_init,
+    // a first (timed) iteration, then a device-side WHILE loop of bodies of
+    // GRAPH_ITERS iterations that ends when no system is active. No host
+    // polling; at most GRAPH_ITERS - 1 iterations run past convergence
+    // (their kernels return at once for finished systems).
+    if (ctx->scheduler == CFEM_SCHED_GRAPH_POLLED) {
+        // Plain graphs of POLL_ITERS iterations replayed by the host, which
+        // polls the active count one replay behind (every kernel launch is
+        // visible to per-launch profilers).
+        P->polled = true;
         for (int gi = 0; gi < 2; ++gi) {
             CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
-            for (int it = 0; it < GRAPH_ITERS; ++it) {
-                for (int t = 0; t < 4; t += 2) {   // scalar types only
-                    const int n = (int)lb[t].size();
-                    if (!n) continue;
-                    const unsigned g = (unsigned)(n / GROUP);
-                    if (t == 0) k_gp<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (t == 2) k_gp<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (it == 0 && gi == 0) ++per_iter;
-                }
-                if (it == 0) CFEM_CUDA(cudaEventRecordWithFlags(ctx->tev[gi][0], w, cudaEventRecordExternal));
-                for (int t = 0; t < 4; ++t) {
-                    const int n = (int)la[t].size();
-                    if (!n) continue;
-                    const unsigned g = (unsigned)(n / GROUP);
-                    if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                    if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                    if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                    if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pa[t], n);
-                    if (it == 0 && gi == 0) ++per_iter;
-                }
-                if (it == 0) CFEM_CUDA(cudaEventRecordWithFlags(ctx->tev[gi][1], w, cudaEventRecordExternal));
-                k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 0);
-                for (int t = 0; t < 4; ++t) {
-                    const int n = (int)lb[t].size();
-                    if (!n) continue;
-                    const unsigned g = (unsigned)(n / GROUP);
-                    if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, w>>>(d_sys, d_st, pb[t], n);
-                    if (it == 0 && gi == 0) ++per_iter;
-                }
-                k_greduce<<<n_systems, RED_THREADS, 0, w>>>(d_sys, d_st, d_bar, 1);
-            }
-            cudaError_t ce = cudaStreamEndCapture(w, &graph[gi]);
+            for (int it = 0; it < POLL_ITERS; ++it)
+                CFEM_TRY(iteration(w, it == 0 && gi == 0, it == 0 ? P->tev[gi][0] : nullptr,
+                                   it == 0 ? P->tev[gi][1] : nullptr));
+            cudaError_t ce = cudaStreamEndCapture(w, &P->pgraph[gi]);
             CFEM_CUDA(ce);
             CFEM_CUDA(cudaGetLastError());
-            CFEM_CUDA(cudaGraphInstantiate(&exec[gi], graph[gi], 0));
+            CFEM_CUDA(cudaGraphInstantiate(&P->pexec[gi], P->pgraph[gi], 0));
         }
-        // Each iteration takes one X+B pair, each true-residual replacement
-        // one more; a replay holds GRAPH_ITERS pairs. Poll the number of
-        // active systems one replay behind so the queue never drains.
-        const int max_replays = (2 * max_iter + 32) / GRAPH_ITERS + 2;
-        volatile int *flags = ctx->h_flags;
+        P->per_iter = per_iter;
+        return CFEM_OK;
+    }
+    const unsigned max_rounds = (unsigned)((2 * max_iter + 32) / GRAPH_ITERS + 2);
+    CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
+    CFEM_CUDA(cudaMemsetAsync(P->ws_state, 0, P->state_bytes, w));
+    k_plan_start<<<1, 32, 0, w>>>(d_bar, n_systems);
+    k_pcg_init<<<grid_for((int64_t)n_chunks * 32, 256), 256, 0, w>>>(
+        d_sys, d_st, P->d_chunks, n_chunks, d_bar);
+    CFEM_TRY(iteration(w, false, P->tev[0][0], P->tev[0][1]));
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t cap = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CFEM_CUDA(cudaStreamGetCaptureInfo(w, &cst, nullptr, &cap, &deps, &ndeps));
+    cudaGraphConditionalHandle handle;
+    CFEM_CUDA(cudaGraphConditionalHandleCreate(&handle, cap, 1, cudaGraphCondAssignDefault));
+    k_loop_cond<<<1, 32, 0, w>>>(handle, d_bar, max_rounds);
+    CFEM_CUDA(cudaStreamGetCaptureInfo(w, &cst, nullptr, &cap, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop;
+    CFEM_CUDA(cudaGraphAddNode(&loop, cap, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CFEM_CUDA(cudaStreamUpdateCaptureDependencies(w, &loop, 1, cudaStreamSetCaptureDependencies));
+    CFEM_CUDA(cudaStreamBeginCaptureToGraph(P->w2, body, nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < GRAPH_ITERS; ++it) CFEM_TRY(iteration(P->w2, it == 0, nullptr, nullptr));
+    k_loop_cond<<<1, 32, 0, P->w2>>>(handle, d_bar, max_rounds);
+    cudaGraph_t body_out = nullptr;
+    CFEM_CUDA(cudaStreamEndCapture(P->w2, &body_out));
+    cudaError_t ce = cudaStreamEndCapture(w, &P->graph);
+    CFEM_CUDA(ce);
+    CFEM_CUDA(cudaGetLastError());
+    CFEM_CUDA(cudaGraphInstantiate(&P->exec, P->graph, 0));
+    P->per_iter = per_iter;
+    return CFEM_OK;
+}
+
+static int plan_run(cfem_pcg_plan *P, cfem_solve_stats *stats, cudaStream_t s) {
+    const int n_systems = P->n_systems;
+    cudaStream_t w = P->w;
+    SysDev *d_sys = P->d_sys;
+    SysState *d_st = P->d_st;
+    GridBar *d_bar = P->d_bar;
+    int n_chunks = P->n_chunks;
+    int max_steps = 3 * P->max_iter + 16;
+    double spmv_ms = 0.0;
+    int spmv_samples = 0;
+    // The plan's stream runs after everything queued so far on s.
+    CFEM_CUDA(cudaEventRecord(P->ev[0], s));
+    CFEM_CUDA(cudaStreamWaitEvent(w, P->ev[0], 0));
+    if (P->persistent || P->polled) {
+        CFEM_CUDA(cudaMemsetAsync(P->ws_state, 0, P->state_bytes, w));
+        P->h_flags[2] = n_systems;
+        CFEM_CUDA(cudaMemcpyAsync(&d_bar->active, &P->h_flags[2], sizeof(int),
+                                  cudaMemcpyHostToDevice, w));
+        CFEM_CUDA(cudaEventRecord(P->ev[2], w));
+        CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, w,
+                    d_sys, d_st, P->d_chunks, n_chunks, d_bar);
+    }
+    if (P->persistent) {
+        void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&P->d_chunks,
+                        (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
+        CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(P->grid),
+                                              dim3(SOLVE_THREADS), args, 0, w));
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    } else if (P->polled) {
+        const int max_replays = (2 * P->max_iter + 32) / POLL_ITERS + 2;
+        volatile int *flags = P->h_flags;
         flags[0] = flags[1] = 1;
-        int rep = 0;
-        for (; rep < max_replays; ++rep) {
-            CFEM_CUDA(cudaGraphLaunch(exec[rep & 1], w));
-            g_launches.fetch_add((int64_t)per_iter * GRAPH_ITERS, std::memory_order_relaxed);
-            CFEM_CUDA(cudaMemcpyAsync((void *)&ctx->h_flags[rep & 1], &d_bar->active,
+        int active_before = n_systems;
+        for (int rep = 0; rep < max_replays; ++rep) {
+            CFEM_CUDA(cudaGraphLaunch(P->pexec[rep & 1], w));
+            g_launches.fetch_add((int64_t)P->per_iter * POLL_ITERS, std::memory_order_relaxed);
+            CFEM_CUDA(cudaMemcpyAsync((void *)&P->h_flags[rep & 1], &d_bar->active,
                                       sizeof(int), cudaMemcpyDeviceToHost, w));
-            CFEM_CUDA(cudaEventRecord(ctx->ev[rep & 1], w));
+            CFEM_CUDA(cudaEventRecord(P->ev[rep & 1], w));
             if (rep >= 1) {
                 const int prev = (rep - 1) & 1;
-                CFEM_CUDA(cudaEventSynchronize(ctx->ev[prev]));
+                CFEM_CUDA(cudaEventSynchronize(P->ev[prev]));
                 float sms = 0.0f;
-                if (cudaEventElapsedTime(&sms, ctx->tev[prev][0], ctx->tev[prev][1]) ==
+                if (cudaEventElapsedTime(&sms, P->tev[prev][0], P->tev[prev][1]) ==
                         cudaSuccess) {
-                    if (flags[prev] > 0) {
+                    if (active_before > 0) {
                         spmv_ms += sms;
                         ++spmv_samples;
                     }
                 } else {
                     (void)cudaGetLastError();   // timing is best effort
                 }
+                active_before = flags[prev];
                 if (flags[prev] <= 0) break;
             }
         }
-        CFEM_CUDA(cudaStreamSynchronize(w));
-        for (int gi = 0; gi < 2; ++gi) {
-            cudaGraphExecDestroy(exec[gi]);
-            cudaGraphDestroy(graph[gi]);
-        }
+    } else {
+        CFEM_CUDA(cudaEventRecord(P->ev[2], w));
+        CFEM_CUDA(cudaGraphLaunch(P->exec, w));
     }
-    CFEM_CUDA(cudaEventRecord(ctx->ev[3], w));
-    CFEM_CUDA(cudaEventRecord(ctx->ev[0], w));
-    CFEM_CUDA(cudaStreamWaitEvent(s, ctx->ev[0], 0));
+    CFEM_CUDA(cudaEventRecord(P->ev[3], w));
     std::vector<SysState> hst(n_systems);
     int h_err = 0;
     CFEM_CUDA(cudaMemcpyAsync(hst.data(), d_st, n_systems * sizeof(SysState),
-                              cudaMemcpyDeviceToHost, s));
+                              cudaMemcpyDeviceToHost, w));
     CFEM_CUDA(cudaMemcpyAsync(&h_err, &d_bar->err, sizeof(int),
-                              cudaMemcpyDeviceToHost, s));
-    tmp_free(ws, s);
-    CFEM_CUDA(cudaStreamSynchronize(s));
+                              cudaMemcpyDeviceToHost, w));
+    CFEM_CUDA(cudaStreamSynchronize(w));
+    // later work on s sees the solution
+    CFEM_CUDA(cudaEventRecord(P->ev[0], w));
+    CFEM_CUDA(cudaStreamWaitEvent(s, P->ev[0], 0));
     float kms = 0.0f;
-    CFEM_CUDA(cudaEventElapsedTime(&kms, ctx->ev[2], ctx->ev[3]));
+    CFEM_CUDA(cudaEventElapsedTime(&kms, P->ev[2], P->ev[3]));
+    if (!P->persistent && !P->polled) {
+        unsigned rounds = 0;
+        CFEM_CUDA(cudaMemcpy(&rounds, &d_bar->rounds, sizeof(unsigned),
+                             cudaMemcpyDeviceToHost));
+        const int64_t bodies = rounds > 0 ? (int64_t)rounds - 1 : 0;
+        g_launches.fetch_add(3 + P->per_iter + bodies * (GRAPH_ITERS * P->per_iter + 1),
+                             std::memory_order_relaxed);
+        float sms = 0.0f;
+        if (cudaEventElapsedTime(&sms, P->tev[0][0], P->tev[0][1]) == cudaSuccess) {
+            spmv_ms += sms;
+            ++spmv_samples;
+        } else {
+            (void)cudaGetLastError();   // timing is best effort
+        }
+    }
     for (int i = 0; i < n_systems; ++i) {
         stats[i].status = hst[i].status;
         if (hst[i].status == CFEM_OK && hst[i].phase != PH_DONE)
@@ -1589,6 +1905,63 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
     return CFEM_OK;
+}
+
+}  // namespace cfem
+
+extern "C" int cfem_pcg_plan_create(cfem_ctx *ctx, const cfem_linsys *systems,
+                                    int32_t n_systems, void *stream,
+                                    cfem_pcg_plan **out) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && systems && out && n_systems > 0, CFEM_ERR_INVALID,
+               "cfem_pcg_plan_create: bad args");
+    *out = nullptr;
+    CFEM_TRY(set_device(ctx->device));
+    cfem_pcg_plan *P = new cfem_pcg_plan();
+    const int st = plan_build(ctx, systems, n_systems, (cudaStream_t)stream, P);
+    if (st != CFEM_OK) {
+        plan_free(P);
+        return st;
+    }
+    *out = P;
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_plan_refresh(cfem_pcg_plan *plan, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(plan, CFEM_ERR_INVALID, "cfem_pcg_plan_refresh: plan is NULL");
+    CFEM_TRY(set_device(plan->device));
+    return plan_copies(plan, (cudaStream_t)stream);
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_plan_solve(cfem_pcg_plan *plan, cfem_solve_stats *stats,
+                                   void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(plan && stats, CFEM_ERR_INVALID, "cfem_pcg_plan_solve: bad args");
+    CFEM_TRY(set_device(plan->device));
+    return plan_run(plan, stats, (cudaStream_t)stream);
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_plan_destroy(cfem_pcg_plan *plan) {
+    plan_free(plan);
+    return CFEM_OK;
+}
+
+extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
+                              int32_t n_systems, cfem_solve_stats *stats,
+                              void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && systems && stats && n_systems > 0, CFEM_ERR_INVALID,
+               "cfem_pcg_solve: bad args");
+    CFEM_TRY(set_device(ctx->device));
+    cfem_pcg_plan *P = new cfem_pcg_plan();
+    int st = plan_build(ctx, systems, n_systems, (cudaStream_t)stream, P);
+    if (st == CFEM_OK) st = plan_run(P, stats, (cudaStream_t)stream);
+    plan_free(P);
+    return st;
     CFEM_API_END
 }
 

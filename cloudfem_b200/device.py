@@ -419,6 +419,51 @@ def pcg(systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None,
     return [SolveResult(s) for s in stats]
 
 
+class PcgPlan:
+    """Set-up of a batch solve kept for repeated solves (time steps, a
+    serving loop): working copies of the matrices, solver vectors and the
+    captured iteration graphs stay on the device. Each solve() starts from
+    the current contents of every system's b and x. After changing matrix
+    values in place, call refresh()."""
+
+    def __init__(self, systems, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None,
+                 reliable_delta=0.0, max_stall=0):
+        if not systems:
+            raise ValueError("a plan needs at least one system")
+        self.rt = systems[0].rt
+        self.systems = list(systems)        # keeps the device arrays alive
+        arr = (N.LinSys * len(systems))()
+        for i, sy in enumerate(systems):
+            mi = max_iter if max_iter is not None else max(
+                1000, 20 * int(np.sqrt(sy.n_rows * sy.bs)) + 2000)
+            arr[i] = sy.linsys(mode, rtol, mi, reliable_delta, max_stall)
+        self._arr = arr
+        self._stats = (N.SolveStats * len(systems))()
+        h = N._vp()
+        N.check(self.rt.lib.cfem_pcg_plan_create(self.rt.ctx, arr, len(systems),
+                                                 self.rt.stream(), ctypes.byref(h)))
+        self.handle = h
+
+    def refresh(self):
+        N.check(self.rt.lib.cfem_pcg_plan_refresh(self.handle, self.rt.stream()))
+
+    def solve(self):
+        N.check(self.rt.lib.cfem_pcg_plan_solve(self.handle, self._stats,
+                                                self.rt.stream()))
+        return [SolveResult(st) for st in self._stats]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.rt.lib.cfem_pcg_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
 def pcg_noalloc(system, mode=N.SOLVE_FP64, rtol=1e-12, max_iter=None):
     """Solve one BlockSystem without any device allocation by the library.
 

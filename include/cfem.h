@@ -136,14 +136,20 @@ CFEM_API int cfem_version(void);
 CFEM_API int cfem_ctx_create(int device, cfem_ctx **out);
 CFEM_API int cfem_ctx_destroy(cfem_ctx *ctx);
 /* How cfem_pcg_solve runs its iterations:
- * PERSISTENT - one cooperative launch, grid barrier between phases (lowest
- *              latency when the whole batch fits in one wave of warps);
- * GRAPH      - two kernels per iteration (SpMV phase, update phase) with a
- *              warp per row chunk, replayed from a CUDA graph of 16
- *              iterations; the host polls convergence once per replay;
- * AUTO       - PERSISTENT when all row chunks fit in one resident wave,
- *              else GRAPH (default). */
-enum { CFEM_SCHED_AUTO = 0, CFEM_SCHED_PERSISTENT = 1, CFEM_SCHED_GRAPH = 2 };
+ * PERSISTENT    - one cooperative launch, grid barrier between phases
+ *                 (lowest latency when the whole batch fits in one wave);
+ * GRAPH         - per-phase kernels with a warp per row chunk (direction,
+ *                 SpMV, reduction, update, reduction per iteration); the
+ *                 whole solve is ONE CUDA graph launch whose device-side
+ *                 WHILE node repeats 2-iteration bodies until no system is
+ *                 active (no host polling);
+ * GRAPH_POLLED  - the same kernels replayed from plain graphs of 16
+ *                 iterations, the host polling convergence once per replay
+ *                 (every launch visible to per-launch profilers);
+ * AUTO          - PERSISTENT when all row chunks fit in one resident wave,
+ *                 else GRAPH (default). */
+enum { CFEM_SCHED_AUTO = 0, CFEM_SCHED_PERSISTENT = 1, CFEM_SCHED_GRAPH = 2,
+       CFEM_SCHED_GRAPH_POLLED = 3 };
 CFEM_API int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler);
 /* The library's device memory (patterns, solver workspaces, sort buffers)
  * comes from one stream-ordered pool per GPU that keeps what it has mapped,
@@ -281,17 +287,39 @@ CFEM_API int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
                                void *stream);
 
 /* ---- solver -------------------------------------------------------------
- * Jacobi-preconditioned CG on a batch of independent systems in ONE
- * persistent cooperative launch (two grid barriers per iteration, per-
- * system scalars reduced in a fixed order, so each result is bitwise the
- * same alone and in any batch). CFEM_SOLVE_MIXED runs the CG in FP32 and
- * keeps FP64 for the true residual r = b - A x, the solution update and
- * the convergence test (reliable updates). Replaces spla.spsolve /
- * spla.factorized (tet_poisson.py:121, tet10.py:177, elastic3d.py:230).
- * Writes one stats record per system. Synchronises. Returns CFEM_OK when
- * the launch ran; per-system outcomes are in stats[i].status. */
+ * Jacobi-preconditioned CG on a batch of independent systems. Batches whose
+ * work fits one resident wave run in ONE persistent cooperative launch (two
+ * grid barriers per iteration); larger ones replay captured CUDA graphs of
+ * 16 iterations (direction update, SpMV, reduction, update, reduction per
+ * iteration). Per-system scalars are reduced in a fixed order, so each
+ * result is bitwise the same alone and in any batch on a given scheduler.
+ * CFEM_SOLVE_MIXED runs the CG in FP32 and keeps FP64 for the true residual
+ * r = b - A x, the solution update and the convergence test (reliable
+ * updates). Replaces spla.spsolve / spla.factorized (tet_poisson.py:121,
+ * tet10.py:177, elastic3d.py:230). Writes one stats record per system.
+ * Synchronises. Returns CFEM_OK when the solve ran; per-system outcomes are
+ * in stats[i].status. Equivalent to plan create + solve + destroy. */
 CFEM_API int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
                    int32_t n_systems, cfem_solve_stats *stats, void *stream);
+
+/* Solve plans: the set-up of cfem_pcg_solve kept for repeated solves of the
+ * same systems (time steps, serving), as spla.factorized is kept by
+ * tet_heat.py:254 and tet10.py:524. Create captures the systems' device
+ * pointers, options and working copies of the matrix values and builds the
+ * iteration graphs; each solve re-initialises the solver state from the
+ * current contents of b, x (initial guess with Dirichlet values) and the
+ * fixed mask. After changing matrix values in place, call refresh before
+ * the next solve. A plan has its own stream, events and workspace: plans of
+ * one context may be solved from different host threads at the same time.
+ * Destroy waits for the plan's work. */
+typedef struct cfem_pcg_plan cfem_pcg_plan;
+CFEM_API int cfem_pcg_plan_create(cfem_ctx *ctx, const cfem_linsys *systems,
+                                  int32_t n_systems, void *stream,
+                                  cfem_pcg_plan **out);
+CFEM_API int cfem_pcg_plan_refresh(cfem_pcg_plan *plan, void *stream);
+CFEM_API int cfem_pcg_plan_solve(cfem_pcg_plan *plan, cfem_solve_stats *stats,
+                                 void *stream);
+CFEM_API int cfem_pcg_plan_destroy(cfem_pcg_plan *plan);
 
 /* Allocation-free variant of cfem_pcg_solve for ONE system. It has no
  * counterpart in the reference, which only solves on the host with SciPy.

@@ -162,7 +162,7 @@ def test_graph_scheduler_matches_persistent(torch, bs, mode):
     rtol = 1e-12 if mode == "fp64" else 1e-10
     out = {}
     try:
-        for sched in (N.SCHED_PERSISTENT, N.SCHED_GRAPH):
+        for sched in (N.SCHED_PERSISTENT, N.SCHED_GRAPH, N.SCHED_GRAPH_POLLED):
             N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, sched))
             x = x0.clone()
             r = pcg([make(x)], md, rtol, 20000)[0]
@@ -170,6 +170,37 @@ def test_graph_scheduler_matches_persistent(torch, bs, mode):
             out[sched] = x.cpu().numpy()
     finally:
         N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, N.SCHED_AUTO))
-    a, b = out[N.SCHED_PERSISTENT], out[N.SCHED_GRAPH]
+    a = out[N.SCHED_PERSISTENT]
     tol = 1e-10 if mode == "fp64" else 1e-8
-    assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
+    for sched in (N.SCHED_GRAPH, N.SCHED_GRAPH_POLLED):
+        b = out[sched]
+        assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
+    # device-looped and host-polled graphs run the same kernels in order
+    assert np.array_equal(out[N.SCHED_GRAPH], out[N.SCHED_GRAPH_POLLED])
+
+
+def test_plan_repeated_solves_match_one_shot(torch):
+    """A solve plan reused for several right-hand sides gives, each time,
+    bitwise the answer of a one-shot solve of the same system."""
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import PcgPlan, pcg
+    dm, sysm = _poisson_system(torch, 6, seed=5)
+    x0 = sysm.x.clone()
+    b0 = sysm.b.clone()
+    for sched in (N.SCHED_PERSISTENT, N.SCHED_GRAPH, N.SCHED_GRAPH_POLLED):
+        N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, sched))
+        try:
+            plan = PcgPlan([sysm], N.SOLVE_MIXED, 1e-10, 5000)
+            for scale in (1.0, -2.5, 0.75):
+                sysm.b.copy_(b0 * scale)
+                sysm.x.copy_(x0)
+                r1 = plan.solve()[0]
+                x_plan = sysm.x.clone()
+                sysm.x.copy_(x0)
+                r2 = pcg([sysm], N.SOLVE_MIXED, 1e-10, 5000)[0]
+                assert r1.status == N.CFEM_OK and r2.status == N.CFEM_OK
+                assert r1.iterations == r2.iterations
+                assert torch.equal(x_plan, sysm.x)
+            plan.close()
+        finally:
+            N.check(dm.rt.lib.cfem_ctx_set_scheduler(dm.rt.ctx, N.SCHED_AUTO))
