@@ -26,6 +26,7 @@ CFEM_ERR_UNSUPPORTED = 7
 
 OP_P1_STIFF, OP_P1_MASS, OP_T10_STIFF, OP_T10_MASS = 1, 2, 3, 4
 OP_P1_ELAST, OP_T10_ELAST = 5, 6
+OP_T10_CURLCURL, OP_T10_NGRAD_X, OP_T10_NGRAD_Y, OP_T10_NGRAD_Z = 7, 8, 9, 10
 COEF_CONST, COEF_ELEM, COEF_QP, COEF_NODAL = 0, 1, 2, 3
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK = 0, 1
@@ -94,6 +95,8 @@ SIGNATURES = [
     ("cfem_assemble", ctypes.c_int,
      [_vp, _vp, _i32, _vp, _vp, ctypes.POINTER(Coef), ctypes.POINTER(Coef),
       _vp, _vp, _i32, _vp]),
+    ("cfem_assemble_curlcurl", ctypes.c_int,
+     [_vp, _vp, _vp, _vp, Coef, _vp, ctypes.c_int, _vp]),
     ("cfem_assemble_batch", ctypes.c_int,
      [_vp, _i32, ctypes.POINTER(AssemblyJob), _i32, _vp]),
     ("cfem_assemble_elastic", ctypes.c_int,

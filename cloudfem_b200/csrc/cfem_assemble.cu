@@ -319,7 +319,21 @@ __device__ __forceinline__ void t10_scalar_elem(const double *__restrict__ nodes
                                                 double *fe, double (*sG)[10][3],
                                                 int lane) {
     const int32_t *el = elems + e * 10;
-    if (OP == CFEM_OP_T10_STIFF) {
+    if (OP == CFEM_OP_T10_NGRAD_X || OP == CFEM_OP_T10_NGRAD_Y || OP == CFEM_OP_T10_NGRAD_Z) {
+        // ke[p][j] = (sigma V) sum_q w_q N_qp dN_j/dx_m (em3d_tet10.py:225)
+        constexpr int m = OP - CFEM_OP_T10_NGRAD_X;
+        double vol;
+        t10_stage_grads(nodes, el, sG, lane, vol);
+        const double sv = coef_at(coef, e, 0) * vol;
+        for (int t = lane; t < 100; t += 32) {
+            int a = t / 10, b = t - (t / 10) * 10;
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s += c_wq[q] * c_N[q][a] * sG[q][b][m];
+            ke[t] = sv * s;
+        }
+        __syncwarp();
+    } else if (OP == CFEM_OP_T10_STIFF) {
         double vol;
         t10_stage_grads(nodes, el, sG, lane, vol);
         double wk[5];
@@ -427,6 +441,46 @@ k_t10_elastic(const double *__restrict__ nodes, const int32_t *__restrict__ elem
             }
         }
         fe[e * 30 + lane] = vol * sb + vol * st;
+    }
+}
+
+// Tet10 nodal curl-curl: block (a,b) = (nu V) sum_q w_q ((g_a.g_b) I - g_b g_a^T),
+// the Levi-Civita contraction of em3d_tet10.py:205-208 in closed form.
+__global__ void __launch_bounds__(32 * T10_WARPS)
+k_t10_curlcurl(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
+               int64_t M, Coef nu, double *__restrict__ ke) {
+    __shared__ double sG[T10_WARPS][5][10][3];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t e = (int64_t)blockIdx.x * T10_WARPS + w;
+    if (e >= M) return;
+    const int32_t *el = elems + e * 10;
+    double vol;
+    t10_stage_grads(nodes, el, sG[w], lane, vol);
+    const double sv = coef_at(nu, e, 0) * vol;
+    for (int t = lane; t < 100; t += 32) {
+        int a = t / 10, b = t - (t / 10) * 10;
+        double blk[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) blk[v] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double wq = c_wq[q];
+            double ga[3], gb[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                ga[c] = sG[w][q][a][c];
+                gb[c] = sG[w][q][b][c];
+            }
+            const double dot = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    blk[c * 3 + d] += wq * ((c == d ? dot : 0.0) - ga[d] * gb[c]);
+        }
+        double *dst = ke + (e * 100 + t) * 9;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) dst[v] = sv * blk[v];
     }
 }
 
@@ -622,11 +676,15 @@ int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
     CFEM_CHECK(ctx && p && d_nodes && d_elems && d_vals, CFEM_ERR_INVALID,
                "cfem_assemble: NULL argument");
     const bool p1 = (op == CFEM_OP_P1_STIFF || op == CFEM_OP_P1_MASS);
-    const bool t10 = (op == CFEM_OP_T10_STIFF || op == CFEM_OP_T10_MASS);
+    const bool ngrad = (op >= CFEM_OP_T10_NGRAD_X && op <= CFEM_OP_T10_NGRAD_Z);
+    const bool t10 = (op == CFEM_OP_T10_STIFF || op == CFEM_OP_T10_MASS || ngrad);
     CFEM_CHECK(p1 || t10, CFEM_ERR_INVALID, "cfem_assemble: unknown op %d", op);
     CFEM_CHECK(p->npe == (p1 ? 4 : 10), CFEM_ERR_INVALID,
                "operator %d needs %d-node elements, pattern has %d", op,
                p1 ? 4 : 10, p->npe);
+    CFEM_CHECK(!ngrad || !coef || coef->mode == CFEM_COEF_CONST ||
+                   coef->mode == CFEM_COEF_ELEM,
+               CFEM_ERR_INVALID, "coupling operators take a constant or per-element coefficient");
     CFEM_TRY(check_coef(coef, op == CFEM_OP_T10_STIFF, "coef"));
     CFEM_TRY(check_coef(load, op == CFEM_OP_T10_STIFF, "load"));
     CFEM_CHECK(!coef || coef->mode != CFEM_COEF_NODAL, CFEM_ERR_INVALID,
@@ -663,6 +721,18 @@ int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
         case CFEM_OP_T10_STIFF:
             CFEM_LAUNCH(k_t10_scalar<CFEM_OP_T10_STIFF>, grid_for(M, T10_WARPS),
                         32 * T10_WARPS, 0, s, d_nodes, d_elems, M, kc, lc, ke, fe);
+            break;
+        case CFEM_OP_T10_NGRAD_X:
+            CFEM_LAUNCH(k_t10_scalar<CFEM_OP_T10_NGRAD_X>, grid_for(M, T10_WARPS),
+                        32 * T10_WARPS, 0, s, d_nodes, d_elems, M, kc, lc, ke, nullptr);
+            break;
+        case CFEM_OP_T10_NGRAD_Y:
+            CFEM_LAUNCH(k_t10_scalar<CFEM_OP_T10_NGRAD_Y>, grid_for(M, T10_WARPS),
+                        32 * T10_WARPS, 0, s, d_nodes, d_elems, M, kc, lc, ke, nullptr);
+            break;
+        case CFEM_OP_T10_NGRAD_Z:
+            CFEM_LAUNCH(k_t10_scalar<CFEM_OP_T10_NGRAD_Z>, grid_for(M, T10_WARPS),
+                        32 * T10_WARPS, 0, s, d_nodes, d_elems, M, kc, lc, ke, nullptr);
             break;
         default:
             CFEM_LAUNCH(k_t10_scalar<CFEM_OP_T10_MASS>, grid_for(M, T10_WARPS),
@@ -847,6 +917,37 @@ int cfem_assemble_elastic(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
     int st = reduce_all(p, 3, ke, fe, d_vals, d_rhs, accumulate, ctx->num_sms, s);
     tmp_free(ke, s);
     tmp_free(fe, s);
+    return st;
+    CFEM_API_END
+}
+
+int cfem_assemble_curlcurl(cfem_ctx *ctx, const cfem_pattern *p,
+                           const double *d_nodes, const int32_t *d_elems,
+                           cfem_coef nu, double *d_vals, int accumulate,
+                           void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && p && d_nodes && d_elems && d_vals, CFEM_ERR_INVALID,
+               "cfem_assemble_curlcurl: NULL argument");
+    CFEM_CHECK(p->npe == 10, CFEM_ERR_INVALID,
+               "curl-curl needs 10-node elements, pattern has %d", p->npe);
+    CFEM_CHECK(nu.mode == CFEM_COEF_CONST || (nu.mode == CFEM_COEF_ELEM && nu.d_values),
+               CFEM_ERR_INVALID, "nu must be constant or per element");
+    CFEM_CHECK(((uintptr_t)d_elems & 15) == 0, CFEM_ERR_INVALID,
+               "element array must be 16-byte aligned");
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t M = p->n_elems;
+    if (M == 0) {
+        if (p->nnz && !accumulate)
+            CFEM_CUDA(cudaMemsetAsync(d_vals, 0, p->nnz * 9 * sizeof(double), s));
+        return CFEM_OK;
+    }
+    double *ke = nullptr;
+    CFEM_TRY(tmp_alloc(&ke, M * 100 * 9, s));
+    CFEM_LAUNCH(k_t10_curlcurl, grid_for(M, T10_WARPS), 32 * T10_WARPS, 0, s,
+                d_nodes, d_elems, M, to_coef(&nu), ke);
+    int st = reduce_all(p, 3, ke, nullptr, d_vals, nullptr, accumulate, ctx->num_sms, s);
+    tmp_free(ke, s);
     return st;
     CFEM_API_END
 }

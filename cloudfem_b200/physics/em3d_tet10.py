@@ -1,0 +1,190 @@
+"""Tet10 nodal A-V eddy-current blocks on the GPU.
+
+Drop-in for the assembly of cloudfem/physics/em3d_tet10.py:
+
+* ``assemble_tet10_av`` (:172-264): real blocks K (curl-curl, nu), M (sigma
+  vector mass with the gauge conductivity in air), G (A-V coupling) and
+  S (sigma scalar stiffness on the conductor V nodes), plus v_nodes, the
+  per-element conductivity and the conducting mask;
+* ``_assemble_curl_curl_tet10_nu`` (:746-771): K alone for per-element nu
+  (rebuilt at every Picard step of the nonlinear solver, :938).
+
+Element matrices are computed by warp-per-element kernels (Keast-5
+gradients staged in shared memory) and summed into the node pattern by the
+deterministic segmented reduction: K is a 3x3-block curl-curl operator on
+the mesh pattern, M and S reuse the scalar Tet10 mass and stiffness kernels
+with per-element coefficients, G the N_p dN_j/dx_m coupling kernels (one per
+component m), S and G on the pattern of the conducting elements. The
+conductor components (one pinned node each, :140-169) are found with a
+connected-components pass on the host. Returned matrices are SciPy CSR with
+the reference's sorted, canonical structure.
+"""
+
+import ctypes
+import types
+
+import numpy as np
+import scipy.sparse as sp
+from scipy.sparse.csgraph import connected_components
+
+from .. import _native as N
+from ..device import DeviceMesh, centroids, evaluate, ptr
+
+MU0 = 4e-7 * np.pi
+
+__all__ = ["assemble_tet10_av", "MU0"]
+
+
+def _element_values(mesh, q):
+    """Float or callable(x, y, z) at element centroids, (M,) float."""
+    els = np.asarray(mesh.elements)
+    v = evaluate(q, centroids(np.asarray(mesh.nodes, dtype=float), els))
+    return np.full(len(els), float(v)) if np.isscalar(v) else np.asarray(v, dtype=float)
+
+
+def _conductor_components(mesh, conducting):
+    """V-node ids: the nodes of conducting elements minus the smallest node
+    of each connected conductor part (em3d_tet10.py:140-169)."""
+    els = np.asarray(mesh.elements)[conducting]
+    if els.size == 0:
+        return np.zeros(0, dtype=int)
+    cond_nodes = np.unique(els)
+    local = np.searchsorted(cond_nodes, els)
+    npe = els.shape[1]
+    rows = np.repeat(local[:, :1], npe - 1, axis=1).ravel()
+    cols = local[:, 1:].ravel()
+    g = sp.coo_matrix((np.ones(len(rows)), (rows, cols)),
+                      shape=(len(cond_nodes), len(cond_nodes)))
+    _, label = connected_components(g, directed=False)
+    pinned = np.zeros(len(cond_nodes), dtype=bool)
+    first = np.full(label.max() + 1, len(cond_nodes))
+    np.minimum.at(first, label, np.arange(len(cond_nodes)))
+    pinned[first] = True                   # smallest node id of each part
+    return cond_nodes[~pinned].astype(int)
+
+
+def _coef(dm, values):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(values, dtype=float)).to(dm.rt.device)
+    return N.Coef(ptr(t), 0.0, N.COEF_ELEM, 0), t
+
+
+def _sub_mesh(mesh, sel):
+    return types.SimpleNamespace(nodes=mesh.nodes,
+                                 elements=np.asarray(mesh.elements)[sel],
+                                 boundaries={}, n_nodes=mesh.n_nodes)
+
+
+def _scalar_csr(dm, op, values):
+    """Node-level CSR (indptr, indices, data) of one scalar operator with a
+    per-element coefficient on dm's pattern (host arrays)."""
+    import torch
+    pat = dm.pattern
+    coef, keep = _coef(dm, values)
+    vals = torch.empty(max(pat.nnz, 1), dtype=torch.float64, device=dm.rt.device)
+    N.check(dm.rt.lib.cfem_assemble(dm.rt.ctx, pat.handle, op, ptr(dm.nodes),
+                                    ptr(dm.elems), ctypes.byref(coef), None,
+                                    ptr(vals), None, 0, dm.rt.stream()))
+    indptr, indices = pat.expand(1)
+    del keep
+    return (indptr.cpu().numpy().astype(np.int64), indices.cpu().numpy(),
+            vals[: pat.nnz].cpu().numpy())
+
+
+def _componentwise(indptr, indices, datas, n_rows, col_map=None):
+    """CSR with row 3p+m holding row p of the node-level CSR for component m
+    (data datas[m]); columns 3j+m, or col_map[j] (entries with col_map < 0
+    dropped) when given."""
+    lens_node = np.diff(indptr)
+    row_of = np.repeat(np.arange(n_rows), lens_node)
+    if col_map is None:
+        keep = np.ones(len(indices), dtype=bool)
+    else:
+        keep = col_map[indices] >= 0
+    kept_per_row = np.bincount(row_of[keep], minlength=n_rows)
+    lens = np.repeat(kept_per_row, 3)
+    out_ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    k_rows = row_of[keep]
+    k_idx = indices[keep].astype(np.int64)
+    # rank of each kept entry within its node row
+    start_kept = np.concatenate([[0], np.cumsum(kept_per_row)])[:-1]
+    rank = np.arange(len(k_rows)) - start_kept[k_rows]
+    out_idx = np.empty(lens.sum(), dtype=np.int64)
+    out_dat = np.empty(lens.sum(), dtype=float)
+    for m in range(3):
+        pos = out_ptr[3 * k_rows + m] + rank
+        out_idx[pos] = (3 * k_idx + m) if col_map is None else col_map[k_idx]
+        out_dat[pos] = datas[m][keep]
+    return out_ptr, out_idx, out_dat
+
+
+def _csr(ptr_, idx, dat, shape):
+    return sp.csr_matrix((dat, idx.astype(np.int32), ptr_.astype(np.int32)),
+                         shape=shape)
+
+
+def _curl_curl(dm, nu_e):
+    import torch
+    pat = dm.pattern
+    coef, keep = _coef(dm, nu_e)
+    vals = torch.empty(max(pat.nnz * 9, 1), dtype=torch.float64, device=dm.rt.device)
+    N.check(dm.rt.lib.cfem_assemble_curlcurl(dm.rt.ctx, pat.handle, ptr(dm.nodes),
+                                             ptr(dm.elems), coef, ptr(vals), 0,
+                                             dm.rt.stream()))
+    del keep
+    return pat.to_scipy(3, vals[: pat.nnz * 9])
+
+
+def _assemble_curl_curl_tet10_nu(mesh, nu_e):
+    """K (3N, 3N) of the curl-curl operator for per-element nu."""
+    nu_e = np.asarray(nu_e, dtype=float)
+    if nu_e.shape != (len(mesh.elements),):
+        raise ValueError("nu_e needs one value per element")
+    return _curl_curl(DeviceMesh(mesh), nu_e)
+
+
+def assemble_tet10_av(mesh, nu=1.0 / MU0, sigma=0.0, gauge_eps=1e-6):
+    """Real blocks of the Tet10 nodal A-V system:
+    (K, M, G, S, v_nodes, sig_e, conducting), as the reference returns."""
+    n = mesh.n_nodes
+    els = np.asarray(mesh.elements)
+    if els.ndim != 2 or els.shape[1] != 10:
+        raise ValueError("assemble_tet10_av needs a Tet10 mesh")
+    nu_e = _element_values(mesh, nu)
+    sig_e = _element_values(mesh, sigma)
+    conducting = sig_e > 0.0
+    sig_max = sig_e.max() if conducting.any() else 0.0
+    sig_reg = gauge_eps * sig_max
+    v_nodes = _conductor_components(mesh, conducting)
+    n_v = len(v_nodes)
+    v_col = np.full(n, -1, dtype=np.int64)
+    v_col[v_nodes] = np.arange(n_v)
+
+    dm = DeviceMesh(mesh)
+    K = _curl_curl(dm, nu_e)
+
+    seff = np.where(conducting, sig_e, sig_reg)
+    msel = seff > 0.0
+    if msel.any():
+        dmm = dm if msel.all() else DeviceMesh(_sub_mesh(mesh, msel))
+        ip, ix, dv = _scalar_csr(dmm, N.OP_T10_MASS, seff[msel])
+        M = _csr(*_componentwise(ip, ix, [dv, dv, dv], n), (3 * n, 3 * n))
+    else:
+        M = sp.csr_matrix((3 * n, 3 * n))
+
+    if conducting.any() and n_v:
+        dmc = dm if conducting.all() else DeviceMesh(_sub_mesh(mesh, conducting))
+        sc = sig_e[conducting]
+        parts = [_scalar_csr(dmc, op, sc) for op in
+                 (N.OP_T10_NGRAD_X, N.OP_T10_NGRAD_Y, N.OP_T10_NGRAD_Z)]
+        ip, ix = parts[0][0], parts[0][1]
+        Gs = _csr(*_componentwise(ip, ix, [p[2] for p in parts], n, v_col),
+                  (3 * n, n_v))
+        sp_, si, sd = _scalar_csr(dmc, N.OP_T10_STIFF, sc)
+        Sfull = _csr(sp_, si, sd, (n, n))
+        S = Sfull[v_nodes][:, v_nodes].tocsr()
+        S.sort_indices()
+    else:
+        Gs = sp.csr_matrix((3 * n, n_v))
+        S = sp.csr_matrix((n_v, n_v))
+    return K, M, Gs, S, v_nodes, sig_e, conducting

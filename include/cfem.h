@@ -54,7 +54,11 @@ enum {
     CFEM_OP_T10_STIFF = 3,  /* tet10.py:138-165       Keast-5 k G G^T, f N      */
     CFEM_OP_T10_MASS = 4,   /* tet10.py:229-249       rho V MASS_REF            */
     CFEM_OP_P1_ELAST = 5,   /* elastic3d.py:105-169   V B^T D B, body, thermal  */
-    CFEM_OP_T10_ELAST = 6   /* elastic_tet10.py:135-192 Keast-5 B^T D B, ...    */
+    CFEM_OP_T10_ELAST = 6,  /* elastic_tet10.py:135-192 Keast-5 B^T D B, ...    */
+    CFEM_OP_T10_CURLCURL = 7, /* em3d_tet10.py:205-210  nu V sum_q w_q curl.curl */
+    CFEM_OP_T10_NGRAD_X = 8,  /* em3d_tet10.py:225-227  sigma V sum_q w_q N_p dN_j/dx */
+    CFEM_OP_T10_NGRAD_Y = 9,  /*   same, d/dy (A-V coupling block G, one       */
+    CFEM_OP_T10_NGRAD_Z = 10  /*   component of the A DOF per op)              */
 };
 
 /* How a coefficient array is sampled. */
@@ -218,6 +222,17 @@ typedef struct cfem_assembly_job {
 CFEM_API int cfem_assemble_batch(cfem_ctx *ctx, int32_t op,
                                  const cfem_assembly_job *jobs, int32_t n_jobs,
                                  void *stream);
+
+/* Tet10 nodal curl-curl operator (CFEM_OP_T10_CURLCURL), replacing the
+ * element loop of em3d_tet10.py:196-210 and _assemble_curl_curl_tet10_nu
+ * (:746-771): 3x3 block (a, b) = nu_e V sum_q w_q ((g_a . g_b) I - g_b g_a^T)
+ * with g = G_q (grad N x e_m . grad N x e_n summed over curl components),
+ * node-major DOF 3 p + m, into d_vals (nnz * 9) of a bs-3 view of the node
+ * pattern. nu: CFEM_COEF_CONST or CFEM_COEF_ELEM. accumulate: add. */
+CFEM_API int cfem_assemble_curlcurl(cfem_ctx *ctx, const cfem_pattern *p,
+                                    const double *d_nodes, const int32_t *d_elems,
+                                    cfem_coef nu, double *d_vals, int accumulate,
+                                    void *stream);
 
 /* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
  * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),

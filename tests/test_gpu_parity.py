@@ -181,3 +181,48 @@ def test_mixed_precision_matches_fp64(cf):
                                                  rtol=1e-10, **kw))
     err = np.linalg.norm(u32 - u64) / np.linalg.norm(u64)
     assert err <= 1e-8, err
+
+
+# ------------------------------------------------------- Tet10 A-V blocks
+def test_av_blocks_golden(cf, golden):
+    """assemble_tet10_av against the reference's blocks on the golden case
+    (structure bit-exact, values 1e-12 of the largest entry)."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    nx, ny, nz, xl, yl, zl = C.AV_BOX
+    m = cf.mesh.box_mesh_tet10(nx, ny, nz, xlim=xl, ylim=yl, zlim=zl)
+    K, M, Gs, S, v_nodes, sig_e, cond = em.assemble_tet10_av(
+        m, nu=C.nu_fn, sigma=C.sigma_fn, gauge_eps=1e-6)
+    g = golden
+    assert_csr_equal(K, golden_csr(g, "av_K"))
+    assert_csr_equal(M, golden_csr(g, "av_M"))
+    assert_csr_equal(Gs, golden_csr(g, "av_G"))
+    assert_csr_equal(S, golden_csr(g, "av_S"))
+    np.testing.assert_array_equal(v_nodes, g["av_vnodes"])
+    np.testing.assert_array_equal(sig_e, g["av_sig_e"])
+    np.testing.assert_array_equal(cond, g["av_cond"])
+
+
+@pytest.mark.parametrize("gauge", [1e-6, 0.0])
+def test_av_blocks_vs_oracle(cf, gauge):
+    """A larger box with two separate conductors (two pinned V nodes) and,
+    with gauge 0, a mass block restricted to the conductors."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    from oracle import cfem_oracle as O
+
+    def sigma(x, y, z):
+        x = np.asarray(x)
+        return np.where((x < 0.3) | (x > 0.75), 3.5e7, 0.0)
+
+    m = cf.mesh.box_mesh_tet10(6, 3, 2, xlim=(0, 1.5), ylim=(0, 0.5), zlim=(0, 0.4))
+    mo = O.box_mesh_tet10(6, 3, 2, (0, 1.5), (0, 0.5), (0, 0.4))
+    ours = em.assemble_tet10_av(m, nu=C.nu_fn, sigma=sigma, gauge_eps=gauge)
+    ref = O.assemble_tet10_av(mo, nu=C.nu_fn, sigma=sigma, gauge_eps=gauge)
+    for a, b in zip(ours[:4], ref[:4]):
+        assert_csr_equal(a, b)
+    np.testing.assert_array_equal(ours[4], ref[4])
+    np.testing.assert_array_equal(ours[5], ref[5])
+    np.testing.assert_array_equal(ours[6], ref[6])
+    # K alone from per-element nu (the nonlinear solver's rebuild)
+    cen = m.nodes[np.asarray(m.elements)[:, :4]].mean(axis=1)
+    nu_e = np.array([C.nu_fn(*c) for c in cen])
+    assert_csr_equal(em._assemble_curl_curl_tet10_nu(m, nu_e), ref[0])
