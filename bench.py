@@ -424,6 +424,9 @@ def run_c3(args, rank, world, local_rank):
     plain_s = time.perf_counter() - t0
     plain_free = sum(batch.items[i]["free"] for i in range(plain_n))
 
+    # autotuner: element-kernel block shape and solve-loop body length
+    from cloudfem_b200 import autotune
+    tuned = autotune.tune_batch(batch, args.precision, rtol, repeat=2)
     for _ in range(args.warmup):
         step(args.precision)
     torch.cuda.synchronize()
@@ -480,6 +483,7 @@ def run_c3(args, rank, world, local_rank):
             "precision": args.precision, "rtol": rtol,
             "iterations_max": int(max(iters)), "iterations_mean": float(np.mean(iters)),
             "rel_err_vs_fp64_max": err,
+            "autotune": {k: v["best"] for k, v in tuned.items()},
             "plain_fp64_per_mesh": {"meshes": plain_n,
                                     "dof_per_s": plain_free / plain_s},
             "l2": "256 MiB buffer written between timed steps",

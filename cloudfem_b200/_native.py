@@ -31,6 +31,7 @@ COEF_CONST, COEF_ELEM, COEF_QP, COEF_NODAL = 0, 1, 2, 3
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK = 0, 1
 SCHED_AUTO, SCHED_PERSISTENT, SCHED_GRAPH, SCHED_GRAPH_POLLED = 0, 1, 2, 3
+PARAM_T10_WARPS, PARAM_P1_THREADS, PARAM_GRAPH_ITERS = 1, 2, 3
 
 STATUS_NAMES = {
     CFEM_OK: "ok", CFEM_ERR_INVALID: "invalid argument",
@@ -82,6 +83,8 @@ SIGNATURES = [
     ("cfem_ctx_destroy", ctypes.c_int, [_vp]),
     ("cfem_ctx_launch_count", _i64, [_vp]),
     ("cfem_ctx_trim", _i32, [_vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("cfem_ctx_set_param", _i32, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("cfem_ctx_get_param", _i32, [_vp, ctypes.c_int]),
     ("cfem_ctx_set_scheduler", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cfem_pattern_create", ctypes.c_int,
      [_vp, _vp, _i64, _i32, _i64, _vp, ctypes.POINTER(_vp)]),
@@ -183,6 +186,12 @@ class Runtime:
 
     def launches(self):
         return int(self.lib.cfem_ctx_launch_count(self.ctx))
+
+    def set_param(self, param, value):
+        check(self.lib.cfem_ctx_set_param(self.ctx, int(param), int(value)))
+
+    def get_param(self, param):
+        return int(self.lib.cfem_ctx_get_param(self.ctx, int(param)))
 
     def trim(self, keep_bytes=0):
         """Return the library pool's unused device memory beyond keep_bytes

@@ -577,17 +577,35 @@ k_p1_scalar_batch(const AsmJob *__restrict__ jobs, int nj, int64_t M,
                        fe ? fe + g * 4 : nullptr);
 }
 
-template <int OP>
-__global__ void __launch_bounds__(32 * T10_WARPS)
+template <int OP, int W>
+__global__ void __launch_bounds__(32 * W)
 k_t10_scalar_batch(const AsmJob *__restrict__ jobs, int nj, int64_t M,
                    double *__restrict__ ke, double *__restrict__ fe) {
-    __shared__ double sG[T10_WARPS][5][10][3];
+    __shared__ double sG[W][5][10][3];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t g = (int64_t)blockIdx.x * T10_WARPS + w;
+    const int64_t g = (int64_t)blockIdx.x * W + w;
     if (g >= M) return;
     const AsmJob &J = jobs[find_job(jobs, nj, g, 0)];
     t10_scalar_elem<OP>(J.nodes, J.elems, g - J.e0, J.coef, J.load, ke + g * 100,
                         fe ? fe + g * 10 : nullptr, sG[w], lane);
+}
+
+// Elements per block of the batched Tet10 kernel (one warp per element), a
+// launch parameter chosen per context (cfem_ctx_set_param, autotuned).
+template <int OP>
+static int launch_t10_batch(int warps, int64_t M, cudaStream_t s, const AsmJob *jobs,
+                            int nj, double *ke, double *fe) {
+    switch (warps) {
+        case 2:
+            CFEM_LAUNCH((k_t10_scalar_batch<OP, 2>), grid_for(M, 2), 64, 0, s, jobs, nj, M, ke, fe);
+            break;
+        case 8:
+            CFEM_LAUNCH((k_t10_scalar_batch<OP, 8>), grid_for(M, 8), 256, 0, s, jobs, nj, M, ke, fe);
+            break;
+        default:
+            CFEM_LAUNCH((k_t10_scalar_batch<OP, 4>), grid_for(M, 4), 128, 0, s, jobs, nj, M, ke, fe);
+    }
+    return CFEM_OK;
 }
 
 __global__ void k_reduce_vals_batch(const AsmJob *__restrict__ jobs, int nj,
@@ -711,11 +729,13 @@ int cfem_assemble(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
     if (!coef) kc.c = 1.0;
     switch (op) {
         case CFEM_OP_P1_STIFF:
-            CFEM_LAUNCH(k_p1_scalar<CFEM_OP_P1_STIFF>, grid_for(M, 128), 128, 0,
+            CFEM_LAUNCH(k_p1_scalar<CFEM_OP_P1_STIFF>, grid_for(M, ctx->p1_threads),
+                        ctx->p1_threads, 0,
                         s, d_nodes, d_elems, M, kc, lc, ke, fe);
             break;
         case CFEM_OP_P1_MASS:
-            CFEM_LAUNCH(k_p1_scalar<CFEM_OP_P1_MASS>, grid_for(M, 128), 128, 0,
+            CFEM_LAUNCH(k_p1_scalar<CFEM_OP_P1_MASS>, grid_for(M, ctx->p1_threads),
+                        ctx->p1_threads, 0,
                         s, d_nodes, d_elems, M, kc, lc, ke, nullptr);
             break;
         case CFEM_OP_T10_STIFF:
@@ -822,17 +842,19 @@ int cfem_assemble_batch(cfem_ctx *ctx, int32_t op, const cfem_assembly_job *jobs
         if (want_rhs) CFEM_TRY(tmp_alloc(&fe, M * npe, s));
         if (M > 0) {
             if (op == CFEM_OP_P1_STIFF)
-                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_STIFF>, grid_for(M, 128), 128, 0, s,
+                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_STIFF>, grid_for(M, ctx->p1_threads),
+                            ctx->p1_threads, 0, s,
                             d_jobs, nj, M, ke, fe);
             else if (op == CFEM_OP_P1_MASS)
-                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_MASS>, grid_for(M, 128), 128, 0, s,
+                CFEM_LAUNCH(k_p1_scalar_batch<CFEM_OP_P1_MASS>, grid_for(M, ctx->p1_threads),
+                            ctx->p1_threads, 0, s,
                             d_jobs, nj, M, ke, nullptr);
             else if (op == CFEM_OP_T10_STIFF)
-                CFEM_LAUNCH(k_t10_scalar_batch<CFEM_OP_T10_STIFF>, grid_for(M, T10_WARPS),
-                            32 * T10_WARPS, 0, s, d_jobs, nj, M, ke, fe);
+                CFEM_TRY(launch_t10_batch<CFEM_OP_T10_STIFF>(ctx->t10_warps, M, s, d_jobs,
+                                                             nj, ke, fe));
             else
-                CFEM_LAUNCH(k_t10_scalar_batch<CFEM_OP_T10_MASS>, grid_for(M, T10_WARPS),
-                            32 * T10_WARPS, 0, s, d_jobs, nj, M, ke, nullptr);
+                CFEM_TRY(launch_t10_batch<CFEM_OP_T10_MASS>(ctx->t10_warps, M, s, d_jobs,
+                                                            nj, ke, nullptr));
         }
         unsigned g = grid_for(K, 256);
         if (g > (unsigned)ctx->num_sms * 32) g = ctx->num_sms * 32;

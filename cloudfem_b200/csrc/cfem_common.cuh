@@ -70,6 +70,10 @@ struct cfem_ctx {
     int cc_major = 0, cc_minor = 0;
     int64_t launches_at_create = 0;
     int scheduler = 0;                 // CFEM_SCHED_*
+    // launch parameters (cfem_ctx_set_param)
+    int t10_warps = 4;                 // Tet10 elements per block (batched)
+    int p1_threads = 128;              // P1 element kernels, threads per block
+    int graph_iters = 2;               // iterations per solve-loop body
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // SpMV timing

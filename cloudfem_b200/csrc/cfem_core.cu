@@ -206,6 +206,41 @@ int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes, uint64_t *reserved_bytes) 
     CFEM_API_END
 }
 
+int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
+    CFEM_CHECK(ctx, CFEM_ERR_INVALID, "cfem_ctx_set_param: ctx is NULL");
+    switch (param) {
+        case CFEM_PARAM_T10_WARPS:
+            CFEM_CHECK(value == 2 || value == 4 || value == 8, CFEM_ERR_INVALID,
+                       "Tet10 elements per block must be 2, 4 or 8 (got %d)", value);
+            ctx->t10_warps = value;
+            return CFEM_OK;
+        case CFEM_PARAM_P1_THREADS:
+            CFEM_CHECK(value == 32 || value == 64 || value == 128, CFEM_ERR_INVALID,
+                       "P1 threads per block must be 32, 64 or 128 (got %d)", value);
+            ctx->p1_threads = value;
+            return CFEM_OK;
+        case CFEM_PARAM_GRAPH_ITERS:
+            CFEM_CHECK(value == 1 || value == 2 || value == 4 || value == 8 || value == 16,
+                       CFEM_ERR_INVALID,
+                       "iterations per solve-loop body must be 1, 2, 4, 8 or 16 (got %d)",
+                       value);
+            ctx->graph_iters = value;
+            return CFEM_OK;
+        default:
+            return fail(CFEM_ERR_INVALID, "unknown parameter %d", param);
+    }
+}
+
+int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
+    if (!ctx) return -1;
+    switch (param) {
+        case CFEM_PARAM_T10_WARPS: return ctx->t10_warps;
+        case CFEM_PARAM_P1_THREADS: return ctx->p1_threads;
+        case CFEM_PARAM_GRAPH_ITERS: return ctx->graph_iters;
+        default: return -1;
+    }
+}
+
 int64_t cfem_ctx_launch_count(const cfem_ctx *ctx) {
     (void)ctx;
     return g_launches.load();

@@ -1371,7 +1371,6 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     }
 }
 
-constexpr int GRAPH_ITERS = 2;    // iterations per body of the solve loop
 constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
 
 // Start of a graph-scheduled solve: every system active, no barrier error.
@@ -1454,6 +1453,7 @@ struct cfem_pcg_plan {
     // host-polled variant (CFEM_SCHED_GRAPH_POLLED): two instantiations of
     // POLL_ITERS iterations replayed in turn
     bool polled = false;
+    int giters = 2;               // iterations per body of the solve loop
     cudaGraph_t pgraph[2] = {nullptr, nullptr};
     cudaGraphExec_t pexec[2] = {nullptr, nullptr};
 };
@@ -1761,6 +1761,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         P->per_iter = per_iter;
         return CFEM_OK;
     }
+    P->giters = ctx->graph_iters;
+    const int GRAPH_ITERS = P->giters;
     const unsigned max_rounds = (unsigned)((2 * max_iter + 32) / GRAPH_ITERS + 2);
     CFEM_CUDA(cudaStreamBeginCapture(w, cudaStreamCaptureModeThreadLocal));
     CFEM_CUDA(cudaMemsetAsync(P->ws_state, 0, P->state_bytes, w));
@@ -1878,7 +1880,7 @@ static int plan_run(cfem_pcg_plan *P, cfem_solve_stats *stats, cudaStream_t s) {
         CFEM_CUDA(cudaMemcpy(&rounds, &d_bar->rounds, sizeof(unsigned),
                              cudaMemcpyDeviceToHost));
         const int64_t bodies = rounds > 0 ? (int64_t)rounds - 1 : 0;
-        g_launches.fetch_add(3 + P->per_iter + bodies * (GRAPH_ITERS * P->per_iter + 1),
+        g_launches.fetch_add(3 + P->per_iter + bodies * (P->giters * P->per_iter + 1),
                              std::memory_order_relaxed);
         float sms = 0.0f;
         if (cudaEventElapsedTime(&sms, P->tev[0][0], P->tev[0][1]) == cudaSuccess) {

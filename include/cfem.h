@@ -163,6 +163,17 @@ CFEM_API int cfem_ctx_set_scheduler(cfem_ctx *ctx, int scheduler);
  * No counterpart in the reference (SciPy allocates host memory per call). */
 CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
                            uint64_t *reserved_bytes);
+/* Launch parameters of a context, chosen by the autotuner
+ * (cloudfem_b200/autotune.py) or by hand; no counterpart in the reference.
+ * T10_WARPS: Tet10 elements (one warp each) per block of the batched element
+ * kernel, 2, 4 (default) or 8. P1_THREADS: threads (one element each) per
+ * block of the P1 element kernels, 32, 64 or 128 (default). GRAPH_ITERS:
+ * iterations per body of the graph scheduler's solve loop, 1, 2 (default),
+ * 4, 8 or 16 (longer bodies: fewer loop-condition launches, more work past
+ * convergence). get returns -1 for an unknown parameter. */
+enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3 };
+CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
+CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */
 CFEM_API int64_t cfem_ctx_launch_count(const cfem_ctx *ctx);
 

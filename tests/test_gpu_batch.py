@@ -95,3 +95,41 @@ def test_batch_result_same_alone_and_in_mix(torch):
     for i in (0, 3, 6):
         alone = solve_batch([probs[i]], precision="mixed", rtol=1e-10)[0]
         assert np.abs(alone - mix[i]).max() <= 1e-9 * np.abs(mix[i]).max()
+
+
+def test_autotuned_batch_gives_identical_results(tmp_path, monkeypatch):
+    """Launch-parameter choices change block shapes and loop bodies, never
+    the arithmetic: a batch solved after tuning is bitwise the same."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200 import autotune
+    from cloudfem_b200.batch import BatchSolver, HeatProblem
+    from cloudfem_b200.mesh import box_mesh, box_mesh_tet10
+    monkeypatch.setenv("CLOUDFEM_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    bc = {s: 0.0 for s in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")}
+    rng = np.random.default_rng(2)
+    meshes = [box_mesh_tet10(5, 4, 4), box_mesh(9, 8, 7), box_mesh_tet10(3, 3, 3)]
+    probs = [HeatProblem(m, k=rng.lognormal(0, 1, len(m.elements)), f=1.0, bc=bc)
+             for m in meshes]
+    solver = BatchSolver()
+    rt = solver.rt
+    try:
+        N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_GRAPH))
+        batch = solver.prepare(probs)
+        batch.assemble()
+        batch.solve("mixed", rtol=1e-10)
+        before = [x.copy() for x in batch.solutions()]
+        out = autotune.tune_batch(batch, "mixed", 1e-10, repeat=1)
+        assert out["assembly"]["best"]["t10_elements_per_block"] in autotune.T10_WARPS
+        assert out["solve"]["best"]["iterations_per_loop_body"] in autotune.GRAPH_ITERS
+        batch.assemble()
+        batch.solve("mixed", rtol=1e-10)
+        for a, b in zip(before, batch.solutions()):
+            assert np.array_equal(a, b)
+    finally:
+        for p, v in ((N.PARAM_T10_WARPS, 4), (N.PARAM_P1_THREADS, 128),
+                     (N.PARAM_GRAPH_ITERS, 2)):
+            rt.set_param(p, v)
+        N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
