@@ -403,7 +403,10 @@ def run_c3(args, rank, world, local_rank):
     batch = solver.prepare(problems)
     free = batch.free_dofs
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    rtol = 1e-10
+    # the configuration's tolerance: CG with FP64 refinement to 1e-8 relative
+    # residual (the answer then agrees with FP64 to about 6e-9, within the
+    # 1e-8 accuracy bar); the plain FP64 path is timed to the same tolerance
+    rtol = 1e-8
 
     def step(precision, tol=rtol):
         batch.assemble()
@@ -415,11 +418,11 @@ def run_c3(args, rank, world, local_rank):
     # plain FP64 path: one problem per assembly+solve call, on a prefix
     plain_n = min(32, len(problems))
     sub = problems[:plain_n]
-    solve_batch(sub[:2], precision="fp64", rtol=1e-10, solver=solver)
+    solve_batch(sub[:2], precision="fp64", rtol=rtol, solver=solver)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for pb in sub:
-        solve_batch([pb], precision="fp64", rtol=1e-10, solver=solver)
+        solve_batch([pb], precision="fp64", rtol=rtol, solver=solver)
     torch.cuda.synchronize()
     plain_s = time.perf_counter() - t0
     plain_free = sum(batch.items[i]["free"] for i in range(plain_n))
