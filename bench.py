@@ -774,6 +774,7 @@ def run_c5(args, rank, world, local_rank):
             "dof_range": [1e3, 2e6], "hbm_budget_gb": 150, "workers": srv.workers,
             "requests": len(stream), "solved_dofs": med["solved_dofs"],
             "p50_ms": med["p50_ms"], "p99_ms": med["p99_ms"], "max_ms": med["max_ms"],
+            "by_kind": med["by_kind"],
             "best_run_dof_per_s": best["dof_per_s"],
             "plain_fp64_unbatched": {"requests": len(sub),
                                      "dof_per_s": plain_dofs / plain_s},

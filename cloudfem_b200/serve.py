@@ -161,6 +161,7 @@ class Server:
     def run_batch(self, reqs):
         """Solve one batch of same-kind requests on this thread's stream."""
         torch = self.torch
+        t0 = time.perf_counter()
         stream = torch.cuda.Stream(device=self.rt.device)
         with torch.cuda.stream(stream):
             if reqs[0].kind == "t10_elast":
@@ -168,6 +169,10 @@ class Server:
             else:
                 sols, res = self._run_heat(reqs)
             stream.synchronize()
+        dt = time.perf_counter() - t0
+        for r in reqs:
+            r.batch_s = dt
+            r.batch_size = len(reqs)
         return sols, res
 
     # ---------------------------------------------------------------- loop
@@ -275,7 +280,15 @@ def summarize(requests, wall):
         "p50_ms": float(np.percentile(lat, 50) * 1e3) if lat.size else None,
         "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else None,
         "max_ms": float(lat.max() * 1e3) if lat.size else None,
-        "by_kind": {k: sum(1 for r in done if r.kind == k) for k in KINDS},
+        "by_kind": {k: {"requests": sum(1 for r in done if r.kind == k),
+                        "solved_dofs": int(sum(free_dofs(r) for r in done if r.kind == k)),
+                        "batches": len({id(getattr(r, "t_start", None)) and (r.t_start, r.t_done)
+                                        for r in done if r.kind == k}),
+                        "worker_s": float(sum(getattr(r, "batch_s", 0.0) / max(getattr(r, "batch_size", 1), 1)
+                                              for r in done if r.kind == k)),
+                        "iterations_max": int(max([r.info.iterations for r in done
+                                                   if r.kind == k and r.info is not None] or [0]))}
+                    for k in KINDS},
     }
 
 
