@@ -74,6 +74,7 @@ struct cfem_ctx {
     int t10_warps = 4;                 // Tet10 elements per block (batched)
     int p1_threads = 128;              // P1 element kernels, threads per block
     int graph_iters = 2;               // iterations per solve-loop body
+    int pdl = 1;                       // dependent launches in solve graphs
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // SpMV timing

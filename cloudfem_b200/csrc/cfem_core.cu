@@ -226,6 +226,11 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
                        value);
             ctx->graph_iters = value;
             return CFEM_OK;
+        case CFEM_PARAM_PDL:
+            CFEM_CHECK(value == 0 || value == 1, CFEM_ERR_INVALID,
+                       "dependent-launch switch must be 0 or 1 (got %d)", value);
+            ctx->pdl = value;
+            return CFEM_OK;
         default:
             return fail(CFEM_ERR_INVALID, "unknown parameter %d", param);
     }
@@ -237,6 +242,7 @@ int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
         case CFEM_PARAM_T10_WARPS: return ctx->t10_warps;
         case CFEM_PARAM_P1_THREADS: return ctx->p1_threads;
         case CFEM_PARAM_GRAPH_ITERS: return ctx->graph_iters;
+        case CFEM_PARAM_PDL: return ctx->pdl;
         default: return -1;
     }
 }

@@ -105,6 +105,15 @@ struct GridBar {
     unsigned int grp[BAR_MAX_GROUPS][32];
 };
 
+// Programmatic dependent launch: kernels of the graph scheduler are
+// captured with programmatic stream serialisation, so the next kernel's
+// launch is processed while the previous one drains; each waits here for
+// its predecessor's completion and memory before reading anything it wrote.
+// A no-op for ordinary launches.
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -1240,6 +1249,7 @@ template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP, (GxOcc<T, BS>::blocks))
 k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
      const int2 *__restrict__ list, int n) {
+    pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
@@ -1275,6 +1285,7 @@ template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
 k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
      const int2 *__restrict__ list, int n) {
+    pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
@@ -1301,6 +1312,7 @@ template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
 k_gp(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
      const int2 *__restrict__ list, int n) {
+    pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
@@ -1336,6 +1348,7 @@ k_gp(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
 constexpr int RED_THREADS = 1024;
 __global__ void __launch_bounds__(RED_THREADS)
 k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which) {
+    pdl_wait();
     __shared__ double red[4][RED_THREADS / 32];
     const int s = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
     const SysDev &S = sys[s];
@@ -1388,6 +1401,7 @@ __global__ void k_plan_start(GridBar *bar, int n_systems) {
 // Loop condition of a graph-scheduled solve: another body while a system is
 // active and the round bound (from the largest max_iter) is not reached.
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, GridBar *bar, unsigned max_rounds) {
+    pdl_wait();
     if (threadIdx.x == 0) {
         const unsigned r = bar->rounds + 1;
         bar->rounds = r;
@@ -1418,6 +1432,25 @@ extern "C" int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
                     d_row_ptr, d_col, d_vals64, d_vals32);
     return CFEM_OK;
     CFEM_API_END
+}
+
+// Launch for stream capture, with programmatic stream serialisation when
+// pdl is set (the captured edge from the previous kernel node becomes a
+// programmatic dependency; the kernel waits in pdl_wait()).
+template <typename... KArgs, typename... Args>
+static void glaunch(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block,
+                    cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    (void)cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 // ---------------------------------------------------------------------------
@@ -1712,39 +1745,49 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // One iteration: direction (scalar systems), SpMV, reduction, update,
     // reduction. The SpMV of the first iteration is bracketed by the
     // timing events when tev is given.
+    const bool use_pdl = ctx->pdl != 0;
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
+        // dependent launches only between kernel nodes (not next to events)
+        const bool pdl = use_pdl && !t0;
+        bool first = true;
+        auto L = [&](bool p) { const bool r = p && !first; first = false; return r; };
         for (int t = 0; t < 4; t += 2) {   // scalar types only
             const int n = (int)lb[t].size();
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
-            if (t == 0) k_gp<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
-            if (t == 2) k_gp<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            if (t == 0) glaunch(L(pdl), k_gp<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
+            if (t == 2) glaunch(L(pdl), k_gp<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
             if (count) ++per_iter;
         }
         if (t0) CFEM_CUDA(cudaEventRecordWithFlags(t0, cs, cudaEventRecordExternal));
+        first = first || t0 != nullptr;
         for (int t = 0; t < 4; ++t) {
             const int n = (int)la[t].size();
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
-            if (t == 0) k_gx<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
-            if (t == 1) k_gx<double, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
-            if (t == 2) k_gx<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
-            if (t == 3) k_gx<float, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pa[t], n);
+            const bool p = L(pdl);
+            if (t == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 2) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
         if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));
-        k_greduce<<<n_systems, RED_THREADS, 0, cs>>>(d_sys, d_st, d_bar, 0);
+        first = first || t1 != nullptr;
+        glaunch(L(use_pdl), k_greduce, n_systems, RED_THREADS, cs, (const SysDev *)d_sys, d_st, d_bar, 0);
         for (int t = 0; t < 4; ++t) {
             const int n = (int)lb[t].size();
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
-            if (t == 0) k_gb<double, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
-            if (t == 1) k_gb<double, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
-            if (t == 2) k_gb<float, 1><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
-            if (t == 3) k_gb<float, 3><<<g, 32 * GROUP, 0, cs>>>(d_sys, d_st, d_bar, pb[t], n);
+            const bool p = L(use_pdl);
+            if (t == 0) glaunch(p, k_gb<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
+            if (t == 1) glaunch(p, k_gb<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
+            if (t == 2) glaunch(p, k_gb<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
+            if (t == 3) glaunch(p, k_gb<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pb[t], n);
             if (count) ++per_iter;
         }
-        k_greduce<<<n_systems, RED_THREADS, 0, cs>>>(d_sys, d_st, d_bar, 1);
+        glaunch(L(use_pdl), k_greduce, n_systems, RED_THREADS, cs, (const SysDev *)d_sys, d_st, d_bar, 1);
+        CFEM_CUDA(cudaGetLastError());
         return CFEM_OK;
     };
     // The whole solve is one graph: reset of the solver state, k_pcg_init,
@@ -1800,7 +1843,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     CFEM_CUDA(cudaStreamBeginCaptureToGraph(P->w2, body, nullptr, nullptr, 0,
                                             cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < GRAPH_ITERS; ++it) CFEM_TRY(iteration(P->w2, it == 0, nullptr, nullptr));
-    k_loop_cond<<<1, 32, 0, P->w2>>>(handle, d_bar, max_rounds);
+    glaunch(use_pdl, k_loop_cond, 1, 32, P->w2, handle, d_bar, max_rounds);
+    CFEM_CUDA(cudaGetLastError());
     cudaGraph_t body_out = nullptr;
     CFEM_CUDA(cudaStreamEndCapture(P->w2, &body_out));
     cudaError_t ce = cudaStreamEndCapture(w, &P->graph);

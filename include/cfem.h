@@ -170,8 +170,12 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * block of the P1 element kernels, 32, 64 or 128 (default). GRAPH_ITERS:
  * iterations per body of the graph scheduler's solve loop, 1, 2 (default),
  * 4, 8 or 16 (longer bodies: fewer loop-condition launches, more work past
- * convergence). get returns -1 for an unknown parameter. */
-enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3 };
+ * convergence). PDL: 1 (default) captures the solve graphs' kernels as
+ * programmatic dependent launches (launch processing overlaps the previous
+ * kernel's drain), 0 as plain launches. get returns -1 for an unknown
+ * parameter. */
+enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
+       CFEM_PARAM_PDL = 4 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */
