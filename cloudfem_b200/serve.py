@@ -173,6 +173,7 @@ class Server:
         for r in reqs:
             r.batch_s = dt
             r.batch_size = len(reqs)
+            r.solve_s = res[0].kernel_ms * 1e-3 if res else 0.0
         return sols, res
 
     # ---------------------------------------------------------------- loop
@@ -286,6 +287,8 @@ def summarize(requests, wall):
                                         for r in done if r.kind == k}),
                         "worker_s": float(sum(getattr(r, "batch_s", 0.0) / max(getattr(r, "batch_size", 1), 1)
                                               for r in done if r.kind == k)),
+                        "solve_device_s": float(sum(getattr(r, "solve_s", 0.0) / max(getattr(r, "batch_size", 1), 1)
+                                                    for r in done if r.kind == k)),
                         "iterations_max": int(max([r.info.iterations for r in done
                                                    if r.kind == k and r.info is not None] or [0]))}
                     for k in KINDS},
