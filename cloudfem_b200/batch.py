@@ -16,8 +16,8 @@ import numpy as np
 
 from . import _native as N
 from ._driver import accept, solver_mode
-from .device import BlockSystem, DeviceMesh, centroids, evaluate, fixed_scalar
-from .device import keast_points, pcg, ptr
+from .device import BlockSystem, DeviceMesh, evaluate, fixed_scalar
+from .device import pcg, ptr
 
 OPS = {4: N.OP_P1_STIFF, 10: N.OP_T10_STIFF}
 
@@ -69,12 +69,10 @@ class BatchSolver:
             return N.Coef(ptr(t), 0.0, N.COEF_ELEM, 0), t
         if not callable(spec):
             return N.Coef(None, float(spec), N.COEF_CONST, 0), None
-        host = dm.host
-        els = np.asarray(host.elements)
         if dm.npe == 10:
-            vals, mode = evaluate(spec, keast_points(host.nodes, els)), N.COEF_QP
+            vals, mode = evaluate(spec, dm.sample_points("qp")), N.COEF_QP
         else:
-            vals, mode = evaluate(spec, centroids(host.nodes, els)), N.COEF_ELEM
+            vals, mode = evaluate(spec, dm.sample_points("centroid")), N.COEF_ELEM
         if np.isscalar(vals):
             return N.Coef(None, float(vals), N.COEF_CONST, 0), None
         t = torch.from_numpy(np.ascontiguousarray(vals, dtype=float)).to(

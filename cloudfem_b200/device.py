@@ -208,19 +208,41 @@ class DeviceMesh:
         """
         if not callable(spec):
             return N.Coef(None, float(spec), N.COEF_CONST, 0), None
-        host = self.host
-        els = np.asarray(host.elements)
         if where == "qp":
-            vals = evaluate(spec, keast_points(host.nodes, els))
+            vals = evaluate(spec, self.sample_points("qp"))
             mode = N.COEF_QP
         else:
-            vals = evaluate(spec, centroids(host.nodes, els))
+            vals = evaluate(spec, self.sample_points("centroid"))
             mode = N.COEF_ELEM
         if np.isscalar(vals):
             return N.Coef(None, float(vals), N.COEF_CONST, 0), None
         t = _torch().from_numpy(np.ascontiguousarray(vals, dtype=float)).to(
             self.rt.device)
         return N.Coef(ptr(t), 0.0, mode, 0), t
+
+    def sample_points(self, where):
+        """Element centroids (M, 3) or Keast points (M, 5, 3) as host
+        arrays, computed once per mesh on the device (the gather of corner
+        coordinates is the costly part on the host for large meshes) with
+        the same operation order as the host formulas."""
+        pts = self.__dict__.setdefault("_pts", {})
+        if where not in pts:
+            torch = _torch()
+            corner = self.elems[:, :4].long()
+            p = [self.nodes[corner[:, c]] for c in range(4)]
+            if where == "qp":
+                L = torch.as_tensor(KEAST_L, dtype=torch.float64, device=self.nodes.device)
+                out = torch.empty((self.n_elems, L.shape[0], 3), dtype=torch.float64,
+                                  device=self.nodes.device)
+                for q in range(L.shape[0]):
+                    acc = L[q, 0] * p[0]
+                    for c in range(1, 4):
+                        acc = acc + L[q, c] * p[c]
+                    out[:, q] = acc
+            else:
+                out = (((p[0] + p[1]) + p[2]) + p[3]) / 4.0
+            pts[where] = out.cpu().numpy()
+        return pts[where]
 
     def nodal_coef(self, values):
         t = _torch().from_numpy(
