@@ -484,6 +484,77 @@ k_t10_curlcurl(const double *__restrict__ nodes, const int32_t *__restrict__ ele
     }
 }
 
+// Centroid strain and stress per element (Voigt xx, yy, zz, yz, xz, xy,
+// engineering shears), elastic3d.py:171-185 and elastic_tet10.py:232-262:
+// eps = B(G_c) u_e with G_c the physical gradients at the centroid (Keast
+// point 0 for Tet10), sig = D (eps - alpha (T_c - T_ref) [1,1,1,0,0,0]) with
+// the isotropic D, T_c the centroid temperature (per-element value, or the
+// nodal field interpolated: corner mean for P1, N(centroid) for Tet10).
+template <int NPE>
+__global__ void __launch_bounds__(128)
+k_elem_stress(const double *__restrict__ nodes, const int32_t *__restrict__ elems,
+              int64_t M, const double *__restrict__ u, double lam, double mu,
+              Coef temp, int thermal, double alpha, double tref,
+              double *__restrict__ sig, double *__restrict__ eps) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= M) return;
+    const int32_t *el = elems + e * NPE;
+    Geo g;
+    tet_geo(nodes, __ldg(el + 0), __ldg(el + 1), __ldg(el + 2), __ldg(el + 3), g);
+    double ev[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        double G[3];
+        if (NPE == 4) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                G[c] = a == 0 ? -(g.inv[0][c] + g.inv[1][c] + g.inv[2][c]) : g.inv[a - 1][c];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                G[j] = c_dNdxi[0][a][0] * g.inv[0][j] + c_dNdxi[0][a][1] * g.inv[1][j] +
+                       c_dNdxi[0][a][2] * g.inv[2][j];
+        }
+        const int64_t n = __ldg(el + a);
+        const double ux = __ldg(u + 3 * n), uy = __ldg(u + 3 * n + 1), uz = __ldg(u + 3 * n + 2);
+        ev[0] += G[0] * ux;
+        ev[1] += G[1] * uy;
+        ev[2] += G[2] * uz;
+        ev[3] += G[2] * uy + G[1] * uz;
+        ev[4] += G[2] * ux + G[0] * uz;
+        ev[5] += G[1] * ux + G[0] * uy;
+    }
+    double th = 0.0;
+    if (thermal) {
+        double Tc;
+        if (temp.mode == CFEM_COEF_NODAL) {
+            if (NPE == 4) {
+                Tc = (((temp.v[__ldg(el)] + temp.v[__ldg(el + 1)]) + temp.v[__ldg(el + 2)]) +
+                      temp.v[__ldg(el + 3)]) / 4.0;
+            } else {
+                Tc = 0.0;
+#pragma unroll
+                for (int s2 = 0; s2 < 10; ++s2) Tc += temp.v[__ldg(el + s2)] * c_N[0][s2];
+            }
+        } else {
+            Tc = coef_at(temp, e, 0);
+        }
+        th = alpha * (Tc - tref);
+    }
+    double em[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) em[i] = ev[i] - (i < 3 ? th : 0.0);
+    const double d0 = lam + 2.0 * mu;
+    sig[e * 6 + 0] = d0 * em[0] + lam * em[1] + lam * em[2];
+    sig[e * 6 + 1] = lam * em[0] + d0 * em[1] + lam * em[2];
+    sig[e * 6 + 2] = lam * em[0] + lam * em[1] + d0 * em[2];
+    sig[e * 6 + 3] = mu * em[3];
+    sig[e * 6 + 4] = mu * em[4];
+    sig[e * 6 + 5] = mu * em[5];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) eps[e * 6 + i] = ev[i];
+}
+
 // ------------------------------------------------------------- reductions
 template <int BS>
 __global__ void k_reduce_vals(const int32_t *__restrict__ seg,
@@ -940,6 +1011,34 @@ int cfem_assemble_elastic(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
     tmp_free(ke, s);
     tmp_free(fe, s);
     return st;
+    CFEM_API_END
+}
+
+int cfem_element_stress(cfem_ctx *ctx, const double *d_nodes, const int32_t *d_elems,
+                        int64_t n_elems, int32_t npe, const double *d_u, double E,
+                        double nu, const cfem_coef *temp, double alpha, double T_ref,
+                        double *d_sig, double *d_eps, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_nodes && d_elems && d_u && d_sig && d_eps && n_elems >= 0 &&
+                   (npe == 4 || npe == 10),
+               CFEM_ERR_INVALID, "cfem_element_stress: bad args");
+    CFEM_CHECK(E > 0.0 && nu > -1.0 && nu < 0.5, CFEM_ERR_INVALID,
+               "material constants out of range (E %g, nu %g)", E, nu);
+    CFEM_TRY(check_coef(temp, false, "temperature"));
+    if (n_elems == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mu = E / (2.0 * (1.0 + nu));
+    const int thermal = (temp != nullptr && alpha != 0.0) ? 1 : 0;
+    Coef tc = to_coef(temp);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (npe == 4)
+        CFEM_LAUNCH(k_elem_stress<4>, grid_for(n_elems, 128), 128, 0, s, d_nodes, d_elems,
+                    n_elems, d_u, lam, mu, tc, thermal, alpha, T_ref, d_sig, d_eps);
+    else
+        CFEM_LAUNCH(k_elem_stress<10>, grid_for(n_elems, 128), 128, 0, s, d_nodes, d_elems,
+                    n_elems, d_u, lam, mu, tc, thermal, alpha, T_ref, d_sig, d_eps);
+    return CFEM_OK;
     CFEM_API_END
 }
 

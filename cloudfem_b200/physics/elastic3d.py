@@ -9,13 +9,15 @@ whole chain on the device with 3 x 3 block-Jacobi PCG on the nodal block
 matrix. Stress recovery (:252-302) is vectorised on the host.
 """
 
+import ctypes
+
 import numpy as np
 import scipy.sparse as sp
 
 from .. import _native as N
 from .. import _faces
 from .._driver import solve_block, solve_csr
-from ..device import DeviceMesh, csr_to_device, evaluate, fixed_vector
+from ..device import DeviceMesh, csr_to_device, evaluate, fixed_vector, ptr
 from ..fem.tet_poisson import _tet_gradients
 
 
@@ -168,21 +170,37 @@ def _bmat(G):
     return B
 
 
-def element_stress_strain_3d(mesh, u, E, nu, T=None, alpha=0.0, T_ref=0.0):
-    """Per-element (sig, eps), each (M, 6), Voigt order."""
-    uv = _as_vector(mesh, u)
-    D = constitutive_3d(E, nu)
-    G, p = _grads_p1(mesh)
-    els = np.asarray(mesh.elements)
-    dofs = (3 * els[:, :, None] + np.arange(3)).reshape(len(els), -1)
-    eps = np.einsum("eai,ei->ea", _bmat(G), uv[dofs])
-    eth = np.zeros_like(eps)
+def _element_stress(mesh, u, E, nu, T, alpha, T_ref):
+    """Centroid (sig, eps) per element on the device (cfem_element_stress)."""
+    import torch
+    dm = DeviceMesh(mesh)
+    dev = dm.rt.device
+    uv = torch.from_numpy(np.ascontiguousarray(_as_vector(mesh, u), dtype=float)).to(dev)
+    if uv.numel() != 3 * dm.n_nodes:
+        raise ValueError(f"displacement has {uv.numel()} values, mesh needs "
+                         f"{3 * dm.n_nodes}")
+    tcoef, keep = None, None
     if T is not None and alpha != 0.0:
-        Tc = (evaluate(T, p.mean(axis=1)) if callable(T)
-              else np.asarray(T, dtype=float)[els].mean(axis=1))
-        eth = (alpha * (np.asarray(Tc) - T_ref))[..., None] * _EYE3
-    sig = np.einsum("ab,eb->ea", D, eps - eth)
-    return sig, eps
+        if callable(T):
+            vals = np.asarray(evaluate(T, dm.sample_points("centroid")), dtype=float)
+            vals = np.array(np.broadcast_to(vals, (dm.n_elems,)), dtype=float)
+            keep = torch.from_numpy(vals).to(dev)
+            tcoef = N.Coef(ptr(keep), 0.0, N.COEF_ELEM, 0)
+        else:
+            tcoef, keep = dm.nodal_coef(np.asarray(T, dtype=float))
+    sig = torch.empty(dm.n_elems * 6, dtype=torch.float64, device=dev)
+    eps = torch.empty_like(sig)
+    N.check(dm.rt.lib.cfem_element_stress(
+        dm.rt.ctx, ptr(dm.nodes), ptr(dm.elems), dm.n_elems, dm.npe, ptr(uv),
+        float(E), float(nu), ctypes.byref(tcoef) if tcoef is not None else None,
+        float(alpha), float(T_ref), ptr(sig), ptr(eps), dm.rt.stream()))
+    del keep
+    return (sig.cpu().numpy().reshape(-1, 6), eps.cpu().numpy().reshape(-1, 6))
+
+
+def element_stress_strain_3d(mesh, u, E, nu, T=None, alpha=0.0, T_ref=0.0):
+    """Per-element (sig, eps), each (M, 6), Voigt order (elastic3d.py:171-185)."""
+    return _element_stress(mesh, u, E, nu, T, alpha, T_ref)
 
 
 def von_mises_3d(sig):

@@ -18,7 +18,7 @@ from .._faces import face_shape6 as _face_shape  # noqa: F401
 from ..device import DeviceMesh, evaluate
 from ..fem.tet10 import element_operators, shape_functions  # noqa: F401
 from ..mesh.tet10_mesh import EDGES  # noqa: F401
-from .elastic3d import (_EYE3, _as_vector, _assemble, _bmat, _solve,
+from .elastic3d import (_EYE3, _as_vector, _assemble, _bmat, _element_stress, _solve,
                         apply_dirichlet_vec3, constitutive_3d)  # noqa: F401
 
 __all__ = [
@@ -64,24 +64,6 @@ def solve_elasticity_tet10(mesh, E, nu, bc=None, body=None, traction=None,
 
 
 def element_stress_tet10(mesh, u, E, nu, T=None, alpha=0.0, T_ref=0.0):
-    """Centroid strain and stress per element, each (M, 6)."""
-    uv = _as_vector(mesh, u)
-    D = constitutive_3d(E, nu)
-    els = np.asarray(mesh.elements)
-    Lc = np.array([[0.25, 0.25, 0.25, 0.25]])
-    Nc, dN = shape_functions(Lc)
-    dxi = np.stack([dN[0, :, 1] - dN[0, :, 0], dN[0, :, 2] - dN[0, :, 0],
-                    dN[0, :, 3] - dN[0, :, 0]], axis=-1)
-    p = mesh.nodes[els[:, :4]]
-    J = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0],
-                  p[:, 3] - p[:, 0]], axis=2)
-    Gc = np.einsum("ai,eij->eaj", dxi, np.linalg.inv(J))
-    dofs = (3 * els[:, :, None] + np.arange(3)).reshape(len(els), -1)
-    eps = np.einsum("eai,ei->ea", _bmat(Gc), uv[dofs])
-    eth = np.zeros_like(eps)
-    if T is not None and alpha != 0.0:
-        Tc = (evaluate(T, p.mean(axis=1)) if callable(T)
-              else np.asarray(T, dtype=float)[els] @ Nc[0])
-        eth = (alpha * (np.asarray(Tc) - T_ref))[..., None] * _EYE3
-    sig = np.einsum("ab,eb->ea", D, eps - eth)
-    return sig, eps
+    """Centroid strain and stress per element, each (M, 6)
+    (elastic_tet10.py:232-262), on the device."""
+    return _element_stress(mesh, u, E, nu, T, alpha, T_ref)

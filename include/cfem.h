@@ -249,6 +249,18 @@ CFEM_API int cfem_assemble_curlcurl(cfem_ctx *ctx, const cfem_pattern *p,
                                     cfem_coef nu, double *d_vals, int accumulate,
                                     void *stream);
 
+/* Centroid strain and stress per element (elastic3d.py:171-185,
+ * elastic_tet10.py:232-262): d_sig, d_eps (n_elems * 6, Voigt xx yy zz yz
+ * xz xy with engineering shears) from the nodal displacement d_u (3 N,
+ * node-major), isotropic E, nu, and an optional temperature (per-element
+ * centroid values CFEM_COEF_ELEM, or a nodal field CFEM_COEF_NODAL
+ * interpolated at the centroid; NULL or alpha 0: no thermal strain). */
+CFEM_API int cfem_element_stress(cfem_ctx *ctx, const double *d_nodes,
+                                 const int32_t *d_elems, int64_t n_elems, int32_t npe,
+                                 const double *d_u, double E, double nu,
+                                 const cfem_coef *temp, double alpha, double T_ref,
+                                 double *d_sig, double *d_eps, void *stream);
+
 /* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
  * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),
  * thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or QP). */
