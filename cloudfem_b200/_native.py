@@ -128,6 +128,8 @@ SIGNATURES = [
     ("cfem_pcg_plan_refresh", ctypes.c_int, [_vp, _vp]),
     ("cfem_pcg_plan_solve", ctypes.c_int, [_vp, ctypes.POINTER(SolveStats), _vp]),
     ("cfem_pcg_plan_destroy", ctypes.c_int, [_vp]),
+    ("cfem_cocg_solve", ctypes.c_int,
+     [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _f64, _i32, ctypes.POINTER(SolveStats), _vp]),
     ("cfem_pcg_noalloc_capacity", ctypes.c_size_t, []),
     ("cfem_pcg_solve_noalloc", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), ctypes.POINTER(SolveStats), _vp]),

@@ -363,6 +363,18 @@ CFEM_API int cfem_pcg_plan_solve(cfem_pcg_plan *plan, cfem_solve_stats *stats,
                                  void *stream);
 CFEM_API int cfem_pcg_plan_destroy(cfem_pcg_plan *plan);
 
+/* Jacobi-preconditioned COCG (CG with the unconjugated form x^T y) for one
+ * complex symmetric CSR system (A^T = A), values and vectors interleaved
+ * (re, im) FP64, 16-byte aligned. Replaces spla.spsolve in the phasor A-V
+ * eddy-current solve (em3d_tet10.py:267-375) once its V rows are scaled by
+ * 1/(i omega), which makes that system complex symmetric. d_x: initial
+ * guess in, solution out. Stops at ||r|| <= rtol ||b||; stats: status,
+ * iterations, relres, bnorm, kernel_ms. Synchronises. */
+CFEM_API int cfem_cocg_solve(cfem_ctx *ctx, int64_t n, const int32_t *d_indptr,
+                             const int32_t *d_indices, const double *d_vals,
+                             const double *d_b, double *d_x, double rtol,
+                             int32_t max_iter, cfem_solve_stats *stats, void *stream);
+
 /* Allocation-free variant of cfem_pcg_solve for ONE system. It has no
  * counterpart in the reference, which only solves on the host with SciPy.
  * It is for callers that cannot allocate device memory while solving: an

@@ -1012,3 +1012,85 @@ def assemble_tet10_av(mesh, nu, sigma=0.0, gauge_eps=1e-6):
     Gs = _coo(g_r, g_c, g_d, (3 * n, n_v))
     S = _coo(s_r, s_c, s_d, (n_v, n_v))
     return K, M, Gs, S, v_nodes, sig_e, conducting
+
+
+# ------------------------------------------------ Tet10 A-V phasor solve
+def boundary_nodes_em(mesh, boundary):
+    """em3d.py:85-105: None -> 'outer', 'boundary' or the union of all
+    sets; a name, a list of names, or an index array."""
+    if boundary is None:
+        if "outer" in mesh.boundaries:
+            return np.asarray(mesh.boundaries["outer"], dtype=int)
+        if "boundary" in mesh.boundaries:
+            return np.asarray(mesh.boundaries["boundary"], dtype=int)
+        sets = [np.asarray(v, dtype=int) for v in mesh.boundaries.values()]
+        return np.unique(np.concatenate(sets)) if sets else np.array([], int)
+    if isinstance(boundary, str):
+        return np.asarray(mesh.boundaries[boundary], dtype=int)
+    if isinstance(boundary, (list, tuple)) and boundary and isinstance(boundary[0], str):
+        return np.unique(np.concatenate(
+            [np.asarray(mesh.boundaries[k], dtype=int) for k in boundary]))
+    return np.asarray(boundary, dtype=int)
+
+
+def js_load_tet10(mesh, J_s):
+    """em3d_tet10.py:322-331: rhs[3p+m] += V sum_q w_q J_m(x_q) N_qp
+    (complex J allowed), vectorised over elements."""
+    n = mesh.n_nodes
+    _, wq = quadrature()
+    _, Nq, xq, vol = element_operators_all(mesh)
+    pts = xq.reshape(-1, 3)
+    Jq = np.array([np.asarray(J_s(x, y, z), dtype=complex).ravel() for x, y, z in pts])
+    Jq = Jq.reshape(xq.shape[0], xq.shape[1], 3)
+    fe = vol[:, None, None] * np.einsum("q,eqm,qp->epm", wq, Jq, Nq)
+    rhs = np.zeros(3 * n, dtype=complex)
+    np.add.at(rhs, (3 * mesh.elements[:, :, None] + np.arange(3)).ravel(), fe.ravel())
+    return rhs
+
+
+def solve_eddy_current_tet10(mesh, nu=1.0 / (4e-7 * np.pi), sigma=0.0, omega=0.0,
+                             B_applied=None, J_s=None, boundary=None, a_bc=None,
+                             gauge_eps=1e-6):
+    """em3d_tet10.py:267-375 (SuperLU on the eliminated A-V system)."""
+    if omega <= 0:
+        raise ValueError("omega must be positive")
+    if B_applied is None and J_s is None:
+        raise ValueError("no excitation")
+    K, M, Gs, S, v_nodes, sig_e, conducting = assemble_tet10_av(
+        mesh, nu=nu, sigma=sigma, gauge_eps=gauge_eps)
+    if not conducting.any():
+        raise ValueError("no conducting elements (sigma > 0) in mesh")
+    n = mesh.n_nodes
+    n_v = len(v_nodes)
+    A_sys = sp.bmat([[K + 1j * omega * M, Gs], [1j * omega * Gs.T, S]], format="csr")
+    rhs = np.zeros(3 * n + n_v, dtype=complex)
+    if J_s is not None:
+        rhs[:3 * n] += js_load_tet10(mesh, J_s)
+    fixed = {}
+    for p in boundary_nodes_em(mesh, boundary):
+        x = mesh.nodes[int(p)]
+        val = 0.5 * np.cross(np.asarray(B_applied, dtype=float), x) \
+            if B_applied is not None else np.zeros(3)
+        for m in range(3):
+            fixed[3 * int(p) + m] = complex(val[m])
+    for name, vals in (a_bc or {}).items():
+        fn = vals if callable(vals) else (lambda x, y, z, v=vals: np.asarray(v, dtype=complex))
+        for p in np.asarray(mesh.boundaries[name], dtype=int):
+            vv = np.asarray(fn(*mesh.nodes[int(p)]), dtype=complex).ravel()
+            for m in range(3):
+                fixed[3 * int(p) + m] = vv[m]
+    idx = np.array(sorted(fixed), dtype=int)
+    val = np.array([fixed[i] for i in idx], dtype=complex)
+    keep = np.ones(A_sys.shape[0], dtype=bool)
+    if len(idx):
+        rhs = rhs - A_sys[:, idx] @ val
+        keep[idx] = False
+    A2 = A_sys[keep][:, keep]
+    sol = spla.spsolve(A2.tocsc(), rhs[keep])
+    full = np.zeros(3 * n + n_v, dtype=complex)
+    full[keep] = np.asarray(sol).ravel()
+    if len(idx):
+        full[idx] = val
+    v = np.zeros(n, dtype=complex)
+    v[v_nodes] = full[3 * n:]
+    return full[:3 * n], v

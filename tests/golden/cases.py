@@ -17,6 +17,10 @@ P1_CUBE = 4
 TET10_BOX = (2, 2, 3, (0.0, 1.0), (0.0, 0.5), (0.0, 1.5))
 TET10_BEAM = (6, 1, 2, (0.0, 0.6), (0.0, 0.05), (0.0, 0.1))
 AV_BOX = (2, 2, 2, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+# phasor A-V solves: conductor everywhere, source current, A = 0 outside
+AVP_N = 3
+AVP_SIGMA = 1.0e6
+AVP_OMEGA = 2.0 * np.pi * 1000.0
 
 
 def k_fn(x, y, z):
@@ -75,3 +79,9 @@ def t_nodal(n_nodes):
     """Seeded nodal temperature field used by the thermal-load cases."""
     rng = np.random.default_rng(7)
     return 20.0 + 30.0 * rng.random(n_nodes)
+
+
+def avp_js(x, y, z):
+    """Complex source current density of the phasor A-V cases."""
+    s = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+    return np.array([(1.0 + 2.0j) * 1e9 * s, 0.5e9 * s * (1.0 + x), 0.3j * 1e9 * y * z])

@@ -202,6 +202,14 @@ def main(ref_path):
     put("av_sig_e", sig_e)
     put("av_cond", cond)
 
+    # ---------------- Tet10 A-V phasor solve (SuperLU) ----------------
+    mp = box_mesh_tet10(C.AVP_N, C.AVP_N, C.AVP_N)
+    a, v = em.solve_eddy_current_tet10(mp, nu=C.nu_fn, sigma=C.AVP_SIGMA,
+                                       omega=C.AVP_OMEGA, J_s=C.avp_js,
+                                       boundary=list(C.FACES))
+    put("avp_a", a)
+    put("avp_v", v)
+
     path = os.path.join(HERE, "ref_fixtures.npz")
     np.savez_compressed(path, **out)
     size = os.path.getsize(path)

@@ -226,3 +226,35 @@ def test_av_blocks_vs_oracle(cf, gauge):
     cen = m.nodes[np.asarray(m.elements)[:, :4]].mean(axis=1)
     nu_e = np.array([C.nu_fn(*c) for c in cen])
     assert_csr_equal(em._assemble_curl_curl_tet10_nu(m, nu_e), ref[0])
+
+
+# stated tolerance: COCG to 1e-10 relative residual agrees with SuperLU's
+# answer to 1e-8 relative
+AVP_TOL = 1e-8
+
+
+def test_av_phasor_golden(cf, golden):
+    """Phasor A-V solve (device COCG) against the reference's SuperLU answer."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    m = cf.mesh.box_mesh_tet10(C.AVP_N, C.AVP_N, C.AVP_N)
+    a, v = em.solve_eddy_current_tet10(m, nu=C.nu_fn, sigma=C.AVP_SIGMA,
+                                       omega=C.AVP_OMEGA, J_s=C.avp_js,
+                                       boundary=list(C.FACES))
+    for mine, ref in ((a, golden["avp_a"]), (v, golden["avp_v"])):
+        assert np.linalg.norm(mine - ref) <= AVP_TOL * np.linalg.norm(ref)
+
+
+def test_av_phasor_conductor_in_air(cf):
+    """Half-conducting box in a background field (gauge-regularised air,
+    pinned V node) against the oracle's SuperLU solve."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    from oracle import cfem_oracle as O
+    m = cf.mesh.box_mesh_tet10(4, 4, 4)
+    mo = O.box_mesh_tet10(4, 4, 4)
+    kw = dict(nu=C.nu_fn, sigma=C.sigma_fn, omega=C.AVP_OMEGA, B_applied=(0.0, 0.0, 1e-3))
+    a, v = em.solve_eddy_current_tet10(m, **kw)
+    ao, vo = O.solve_eddy_current_tet10(mo, **kw)
+    assert np.linalg.norm(a - ao) <= 1e-7 * np.linalg.norm(ao)
+    assert np.linalg.norm(v - vo) <= 1e-7 * np.linalg.norm(vo)
+    with pytest.raises(ValueError):
+        em.solve_eddy_current_tet10(m, nu=C.nu_fn, sigma=0.0, omega=1.0, B_applied=(0, 0, 1))

@@ -199,3 +199,12 @@ def test_av_blocks(golden):
     np.testing.assert_array_equal(v_nodes, golden["av_vnodes"])
     np.testing.assert_array_equal(sig_e, golden["av_sig_e"])
     np.testing.assert_array_equal(cond, golden["av_cond"])
+
+
+def test_av_phasor_solve(golden):
+    m = O.box_mesh_tet10(C.AVP_N, C.AVP_N, C.AVP_N)
+    a, v = O.solve_eddy_current_tet10(m, nu=C.nu_fn, sigma=C.AVP_SIGMA,
+                                      omega=C.AVP_OMEGA, J_s=C.avp_js,
+                                      boundary=list(C.FACES))
+    for mine, ref in ((a, golden["avp_a"]), (v, golden["avp_v"])):
+        assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref)
