@@ -778,6 +778,76 @@ def run_av(args, rank, world, local_rank):
     return out
 
 
+def run_avt(args, rank, world, local_rank):
+    """Transient A-V eddy currents: half-conducting Tet10 box, sinusoidal
+    source, Crank-Nicolson, one device PCG solve per step."""
+    import torch
+
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.mesh import box_mesh_tet10
+    from cloudfem_b200.physics import em3d_tet10 as em
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rt = N.runtime(local_rank)
+    n, steps = args.av_n, 50
+
+    def sigma(x, y, z):
+        return np.where(np.asarray(x) < 0.5, 1.0e6, 0.0)
+
+    kw = dict(nu=1.0 / (4e-7 * np.pi), sigma=sigma, t_end=steps * 1e-4, dt=1e-4,
+              method="cn", J_s=lambda x, y, z: np.real(av_js(x, y, z)),
+              time_scale=lambda t: np.sin(2 * np.pi * 500.0 * t),
+              boundary=["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"])
+    mesh = box_mesh_tet10(n, n, n)
+    for _ in range(args.warmup):
+        em.transient_eddy_current_tet10(mesh, precision=args.precision, **kw)
+    walls, l0 = [], rt.launches()
+    with Clocks(local_rank) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = em.transient_eddy_current_tet10(mesh, precision=args.precision, **kw)
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+    launches = rt.launches() - l0
+    if rank != 0:
+        return None
+    fixed = len(np.unique(np.concatenate([mesh.boundaries[f] for f in kw["boundary"]])))
+    unknowns = 3 * (mesh.n_nodes - fixed)
+    wall = float(np.mean(walls))
+    out = {
+        "metric": METRIC, "value": world * unknowns * steps / wall, "unit": "DOF/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 PCG + f64 residual/update",
+        "data": "synthetic (Tet10 box, half conducting, sinusoidal source current)",
+        "config": {"workload": f"transient_av_tet10_box_{n}cubed_{steps}_cn_steps",
+                   "a_unknowns": int(unknowns), "time_steps": steps,
+                   "note": "value and e2e: the public call, A-block DOF-steps per second "
+                           "(device blocks and solves, host power diagnostics)",
+                   "P_last": float(r["P"][-1]), "parallelism": f"replicas x{world}"},
+        "e2e": {"value": world * unknowns * steps / wall, "unit": "DOF/s",
+                "h2d_bytes_per_step": int(mesh.nodes.nbytes + mesh.elements.nbytes),
+                "d2h_bytes_per_step": int(steps * 3 * mesh.n_nodes * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import cfem_oracle as O
+        nb = 8
+        mo = O.box_mesh_tet10(nb, nb, nb)
+        t0 = time.perf_counter()
+        O.transient_eddy_current_tet10(mo, **kw)
+        dt = time.perf_counter() - t0
+        fb = len(np.unique(np.concatenate([mo.boundaries[f] for f in kw["boundary"]])))
+        ub = 3 * (mo.n_nodes - fb)
+        out["cpu_baseline"] = {"value": ub * steps / dt, "unit": "DOF/s",
+                               "cores": os.cpu_count(), "kind": "port", "seconds": dt,
+                               "sample": f"box {nb}^3, {steps} CN steps, one LU"}
+    return out
+
+
 # ---------------------------------------------------------------- C5
 C5_REQUESTS = 200
 
@@ -918,7 +988,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"],
                     help="default: fp64 for c2 (faster there), mixed for c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "av"],
+    ap.add_argument("--workload", default="c2",
+                    choices=["c2", "c3", "c4", "c5", "av", "avt"],
                     help="c2: Tet10 elasticity beam (default); c3: 512 "
                          "batched Tet10 heat meshes; c4: transient P1 heat, "
                          "128^3 box, 200 Crank-Nicolson steps; c5: serving "
@@ -963,6 +1034,8 @@ def main():
             out = run_c5(args, rank, world, local_rank)
         elif args.workload == "av":
             out = run_av(args, rank, world, local_rank)
+        elif args.workload == "avt":
+            out = run_avt(args, rank, world, local_rank)
         else:
             out = run_ours(args, rank, world, local_rank)
         if world > 1:

@@ -1094,3 +1094,118 @@ def solve_eddy_current_tet10(mesh, nu=1.0 / (4e-7 * np.pi), sigma=0.0, omega=0.0
     v = np.zeros(n, dtype=complex)
     v[v_nodes] = full[3 * n:]
     return full[:3 * n], v
+
+
+# ------------------------------------------ Tet10 A-V transient (theta)
+THETA_EM = {"be": 1.0, "implicit_euler": 1.0, "cn": 0.5, "crank_nicolson": 0.5}
+
+
+def _l_nodes():
+    """Barycentric coordinates of the 10 Tet10 nodes (corners, then edge
+    midpoints in EDGES order)."""
+    L = np.zeros((10, 4))
+    L[np.arange(4), np.arange(4)] = 1.0
+    for k, (i, j) in enumerate(EDGES):
+        L[4 + k, i] = L[4 + k, j] = 0.5
+    return L
+
+
+def nodal_gradients_all(mesh):
+    """em3d_tet10.py:122-137 for every element: grad N_j at node p,
+    (M, 10, 10, 3)."""
+    p = mesh.nodes[mesh.elements[:, :4]]
+    J = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]], axis=2)
+    _, dN_dL = shape_functions(_l_nodes())
+    dN_dxi = np.stack([dN_dL[..., 1] - dN_dL[..., 0], dN_dL[..., 2] - dN_dL[..., 0],
+                       dN_dL[..., 3] - dN_dL[..., 0]], axis=-1)          # (10, 10, 3)
+    return np.einsum("pjk,ekl->epjl", dN_dxi, np.linalg.inv(J))
+
+
+def transient_joule_power_tet10(mesh, a_prev, a_new, v, sigma, h, grads=None):
+    """em3d_tet10.py:665-692: sigma V sum_pq MASS_REF E_p.E_q over the
+    conducting elements, E = -(a_new - a_prev)/h - grad V at the nodes."""
+    a_prev = np.asarray(a_prev, dtype=float).reshape(-1, 3)
+    a_new = np.asarray(a_new, dtype=float).reshape(-1, 3)
+    v = np.asarray(v, dtype=float)
+    cen = mesh.nodes[mesh.elements[:, :4]].mean(axis=1)
+    sig_e = np.asarray(eval_points(sigma, cen), dtype=float) * np.ones(len(mesh.elements))
+    p = mesh.nodes[mesh.elements[:, :4]]
+    J = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]], axis=2)
+    vols = np.abs(np.linalg.det(J)) / 6.0
+    on = sig_e > 0.0
+    els = mesh.elements[on]
+    g = (nodal_gradients_all(mesh) if grads is None else grads)[on]
+    Ep = -(a_new[els] - a_prev[els]) / h - np.einsum("epjx,ej->epx", g, v[els])
+    re = np.einsum("epm,eqm->epq", Ep, Ep)
+    Pe = sig_e[on] * vols[on] * np.einsum("pq,epq->e", mass_reference(), re)
+    Q = np.zeros(len(mesh.elements))
+    Q[on] = Pe / vols[on]
+    return float(np.sum(Q * vols)), Q
+
+
+def transient_eddy_current_tet10(mesh, nu=1.0 / (4e-7 * np.pi), sigma=0.0, t_end=1.0,
+                                 dt=0.1, method="cn", J_s=None, time_scale=None,
+                                 B_applied=None, boundary=None, a_bc=None,
+                                 gauge_eps=1e-6):
+    """em3d_tet10.py:479-662 (monolithic theta step, one LU), without the
+    history option; returns {times, P, a_end, v_end}."""
+    theta = THETA_EM[method]
+    K, M, Gs, S, v_nodes, sig_e, conducting = assemble_tet10_av(
+        mesh, nu=nu, sigma=sigma, gauge_eps=gauge_eps)
+    n = mesh.n_nodes
+    n_v = len(v_nodes)
+    nx = 3 * n + n_v
+    E = sp.bmat([[M, sp.csr_matrix((3 * n, n_v))], [Gs.T, sp.csr_matrix((n_v, n_v))]], format="csr")
+    Km = sp.bmat([[K, Gs], [sp.csr_matrix((n_v, 3 * n)), S]], format="csr")
+    n_steps = int(np.ceil(t_end / dt - 1e-12))
+    h = t_end / n_steps
+    A_lhs = (E / h + theta * Km).tocsr()
+    A_rhs = (E / h - (1.0 - theta) * Km).tocsr()
+    fixed = {}
+    Bv = np.asarray(B_applied, dtype=float) if B_applied is not None else None
+    for p in boundary_nodes_em(mesh, boundary):
+        x = mesh.nodes[int(p)]
+        val = 0.5 * np.cross(Bv, x) if Bv is not None else np.zeros(3)
+        for m in range(3):
+            fixed[3 * int(p) + m] = float(val[m])
+    for name, vals in (a_bc or {}).items():
+        fn = vals if callable(vals) else (lambda x, y, z, v=vals: np.asarray(v, dtype=float))
+        for p in np.asarray(mesh.boundaries[name], dtype=int):
+            vv = np.asarray(fn(*mesh.nodes[int(p)]), dtype=float).ravel()
+            for m in range(3):
+                fixed[3 * int(p) + m] = vv[m]
+    idx = np.array(sorted(fixed), dtype=int)
+    val = np.array([fixed[i] for i in idx], dtype=float)
+    keep = np.ones(nx, dtype=bool)
+    keep[idx] = False
+    solve = spla.factorized(A_lhs[keep][:, keep].tocsc())
+    A_kf = A_lhs[keep][:, idx] if len(idx) else None
+    solve_S = spla.factorized(S.tocsc())
+    f_static = np.real(js_load_tet10(mesh, J_s)) if J_s is not None else None
+    ts = (lambda t: 1.0) if time_scale is None else time_scale
+    times = np.linspace(0.0, t_end, n_steps + 1)
+    P = np.zeros(n_steps + 1)
+    grads = nodal_gradients_all(mesh)
+    x = np.zeros(nx)
+    x[idx] = val
+    a_prev = x[:3 * n].copy()
+    v_end = np.zeros(n)
+    for k in range(1, n_steps + 1):
+        f = np.zeros(nx)
+        if f_static is not None:
+            f[:3 * n] = (theta * ts(times[k]) + (1.0 - theta) * ts(times[k - 1])) * f_static
+        b = (A_rhs @ x + f)[keep]
+        if A_kf is not None:
+            b = b - A_kf @ val
+        xk = np.zeros(nx)
+        xk[keep] = solve(b)
+        xk[idx] = val
+        x = xk
+        a_new = x[:3 * n]
+        adot = (a_new - a_prev) / h
+        v_new = np.zeros(n)
+        v_new[v_nodes] = -solve_S(Gs.T @ adot)
+        P[k] = transient_joule_power_tet10(mesh, a_prev, a_new, v_new, sigma, h, grads)[0]
+        a_prev = a_new.copy()
+        v_end = v_new
+    return {"times": times, "P": P, "a_end": x[:3 * n].copy(), "v_end": v_end}

@@ -85,3 +85,18 @@ def avp_js(x, y, z):
     """Complex source current density of the phasor A-V cases."""
     s = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
     return np.array([(1.0 + 2.0j) * 1e9 * s, 0.5e9 * s * (1.0 + x), 0.3j * 1e9 * y * z])
+
+
+# transient A-V: half-conducting box, sinusoidal source, a few CN steps
+AVT_N = 3
+AVT_T_END, AVT_DT = 4e-3, 1e-3
+
+
+def avt_js(x, y, z):
+    """Real source current density pattern of the transient A-V case."""
+    s = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+    return np.array([1e8 * s, 0.5e8 * s * (1.0 + x), 0.2e8 * y * z])
+
+
+def avt_scale(t):
+    return np.sin(2.0 * np.pi * 250.0 * t)

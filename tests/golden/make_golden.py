@@ -210,6 +210,16 @@ def main(ref_path):
     put("avp_a", a)
     put("avp_v", v)
 
+    # ---------------- Tet10 A-V transient (theta method, LU) ----------------
+    mt = box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)
+    res = em.transient_eddy_current_tet10(
+        mt, nu=C.nu_fn, sigma=C.sigma_fn, t_end=C.AVT_T_END, dt=C.AVT_DT,
+        method="cn", J_s=C.avt_js, time_scale=C.avt_scale,
+        boundary=list(C.FACES))
+    put("avt_P", res["P"])
+    put("avt_a_end", res["a_end"])
+    put("avt_v_end", res["v_end"])
+
     path = os.path.join(HERE, "ref_fixtures.npz")
     np.savez_compressed(path, **out)
     size = os.path.getsize(path)

@@ -258,3 +258,20 @@ def test_av_phasor_conductor_in_air(cf):
     assert np.linalg.norm(v - vo) <= 1e-7 * np.linalg.norm(vo)
     with pytest.raises(ValueError):
         em.solve_eddy_current_tet10(m, nu=C.nu_fn, sigma=0.0, omega=1.0, B_applied=(0, 0, 1))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_av_transient_golden(cf, golden, precision):
+    """Transient A-V eddy currents (theta method; device PCG on the
+    symmetrised step matrix) against the reference's LU march."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    m = cf.mesh.box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)
+    r = em.transient_eddy_current_tet10(
+        m, nu=C.nu_fn, sigma=C.sigma_fn, t_end=C.AVT_T_END, dt=C.AVT_DT,
+        method="cn", J_s=C.avt_js, time_scale=C.avt_scale,
+        boundary=list(C.FACES), precision=precision)
+    tol = 1e-9 if precision == "fp64" else 1e-7
+    assert np.abs(r["P"] - golden["avt_P"]).max() <= tol * np.abs(golden["avt_P"]).max()
+    for k in ("a_end", "v_end"):
+        ref = golden["avt_" + k]
+        assert np.linalg.norm(r[k] - ref) <= tol * np.linalg.norm(ref)

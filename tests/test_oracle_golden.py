@@ -208,3 +208,14 @@ def test_av_phasor_solve(golden):
                                       boundary=list(C.FACES))
     for mine, ref in ((a, golden["avp_a"]), (v, golden["avp_v"])):
         assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref)
+
+
+def test_av_transient(golden):
+    m = O.box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)
+    r = O.transient_eddy_current_tet10(
+        m, nu=C.nu_fn, sigma=C.sigma_fn, t_end=C.AVT_T_END, dt=C.AVT_DT,
+        method="cn", J_s=C.avt_js, time_scale=C.avt_scale, boundary=list(C.FACES))
+    assert np.abs(r["P"] - golden["avt_P"]).max() <= 1e-10 * np.abs(golden["avt_P"]).max()
+    for k in ("a_end", "v_end"):
+        ref = golden["avt_" + k]
+        assert np.linalg.norm(r[k] - ref) <= 1e-10 * np.linalg.norm(ref)
