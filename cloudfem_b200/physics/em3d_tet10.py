@@ -263,6 +263,19 @@ def solve_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, omega=0.0,
         mesh, nu=nu, sigma=sigma, gauge_eps=gauge_eps)
     if not conducting.any():
         raise ValueError("no conducting elements (sigma > 0) in mesh")
+    return _solve_phasor_with_K_tet10(mesh, K, M, Gs, S, v_nodes, omega, B_applied,
+                                      J_s, boundary, a_bc, permc_spec, rtol=rtol,
+                                      max_iter=max_iter)
+
+
+def _solve_phasor_with_K_tet10(mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s,
+                               boundary, a_bc, permc_spec=None, *, rtol=1e-10,
+                               max_iter=None):
+    """One linear phasor solve with a given curl-curl block K
+    (em3d_tet10.py:774-846, used by the nonlinear Picard loop, :938): block
+    system with the V rows scaled by 1/(i w), source load, Dirichlet
+    elimination as the reference, device COCG; returns (a, v)."""
+    import torch
     n = mesh.n_nodes
     n_v = len(v_nodes)
     w = float(omega)
