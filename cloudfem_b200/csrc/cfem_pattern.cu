@@ -193,26 +193,11 @@ using namespace cfem;
 
 extern "C" {
 
-int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
-                        int64_t n_elems, int32_t npe, int64_t n_nodes,
-                        void *stream, cfem_pattern **out) {
-    CFEM_API_BEGIN
-    CFEM_CHECK(ctx && out && (d_elems || n_elems == 0), CFEM_ERR_INVALID,
-               "cfem_pattern_create: NULL argument");
-    CFEM_CHECK(npe == 4 || npe == 10, CFEM_ERR_INVALID,
-               "nodes per element must be 4 or 10, got %d", npe);
-    CFEM_CHECK(n_nodes > 0 && n_nodes < (int64_t)1 << 31 && n_elems >= 0,
-               CFEM_ERR_INVALID, "bad mesh size (%lld nodes, %lld elements)",
-               (long long)n_nodes, (long long)n_elems);
-    const int64_t total = n_elems * npe * npe;
-    CFEM_CHECK(total < ((int64_t)1 << 31), CFEM_ERR_INVALID,
-               "mesh too large for one pattern (%lld element entries)",
-               (long long)total);
-    *out = nullptr;
-    CFEM_TRY(set_device(ctx->device));
-    cudaStream_t s = (cudaStream_t)stream;
-
-    cfem_pattern *p = new cfem_pattern();
+// Pattern arrays and contribution lists of p (already sized fields set by
+// the caller); on failure the caller destroys p.
+static int build_pattern(cfem_ctx *ctx, const int32_t *d_elems, int64_t n_elems,
+                         int32_t npe, int64_t n_nodes, int64_t total,
+                         cudaStream_t s, cfem_pattern *p) {
     p->device = ctx->device;
     p->n_nodes = n_nodes;
     p->n_elems = n_elems;
@@ -280,7 +265,6 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
             tmp_free(pos, s);
             tmp_free(d_bad, s);
             cudaStreamSynchronize(s);
-            cfem_pattern_destroy(p);
             return fail(CFEM_ERR_INVALID,
                         "element connectivity references a node id outside "
                         "[0, %lld)", (long long)n_nodes);
@@ -308,6 +292,35 @@ int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
     CFEM_LAUNCH(k_diag, grid_for(n_nodes, 256), 256, 0, s, p->row_ptr, p->col,
                 n_nodes, p->diag);
     CFEM_CUDA(cudaStreamSynchronize(s));
+    return CFEM_OK;
+}
+
+int cfem_pattern_create(cfem_ctx *ctx, const int32_t *d_elems,
+                        int64_t n_elems, int32_t npe, int64_t n_nodes,
+                        void *stream, cfem_pattern **out) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && out && (d_elems || n_elems == 0), CFEM_ERR_INVALID,
+               "cfem_pattern_create: NULL argument");
+    CFEM_CHECK(npe == 4 || npe == 10, CFEM_ERR_INVALID,
+               "nodes per element must be 4 or 10, got %d", npe);
+    CFEM_CHECK(n_nodes > 0 && n_nodes < (int64_t)1 << 31 && n_elems >= 0,
+               CFEM_ERR_INVALID, "bad mesh size (%lld nodes, %lld elements)",
+               (long long)n_nodes, (long long)n_elems);
+    const int64_t total = n_elems * npe * npe;
+    CFEM_CHECK(total < ((int64_t)1 << 31), CFEM_ERR_INVALID,
+               "mesh too large for one pattern (%lld element entries)",
+               (long long)total);
+    *out = nullptr;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+
+    cfem_pattern *p = new cfem_pattern();
+    const int st = build_pattern(ctx, d_elems, n_elems, npe, n_nodes, total, s, p);
+    if (st != CFEM_OK) {
+        cudaStreamSynchronize(s);
+        cfem_pattern_destroy(p);
+        return st;
+    }
     *out = p;
     return CFEM_OK;
     CFEM_API_END
@@ -318,11 +331,10 @@ int cfem_pattern_destroy(cfem_pattern *p) {
     cudaSetDevice(p->device);
     // ordered after all work queued on the legacy stream (which waits for
     // the blocking streams the library's callers use)
-    cudaFreeAsync(p->row_ptr, 0);
-    cudaFreeAsync(p->col, 0);
-    cudaFreeAsync(p->diag, 0);
-    cudaFreeAsync(p->seg, 0);
-    cudaFreeAsync(p->contrib, 0);
+    for (void *ptr : {(void *)p->row_ptr, (void *)p->col, (void *)p->diag,
+                      (void *)p->seg, (void *)p->contrib})
+        if (ptr) cudaFreeAsync(ptr, 0);
+    (void)cudaGetLastError();
     delete p;
     return CFEM_OK;
 }
