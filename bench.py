@@ -872,14 +872,14 @@ def run_c5(args, rank, world, local_rank):
 
     # warm-up on a short stream of small requests (kernels, pools)
     warm = serve.make_stream(30, rate=2000.0, dof_range=(1e3, 2e4), seed=1)
-    serve.Server(local_rank, precision=args.precision).serve(warm, realtime=False)
+    serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol).serve(warm, realtime=False)
 
     # end to end: a new server, every mesh arrives with its request (H2D,
     # pattern build, assembly, solve, D2H per request)
     torch.cuda.synchronize()
-    e2e = serve.Server(local_rank, precision=args.precision).serve(fresh())
+    e2e = serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol).serve(fresh())
     # resident: the same stream again on that server's warm device meshes
-    srv = serve.Server(local_rank, precision=args.precision)
+    srv = serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol)
     srv.serve(fresh(), realtime=False)
     runs = []
     for _ in range(args.warmup):
@@ -891,21 +891,26 @@ def run_c5(args, rank, world, local_rank):
     launches = rt.launches() - l0
     mixed_sol = {r.id: r.result for r in stream}
 
-    # plain FP64 GPU path: one request at a time, unbatched, FP64, on the
-    # first requests of the stream; accuracy of the served answers vs it
-    plain = serve.Server(local_rank, workers=1, precision="fp64", rtol=1e-12)
+    # plain FP64 GPU path: one request at a time, unbatched, FP64, to the
+    # same tolerance, on the first requests of the stream; accuracy of the
+    # served answers against a tight FP64 solve of each
+    plain = serve.Server(local_rank, workers=1, precision="fp64", rtol=args.c5_rtol)
     sub = [r for r in fresh()[: min(40, len(stream))]]
     for r in sub[:2]:
         plain.run_batch([r])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    errs, plain_dofs = [], 0
+    plain_dofs = 0
     for r in sub:
-        sol, _ = plain.run_batch([r])
+        plain.run_batch([r])
         plain_dofs += serve.free_dofs(r)
+    plain_s = time.perf_counter() - t0
+    tight = serve.Server(local_rank, workers=1, precision="fp64", rtol=1e-12)
+    errs = []
+    for r in sub:
+        sol, _ = tight.run_batch([r])
         x = mixed_sol[r.id]
         errs.append(float(np.linalg.norm(x - sol[0]) / max(np.linalg.norm(sol[0]), 1e-300)))
-    plain_s = time.perf_counter() - t0
     if rank != 0:
         return None
     best = max(runs, key=lambda d: d["dof_per_s"])
@@ -921,6 +926,7 @@ def run_c5(args, rank, world, local_rank):
             "workload": f"serving_stream_{len(stream)}_requests_lambda200",
             "mix": "60% P1 heat / 25% Tet10 heat / 15% Tet10 elasticity",
             "dof_range": [1e3, 2e6], "hbm_budget_gb": 150, "workers": srv.workers,
+            "rtol": args.c5_rtol,
             "requests": len(stream), "solved_dofs": med["solved_dofs"],
             "p50_ms": med["p50_ms"], "p99_ms": med["p99_ms"], "max_ms": med["max_ms"],
             "by_kind": med["by_kind"],
@@ -995,6 +1001,8 @@ def main():
                          "stream of mixed requests")
     ap.add_argument("--av-n", type=int, default=AV_N,
                     help="av: cells per box edge of the phasor A-V workload")
+    ap.add_argument("--c5-rtol", type=float, default=1e-8,
+                    help="c5: relative residual each served request is solved to")
     ap.add_argument("--c5-requests", type=int, default=C5_REQUESTS,
                     help="c5: requests in the stream")
     ap.add_argument("--scheduler", default="auto",
