@@ -338,18 +338,31 @@ class DeviceMesh:
         cand = out[: cnt.value].cpu().numpy()
         if cand.size == 0:
             return np.zeros((0, width), dtype=np.int64)
-        e, f = cand // 4, cand % 4
-        els = np.asarray(host.elements, dtype=np.int64)
-        if tet10:
-            table = np.array([c + m for c, m in FACES_T10])
-        else:
-            table = np.array(FACES_P1)
-        full = els[e[:, None], table[f]]
-        keys = np.sort(full[:, :3], axis=1)
+        return exterior_faces(np.asarray(host.elements, dtype=np.int64), cand, tet10)
+
+
+def exterior_faces(els, cand, tet10=False):
+    """Faces (node lists) of candidate face ids e*4+f that occur once among
+    the candidates (by sorted corner triple), in first-occurrence order.
+
+    The corner triple is packed into one int64 over the compact ids of the
+    candidates' corner nodes (exact while there are < 2^21 of them), so one
+    1-D stable unique replaces a row-wise unique."""
+    e, f = cand // 4, cand % 4
+    table = np.array([c + m for c, m in FACES_T10]) if tet10 else np.array(FACES_P1)
+    full = els[e[:, None], table[f]]
+    keys = np.sort(full[:, :3], axis=1)
+    ids, inv = np.unique(keys.ravel(), return_inverse=True)
+    B = len(ids)
+    if B < (1 << 21):
+        k = inv.reshape(-1, 3).astype(np.int64)
+        packed = (k[:, 0] * B + k[:, 1]) * B + k[:, 2]
+        _, first, counts = np.unique(packed, return_index=True, return_counts=True)
+    else:
         _, first, counts = np.unique(keys, axis=0, return_index=True,
                                      return_counts=True)
-        keep = np.sort(first[counts == 1])
-        return full[keep]
+    keep = np.sort(first[counts == 1])
+    return full[keep]
 
 
 # ------------------------------------------------------------ solver

@@ -35,6 +35,7 @@ import scipy.sparse.linalg as spla
 from scipy.sparse.csgraph import connected_components
 
 from .. import _native as N
+from .._faces import add_at
 from ..device import DeviceMesh, centroids, evaluate, ptr
 
 MU0 = 4e-7 * np.pi
@@ -233,7 +234,7 @@ def _js_load(mesh, dm, J_s):
     vol = np.abs(np.linalg.det(J)) / 6.0
     fe = vol[:, None, None] * np.einsum("q,eqm,qp->epm", wq, Jq, Nq)
     rhs = np.zeros(3 * mesh.n_nodes, dtype=complex)
-    np.add.at(rhs, (3 * els[:, :, None] + np.arange(3)).ravel(), fe.ravel())
+    add_at(rhs, (3 * els[:, :, None] + np.arange(3)).ravel(), fe.ravel())
     return rhs
 
 
