@@ -3,9 +3,12 @@
 Default workload: Tet10 3D elasticity, box 2.0 x 0.25 x 0.25 m,
 80 x 10 x 10 Kuhn cells (48,000 Tet10 elements, 71,001 nodes, 213,003
 DOFs, 211,680 free), E = 210 GPa, nu = 0.3, clamped at x = 0, 1 MPa
-traction in -z on x = 2 m, FP32 PCG with FP64 reliable updates to 1e-10
-relative residual. One step = pattern build + Tet10 element matrices +
-CSR reduction + traction load + Dirichlet masking + solve.
+traction in -z on x = 2 m, Jacobi PCG to 1e-10 relative residual in FP64
+(--precision mixed: FP32 PCG with FP64 residual, update and convergence
+test). One step = pattern build + Tet10 element matrices + CSR reduction +
+traction load + Dirichlet masking + solve. Other workloads (--workload):
+batched Tet10 heat meshes, a transient P1 heat march, a serving stream,
+and the Tet10 A-V eddy-current phasor and transient solves.
 
 value  : solved (free) DOF/s with the mesh already resident in HBM.
 e2e    : the same through the public API solve_elasticity_tet10(...) with
@@ -350,12 +353,12 @@ def cpu_baseline(shape=CPU_SAMPLE):
                       f"({free} free DOFs), one solve, {dt:.1f} s"}
 
 
-# --------------------------------------------------------------------- C3
-C3_MESHES = 512
-C3_SEED = 0
+# ---------------------------------------------------- batched Tet10 heat meshes
+BATCH_MESHES = 512
+BATCH_SEED = 0
 
 
-def c3_draw(count=C3_MESHES, seed=C3_SEED):
+def batch_draw(count=BATCH_MESHES, seed=BATCH_SEED):
     """Seeded batch: n ~ U{4..24}, lognormal(0, 1) conductivity per hex cell."""
     rng = np.random.default_rng(seed)
     ns = rng.integers(4, 25, size=count)
@@ -363,7 +366,7 @@ def c3_draw(count=C3_MESHES, seed=C3_SEED):
     return ns, ks
 
 
-def c3_cell_fn(n, kc):
+def batch_cell_fn(n, kc):
     """The per-cell conductivity as the reference's callable API sees it:
     k(x, y, z) = K[i, j, k] of the hex cell containing the point (Keast
     points are interior, so the lookup is exact)."""
@@ -377,7 +380,7 @@ def c3_cell_fn(n, kc):
     return k
 
 
-def c3_problems(ns, ks):
+def batch_problems(ns, ks):
     from cloudfem_b200.batch import HeatProblem
     from cloudfem_b200.mesh import box_mesh_tet10
     meshes = {int(n): box_mesh_tet10(int(n), int(n), int(n)) for n in set(ns)}
@@ -387,7 +390,7 @@ def c3_problems(ns, ks):
             for n, kc in zip(ns, ks)]
 
 
-def run_c3(args, rank, world, local_rank):
+def run_batched_heat(args, rank, world, local_rank):
     import torch
 
     from cloudfem_b200 import _native as N
@@ -397,8 +400,8 @@ def run_c3(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
     _set_scheduler(rt, args.scheduler)
-    ns, ks = c3_draw(args.meshes)
-    problems = c3_problems(ns, ks)
+    ns, ks = batch_draw(args.meshes)
+    problems = batch_problems(ns, ks)
     solver = BatchSolver(local_rank)
     batch = solver.prepare(problems)
     free = batch.free_dofs
@@ -509,11 +512,11 @@ def run_c3(args, rank, world, local_rank):
                                          "fp32" if args.precision == "mixed" else "fp64"),
         }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_c3(ns, ks)
+        out["cpu_baseline"] = cpu_baseline_batched_heat(ns, ks)
     return out
 
 
-def cpu_baseline_c3(ns, ks, cap_n=7, count=12):
+def cpu_baseline_batched_heat(ns, ks, cap_n=7, count=12):
     """Oracle (NumPy + SuperLU) on the first `count` draws with n <= cap_n."""
     from oracle import cfem_oracle as O
     bc = {s: 0.0 for s in O.FACE_NAMES}
@@ -521,7 +524,7 @@ def cpu_baseline_c3(ns, ks, cap_n=7, count=12):
     free, t0 = 0, time.perf_counter()
     for n, kc in picked:
         m = O.box_mesh_tet10(n, n, n)
-        O.solve_tet10_poisson(m, k=c3_cell_fn(n, kc), f=1.0, bc=bc)
+        O.solve_tet10_poisson(m, k=batch_cell_fn(n, kc), f=1.0, bc=bc)
         free += (2 * n - 1) ** 3
     dt = time.perf_counter() - t0
     return {"value": free / dt, "unit": "DOF/s", "cores": os.cpu_count(),
@@ -530,26 +533,26 @@ def cpu_baseline_c3(ns, ks, cap_n=7, count=12):
                       f"({free} free DOFs), one solve each"}
 
 
-# ---------------------------------------------------------------- C4
-C4_N = 128
-C4_STEPS = 200
-C4_PARAMS = dict(k=45.0, rho_cp=3.6e6, t0=20.0, h=25.0, t_inf=20.0,
+# ------------------------------------------------ transient P1 heat, 128^3 box
+TRANSIENT_N = 128
+TRANSIENT_STEPS = 200
+TRANSIENT_PARAMS = dict(k=45.0, rho_cp=3.6e6, t0=20.0, h=25.0, t_inf=20.0,
                  q0=1e7, sigma=0.1, dt=1.0)
-C4_FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+TRANSIENT_FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
 
 
-def c4_source(x, y, z):
+def transient_source(x, y, z):
     """Gaussian heat source of peak q0 at the box centre."""
-    p = C4_PARAMS
+    p = TRANSIENT_PARAMS
     r2 = (np.asarray(x) - 0.5) ** 2 + (np.asarray(y) - 0.5) ** 2 + (np.asarray(z) - 0.5) ** 2
     return p["q0"] * np.exp(-r2 / (2.0 * p["sigma"] ** 2))
 
 
-def c4_robin():
-    return {f: (C4_PARAMS["h"], C4_PARAMS["t_inf"]) for f in C4_FACES}
+def transient_robin():
+    return {f: (TRANSIENT_PARAMS["h"], TRANSIENT_PARAMS["t_inf"]) for f in TRANSIENT_FACES}
 
 
-def _c4_device_march(dm, mesh, precision, n_steps, rtol):
+def _transient_device_march(dm, mesh, precision, n_steps, rtol):
     """Pattern + K, C, F and Robin terms + theta march on resident inputs;
     returns the final field on the device and the per-step solve records."""
     import torch
@@ -557,10 +560,10 @@ def _c4_device_march(dm, mesh, precision, n_steps, rtol):
     from cloudfem_b200 import _native as N
     from cloudfem_b200._driver import last_solve_info, theta_march
     from cloudfem_b200.fem.tet_heat import _terms, add_csr_into
-    p = C4_PARAMS
+    p = TRANSIENT_PARAMS
     dm._pattern = None
-    K, F = dm.assemble(N.OP_P1_STIFF, coef=p["k"], load=c4_source)
-    K_add, F_add = _terms(dm, mesh, None, c4_robin())
+    K, F = dm.assemble(N.OP_P1_STIFF, coef=p["k"], load=transient_source)
+    K_add, F_add = _terms(dm, mesh, None, transient_robin())
     add_csr_into(dm, K, K_add)
     F = F + torch.from_numpy(F_add).to(dm.rt.device)
     C, _ = dm.assemble(N.OP_P1_MASS, coef=p["rho_cp"])
@@ -571,7 +574,7 @@ def _c4_device_march(dm, mesh, precision, n_steps, rtol):
     return T, last_solve_info()
 
 
-def run_c4(args, rank, world, local_rank):
+def run_transient_heat(args, rank, world, local_rank):
     import torch
 
     from cloudfem_b200 import _native as N
@@ -583,8 +586,8 @@ def run_c4(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
     _set_scheduler(rt, args.scheduler)
-    n = args.c4_n
-    n_steps = args.c4_steps
+    n = args.transient_n
+    n_steps = args.transient_steps
     mesh = box_mesh(n, n, n)
     dm = DeviceMesh(mesh, local_rank)
     free = mesh.n_nodes                       # Robin everywhere: no fixed DOF
@@ -593,18 +596,18 @@ def run_c4(args, rank, world, local_rank):
 
     # accuracy gate: the first 20 steps in both precisions
     gate = min(20, n_steps)
-    T64, _ = _c4_device_march(dm, mesh, "fp64", gate, 1e-12)
+    T64, _ = _transient_device_march(dm, mesh, "fp64", gate, 1e-12)
     T64 = T64.clone()
-    Tm, _ = _c4_device_march(dm, mesh, args.precision, gate, rtol)
+    Tm, _ = _transient_device_march(dm, mesh, args.precision, gate, rtol)
     gate_err = float(torch.linalg.norm(Tm - T64) / torch.linalg.norm(T64))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    _c4_device_march(dm, mesh, "fp64", gate, 1e-12)
+    _transient_device_march(dm, mesh, "fp64", gate, 1e-12)
     torch.cuda.synchronize()
     fp64_s = time.perf_counter() - t0
 
     for _ in range(args.warmup):
-        _c4_device_march(dm, mesh, args.precision, min(10, n_steps), rtol)
+        _transient_device_march(dm, mesh, args.precision, min(10, n_steps), rtol)
     torch.cuda.synchronize()
     times, l0 = [], rt.launches()
     with Clocks(local_rank) as clk:
@@ -613,7 +616,7 @@ def run_c4(args, rank, world, local_rank):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            T, infos = _c4_device_march(dm, mesh, args.precision, n_steps, rtol)
+            T, infos = _transient_device_march(dm, mesh, args.precision, n_steps, rtol)
             e1.record()
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
@@ -626,10 +629,10 @@ def run_c4(args, rank, world, local_rank):
     for _ in range(max(1, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        transient_heat_tet(mesh, k=C4_PARAMS["k"], rho_cp=C4_PARAMS["rho_cp"],
-                           f=c4_source, robin=c4_robin(),
-                           t_end=n_steps * C4_PARAMS["dt"], dt=C4_PARAMS["dt"],
-                           T0=C4_PARAMS["t0"], method="cn",
+        transient_heat_tet(mesh, k=TRANSIENT_PARAMS["k"], rho_cp=TRANSIENT_PARAMS["rho_cp"],
+                           f=transient_source, robin=transient_robin(),
+                           t_end=n_steps * TRANSIENT_PARAMS["dt"], dt=TRANSIENT_PARAMS["dt"],
+                           T0=TRANSIENT_PARAMS["t0"], method="cn",
                            precision=args.precision, rtol=rtol)
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
@@ -678,18 +681,18 @@ def run_c4(args, rank, world, local_rank):
             "launch_ms": float(np.mean(spmv)), "traffic": None,
         }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_c4()
+        out["cpu_baseline"] = cpu_baseline_transient_heat()
     return out
 
 
-def cpu_baseline_c4(n=32, n_steps=20):
+def cpu_baseline_transient_heat(n=32, n_steps=20):
     """Oracle (NumPy assembly + SciPy LU, factorised once) on a small box."""
     from oracle import cfem_oracle as O
-    p = C4_PARAMS
+    p = TRANSIENT_PARAMS
     t0 = time.perf_counter()
     m = O.box_mesh(n, n, n)
-    O.transient_heat_p1(m, k=p["k"], rho_cp=p["rho_cp"], f=c4_source,
-                        robin=c4_robin(), t_end=n_steps * p["dt"], dt=p["dt"],
+    O.transient_heat_p1(m, k=p["k"], rho_cp=p["rho_cp"], f=transient_source,
+                        robin=transient_robin(), t_end=n_steps * p["dt"], dt=p["dt"],
                         T0=p["t0"], method="cn")
     dt = time.perf_counter() - t0
     free = (n + 1) ** 3
@@ -698,7 +701,7 @@ def cpu_baseline_c4(n=32, n_steps=20):
             "sample": f"box {n}^3 ({free} nodes), {n_steps} CN steps incl. assembly"}
 
 
-# ---------------------------------------------------------------- A-V
+# ------------------------------------------------ Tet10 A-V eddy currents
 AV_N = 10
 AV_SIGMA, AV_FREQ = 1.0e6, 1000.0
 
@@ -847,11 +850,11 @@ def run_avt(args, rank, world, local_rank):
     return out
 
 
-# ---------------------------------------------------------------- C5
-C5_REQUESTS = 200
+# ---------------------------------------------------- serving a request stream
+SERVE_REQUESTS = 200
 
 
-def run_c5(args, rank, world, local_rank):
+def run_serving(args, rank, world, local_rank):
     import torch
 
     from cloudfem_b200 import _native as N
@@ -862,7 +865,7 @@ def run_c5(args, rank, world, local_rank):
     rt = N.runtime(local_rank)
     _set_scheduler(rt, args.scheduler)
     cache = {}
-    stream = serve.make_stream(args.c5_requests, rate=200.0, seed=7,
+    stream = serve.make_stream(args.serve_requests, rate=200.0, seed=7,
                                mesh_cache=cache)
 
     def fresh():
@@ -872,14 +875,14 @@ def run_c5(args, rank, world, local_rank):
 
     # warm-up on a short stream of small requests (kernels, pools)
     warm = serve.make_stream(30, rate=2000.0, dof_range=(1e3, 2e4), seed=1)
-    serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol).serve(warm, realtime=False)
+    serve.Server(local_rank, precision=args.precision, rtol=args.serve_rtol).serve(warm, realtime=False)
 
     # end to end: a new server, every mesh arrives with its request (H2D,
     # pattern build, assembly, solve, D2H per request)
     torch.cuda.synchronize()
-    e2e = serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol).serve(fresh())
+    e2e = serve.Server(local_rank, precision=args.precision, rtol=args.serve_rtol).serve(fresh())
     # resident: the same stream again on that server's warm device meshes
-    srv = serve.Server(local_rank, precision=args.precision, rtol=args.c5_rtol)
+    srv = serve.Server(local_rank, precision=args.precision, rtol=args.serve_rtol)
     srv.serve(fresh(), realtime=False)
     runs = []
     for _ in range(args.warmup):
@@ -894,7 +897,7 @@ def run_c5(args, rank, world, local_rank):
     # plain FP64 GPU path: one request at a time, unbatched, FP64, to the
     # same tolerance, on the first requests of the stream; accuracy of the
     # served answers against a tight FP64 solve of each
-    plain = serve.Server(local_rank, workers=1, precision="fp64", rtol=args.c5_rtol)
+    plain = serve.Server(local_rank, workers=1, precision="fp64", rtol=args.serve_rtol)
     sub = [r for r in fresh()[: min(40, len(stream))]]
     for r in sub[:2]:
         plain.run_batch([r])
@@ -926,7 +929,7 @@ def run_c5(args, rank, world, local_rank):
             "workload": f"serving_stream_{len(stream)}_requests_lambda200",
             "mix": "60% P1 heat / 25% Tet10 heat / 15% Tet10 elasticity",
             "dof_range": [1e3, 2e6], "hbm_budget_gb": 150, "workers": srv.workers,
-            "rtol": args.c5_rtol,
+            "rtol": args.serve_rtol,
             "requests": len(stream), "solved_dofs": med["solved_dofs"],
             "p50_ms": med["p50_ms"], "p99_ms": med["p99_ms"], "max_ms": med["max_ms"],
             "by_kind": med["by_kind"],
@@ -953,13 +956,13 @@ def run_reference(args, rank):
     if rank != 0:
         return None
     per = []
-    if args.workload == "c3":
-        draw = c3_draw()
+    if args.workload == "batched-heat":
+        draw = batch_draw()
     for i in range(args.warmup + args.steps):
-        if args.workload == "c3":
-            c = cpu_baseline_c3(*draw)
-        elif args.workload == "c4":
-            c = cpu_baseline_c4()
+        if args.workload == "batched-heat":
+            c = cpu_baseline_batched_heat(*draw)
+        elif args.workload == "transient-heat":
+            c = cpu_baseline_transient_heat()
         else:
             c = cpu_baseline()
         if i >= args.warmup:
@@ -974,8 +977,8 @@ def run_reference(args, rank):
         "ms_per_step": float(np.mean([c["seconds"] for c in per])) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": {"c3": "batched_tet10_heat_512_meshes_n4to24",
-                                "c4": f"transient_p1_heat_cn_box_{C4_N}cubed_{C4_STEPS}_steps",
+        "config": {"workload": {"batched-heat": "batched_tet10_heat_512_meshes_n4to24",
+                                "transient-heat": f"transient_p1_heat_cn_box_{TRANSIENT_N}cubed_{TRANSIENT_STEPS}_steps",
                                 }.get(args.workload, "tet10_elasticity_beam_80x10x10"),
                    "sample": c["sample"]},
         "cpu_baseline": c,
@@ -991,34 +994,37 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"],
-                    help="default: fp64 for c2 (faster there), mixed for c3")
+                    help="default: fp64 for the elasticity beam and the A-V transient, "
+                         "mixed otherwise")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2",
-                    choices=["c2", "c3", "c4", "c5", "av", "avt"],
-                    help="c2: Tet10 elasticity beam (default); c3: 512 "
-                         "batched Tet10 heat meshes; c4: transient P1 heat, "
-                         "128^3 box, 200 Crank-Nicolson steps; c5: serving "
-                         "stream of mixed requests")
+    ap.add_argument("--workload", default="elasticity",
+                    choices=["elasticity", "batched-heat", "transient-heat", "serving",
+                             "av-phasor", "av-transient"],
+                    help="elasticity: Tet10 elasticity beam 80x10x10 (default); "
+                         "batched-heat: 512 seeded Tet10 heat meshes; "
+                         "transient-heat: P1 heat, 128^3 box, 200 Crank-Nicolson "
+                         "steps; serving: stream of 200 mixed requests; "
+                         "av-phasor / av-transient: Tet10 A-V eddy currents, 10^3 box")
     ap.add_argument("--av-n", type=int, default=AV_N,
-                    help="av: cells per box edge of the phasor A-V workload")
-    ap.add_argument("--c5-rtol", type=float, default=1e-8,
-                    help="c5: relative residual each served request is solved to")
-    ap.add_argument("--c5-requests", type=int, default=C5_REQUESTS,
-                    help="c5: requests in the stream")
+                    help="av-phasor / av-transient: cells per box edge")
+    ap.add_argument("--serve-rtol", type=float, default=1e-8,
+                    help="serving: relative residual each request is solved to")
+    ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
+                    help="serving: requests in the stream")
     ap.add_argument("--scheduler", default="auto",
                     choices=["auto", "persistent", "graph", "polled"],
                     help="solver scheduler (polled: host-polled graph replays, "
                          "for per-launch profiling)")
-    ap.add_argument("--c4-n", type=int, default=C4_N,
-                    help="c4: cells per box edge")
-    ap.add_argument("--c4-steps", type=int, default=C4_STEPS,
-                    help="c4: time steps per bench step")
-    ap.add_argument("--meshes", type=int, default=C3_MESHES,
-                    help="c3: number of meshes of the seeded draw (a smaller "
+    ap.add_argument("--transient-n", type=int, default=TRANSIENT_N,
+                    help="transient-heat: cells per box edge")
+    ap.add_argument("--transient-steps", type=int, default=TRANSIENT_STEPS,
+                    help="transient-heat: time steps per bench step")
+    ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
+                    help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
     args = ap.parse_args()
     if args.precision is None:
-        args.precision = "fp64" if args.workload in ("c2", "avt") else "mixed"
+        args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -1033,15 +1039,15 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl",
                                     timeout=datetime.timedelta(seconds=300))
-        if args.workload == "c3":
-            out = run_c3(args, rank, world, local_rank)
-        elif args.workload == "c4":
-            out = run_c4(args, rank, world, local_rank)
-        elif args.workload == "c5":
-            out = run_c5(args, rank, world, local_rank)
-        elif args.workload == "av":
+        if args.workload == "batched-heat":
+            out = run_batched_heat(args, rank, world, local_rank)
+        elif args.workload == "transient-heat":
+            out = run_transient_heat(args, rank, world, local_rank)
+        elif args.workload == "serving":
+            out = run_serving(args, rank, world, local_rank)
+        elif args.workload == "av-phasor":
             out = run_av(args, rank, world, local_rank)
-        elif args.workload == "avt":
+        elif args.workload == "av-transient":
             out = run_avt(args, rank, world, local_rank)
         else:
             out = run_ours(args, rank, world, local_rank)
