@@ -71,7 +71,7 @@ def test_repeat_is_bitwise_deterministic(torch):
     assert np.array_equal(u1, u2)
 
 
-def test_config1_full_size_accuracy(torch):
+def test_p1_poisson_20cubed_accuracy(torch):
     """P1 20^3 manufactured problem: the discretisation error matches the
     reference's (L2 = 1.89e-3) and both precisions agree to 1e-8."""
     from cloudfem_b200.fem.tet_poisson import solve_tet_poisson
