@@ -46,13 +46,19 @@ RTOL = 1e-10
 L2_FLUSH_BYTES = 256 << 20
 
 
+SPMV_STAGE = None   # --spmv-stage: None keeps the library default
+
+
 def _set_scheduler(rt, name):
     """Solver scheduler of the run (auto unless asked; polled graphs make
-    every solver launch visible to per-launch profilers)."""
+    every solver launch visible to per-launch profilers), and the scalar
+    SpMV staging when asked."""
     from cloudfem_b200 import _native as N
     code = {"auto": N.SCHED_AUTO, "persistent": N.SCHED_PERSISTENT,
             "graph": N.SCHED_GRAPH, "polled": N.SCHED_GRAPH_POLLED}[name]
     N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, code))
+    if SPMV_STAGE is not None:
+        rt.set_param(N.PARAM_SPMV_STAGE, SPMV_STAGE)
 
 
 def _peaks():
@@ -1022,7 +1028,12 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
                     help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
+    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2],
+                    help="scalar SpMV: 1 bulk-staged 4 KB windows (library default), "
+                         "2 bulk-staged 2 KB windows, 0 register path")
     args = ap.parse_args()
+    global SPMV_STAGE
+    SPMV_STAGE = args.spmv_stage
     if args.precision is None:
         args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -231,6 +231,11 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
                        "dependent-launch switch must be 0 or 1 (got %d)", value);
             ctx->pdl = value;
             return CFEM_OK;
+        case CFEM_PARAM_SPMV_STAGE:
+            CFEM_CHECK(value >= 0 && value <= 2, CFEM_ERR_INVALID,
+                       "scalar SpMV staging must be 0, 1 or 2 (got %d)", value);
+            ctx->spmv_stage = value;
+            return CFEM_OK;
         default:
             return fail(CFEM_ERR_INVALID, "unknown parameter %d", param);
     }
@@ -243,6 +248,7 @@ int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
         case CFEM_PARAM_P1_THREADS: return ctx->p1_threads;
         case CFEM_PARAM_GRAPH_ITERS: return ctx->graph_iters;
         case CFEM_PARAM_PDL: return ctx->pdl;
+        case CFEM_PARAM_SPMV_STAGE: return ctx->spmv_stage;
         default: return -1;
     }
 }

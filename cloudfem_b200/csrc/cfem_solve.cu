@@ -1121,6 +1121,288 @@ __global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-staged scalar SpMV (graph scheduler, A phase of scalar systems).
+// A warp owns one work entry of up to XR_MAX rows, whose entries are one
+// contiguous span of the CSR arrays. The warp streams that span through two
+// shared-memory windows of at most W entries with 1-D bulk copies
+// (cp.async.bulk, the TMA engine, completing on a transaction mbarrier):
+// the copy of window k+1 is in flight while the rows of window k are
+// multiplied, so the HBM stream no longer waits on the dependent gathers.
+// Rows read columns and values from shared memory, eight lanes per row
+// (lane s takes entries s, s+8, ...), and gather p through the read-only
+// path. Only the 16-byte aligned interior of a window's span is bulk-copied;
+// its ragged head and tail (under 16 bytes each) are loaded by lanes, so
+// nothing outside the span is read and any 4- or 8-byte aligned array
+// works. A row longer than a window is multiplied by the whole warp
+// straight from global memory. Window bounds depend only on the system's
+// row pointers, so sums are the same alone and in any batch. Every barrier
+// wait is bounded (2 s); on expiry the warp records an error, waits
+// (bounded) for its other copy and stops.
+constexpr int XR_MAX = 128;    // rows of one staged work entry (X_CHUNKS_VEC * 16)
+
+template <typename TV, int W>
+struct StageWarp {
+    static constexpr int CAP = W + 8;     // entries per window buffer (head/tail slack)
+    int32_t rps[XR_MAX + 4];              // row pointers of the work entry
+    unsigned long long mbar[2];           // one transaction barrier per buffer
+    int32_t c[2][CAP];
+    TV v[2][CAP];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *m) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(m)) : "memory");
+}
+// Initialised barriers visible to the async (bulk-copy) proxy.
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *m, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long *m, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(m)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Wait for the phase of the given parity to complete; false after 2 s, or
+// at once when another warp has already recorded an error in *err.
+__device__ bool mbar_wait(unsigned long long *m, uint32_t parity, const int *err) {
+    if (mbar_test(m, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (!mbar_test(m, parity))
+        if (globaltimer() - t0 > 2000000000ull || *(volatile const int *)err) return false;
+    return true;
+}
+// 1-D bulk copy global -> this CTA's shared memory, completing on m.
+// dst and src 16-byte aligned, bytes a non-zero multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          unsigned long long *m) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(m))
+        : "memory");
+}
+// First entry at or after k (last at or before k) whose address is 16-byte
+// aligned; base must be aligned to its element size.
+template <typename E>
+__device__ __forceinline__ int64_t entry_up16(const E *base, int64_t k) {
+    const uintptr_t a = (uintptr_t)(base + k);
+    return k + (int64_t)(((a + 15) & ~(uintptr_t)15) - a) / (int64_t)sizeof(E);
+}
+template <typename E>
+__device__ __forceinline__ int64_t entry_down16(const E *base, int64_t k) {
+    const uintptr_t a = (uintptr_t)(base + k);
+    return k - (int64_t)(a & 15) / (int64_t)sizeof(E);
+}
+
+// One window: rows [a, b) of the work entry, staged in buffer buf (-1: the
+// single long row a, read from global memory); entry k of the span sits at
+// index k - cb of the column buffer and k - vb of the value buffer.
+struct StageWin {
+    int a, b, buf;
+    int64_t cb, vb;
+};
+
+// Open the window starting at row a (warp-uniform; every lane calls): pick
+// its rows, start the bulk copies of its interior on the buffer's barrier
+// and load its head and tail.
+template <typename TV, int W>
+__device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32_t *ci,
+                                               const TV *va, int a, int nr, int lane,
+                                               int &nbuf) {
+    StageWin w;
+    w.a = a;
+    const int s0 = sm.rps[a];
+    const int64_t lim = (int64_t)s0 + W;
+    int b = a;
+    for (int t0 = a + 1; t0 <= nr; t0 += 32) {
+        const int t = t0 + lane;
+        // row pointers do not decrease: the rows that fit are a prefix
+        const unsigned m = __ballot_sync(0xffffffffu, t <= nr && sm.rps[t] <= lim);
+        if (m) b = t0 + __popc(m) - 1;
+        if (m != 0xffffffffu) break;
+    }
+    if (b == a) {   // row a alone is longer than a window
+        w.b = a + 1;
+        w.buf = -1;
+        w.cb = w.vb = 0;
+        return w;
+    }
+    w.b = b;
+    w.buf = nbuf;
+    nbuf ^= 1;
+    const int s1 = sm.rps[b];
+    constexpr int EC = 4, EV = 16 / (int)sizeof(TV);   // entries per 16 bytes
+    const int64_t ac = entry_up16(ci, s0), av = entry_up16(va, s0);
+    int64_t ec = entry_down16(ci, s1), ev = entry_down16(va, s1);
+    if (ec < ac) ec = ac;   // span without an aligned interior
+    if (ev < av) ev = av;
+    w.cb = ac - EC;
+    w.vb = av - EV;
+    int32_t *cs = sm.c[w.buf];
+    TV *vs = sm.v[w.buf];
+    const uint32_t bc = (uint32_t)(ec - ac) * 4u, bv = (uint32_t)(ev - av) * (uint32_t)sizeof(TV);
+    if (lane == 0) {
+        // earlier generic reads of this buffer before the async-proxy writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect(&sm.mbar[w.buf], bc + bv);
+        if (bc) bulk_load(cs + EC, ci + ac, bc, &sm.mbar[w.buf]);
+        if (bv) bulk_load(vs + EV, va + av, bv, &sm.mbar[w.buf]);
+    }
+    // head [s0, min(a16, s1)) and tail [max(e16, a16), s1): < 16 bytes each
+    const int sl = lane & 3;
+    int64_t k = -1;
+    if (lane < 4) k = s0 + sl < ac && s0 + sl < s1 ? s0 + sl : -1;
+    else if (lane < 8) k = ec + sl < s1 ? ec + sl : -1;
+    if (k >= 0) cs[k - w.cb] = __ldg(ci + k);
+    k = -1;
+    if (lane >= 8 && lane < 12) k = s0 + sl < av && s0 + sl < s1 ? s0 + sl : -1;
+    else if (lane >= 12 && lane < 16) k = ev + sl < s1 ? ev + sl : -1;
+    if (k >= 0) vs[k - w.vb] = __ldg(va + k);
+    return w;
+}
+
+// q = A p and p.q over rows [r0, r1) of one scalar system (A phase), the
+// matrix streamed through the warp's staging windows. DIFF: the FP32
+// difference-form operator (diagonal slot = row sum), applied as
+// s_i p_i + sum_j a_ij (p_j - p_i).
+template <typename T, bool DIFF, int W>
+__device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
+                               int lane, double part[4], StageWarp<T, W> &sm,
+                               const int *err, int *fail) {
+    constexpr int H = 2, U = 4;
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
+    T *q = (T *)S.q;
+    const T *va = (const T *)S.vsoa;
+    const int32_t *ci = S.ci;
+    const int nr = (int)(r1 - r0);
+    const int sub = lane & 7, grp = lane >> 3;
+    T pq = 0;
+    for (int t = lane; t <= nr; t += 32) sm.rps[t] = __ldg(S.rp + r0 + t);
+    if (lane == 0) {
+        mbar_init(&sm.mbar[0]);
+        mbar_init(&sm.mbar[1]);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    int nbuf = 0;
+    uint32_t par = 0;   // bit b: parity of buffer b's next phase
+    StageWin w = stage_open(sm, ci, va, 0, nr, lane, nbuf);
+    while (w.a < nr) {
+        StageWin nx;
+        nx.a = nx.b = nr;
+        nx.buf = -1;
+        nx.cb = nx.vb = 0;
+        if (w.b < nr) nx = stage_open(sm, ci, va, w.b, nr, lane, nbuf);
+        if (w.buf >= 0) {
+            const bool ok = mbar_wait(&sm.mbar[w.buf], (par >> w.buf) & 1u, err);
+            par ^= 1u << w.buf;
+            __syncwarp();   // head and tail stores of the window visible
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (nx.buf >= 0) {   // its own copy still in flight: bounded wait
+                    const unsigned long long t0 = globaltimer();
+                    while (!mbar_test(&sm.mbar[nx.buf], (par >> nx.buf) & 1u) &&
+                           globaltimer() - t0 < 2000000000ull) {
+                    }
+                }
+                *fail = 1;
+                break;
+            }
+            const int32_t *cs = sm.c[w.buf];
+            const T *vs = sm.v[w.buf];
+            for (int base = w.a; base < w.b; base += 4 * H) {
+                int rl[H], k[H], ke[H];
+                T pi[H], acc[H];
+#pragma unroll
+                for (int h = 0; h < H; ++h) {
+                    rl[h] = base + grp + 4 * h;
+                    const bool valid = rl[h] < w.b;
+                    const int rr = valid ? rl[h] : w.a;
+                    k[h] = sm.rps[rr] + sub;
+                    ke[h] = valid ? sm.rps[rr + 1] : 0;
+                    pi[h] = __ldg(pv + r0 + rr);
+                    acc[h] = 0;
+                }
+                while (true) {
+                    bool more = false;
+#pragma unroll
+                    for (int h = 0; h < H; ++h) more |= k[h] < ke[h];
+                    if (!more) break;
+                    int32_t c[H][U];
+                    T a[H][U], pj[H][U];
+#pragma unroll
+                    for (int h = 0; h < H; ++h)
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            const int kk = k[h] + 8 * e;
+                            const bool ok2 = kk < ke[h];
+                            c[h][e] = ok2 ? cs[kk - w.cb] : -1;
+                            a[h][e] = ok2 ? vs[kk - w.vb] : (T)0;
+                        }
+#pragma unroll
+                    for (int h = 0; h < H; ++h)
+#pragma unroll
+                        for (int e = 0; e < U; ++e)
+                            pj[h][e] = c[h][e] >= 0 ? __ldg(pv + c[h][e]) : (T)0;
+#pragma unroll
+                    for (int h = 0; h < H; ++h) {
+                        const int64_t row = r0 + rl[h];
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            T x = pj[h][e];
+                            if (DIFF) x = (c[h][e] == row) ? pi[h] : x - pi[h];
+                            acc[h] += a[h][e] * x;
+                        }
+                        k[h] += 8 * U;
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < H; ++h) {
+                    acc[h] = group_sum<8>(acc[h]);
+                    if (rl[h] < w.b && sub == 0) {
+                        q[r0 + rl[h]] = acc[h];
+                        pq += pi[h] * acc[h];
+                    }
+                }
+            }
+            __syncwarp();   // reads done before the buffer is refilled
+        } else {
+            const int64_t row = r0 + w.a;
+            const int kb = sm.rps[w.a], ke = sm.rps[w.a + 1];
+            const T pi = __ldg(pv + row);
+            T acc = 0;
+            for (int k = kb + lane; k < ke; k += 32) {
+                const int32_t c = __ldg(ci + k);
+                T x = __ldg(pv + c);
+                if (DIFF) x = (c == row) ? pi : x - pi;
+                acc += __ldg(va + k) * x;
+            }
+            acc = group_sum<32>(acc);
+            if (lane == 0) {
+                q[row] = acc;
+                pq += pi * acc;
+            }
+        }
+        w = nx;
+    }
+    part[0] += (double)pq;
+}
+
 // Entry-major working-precision copy of block values (AoS -> SoA).
 template <typename TI, typename TO, int B2>
 __global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict__ out) {
@@ -1281,6 +1563,51 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
+// k_gx for scalar systems with the bulk-staged A phase (W entries per
+// window); R and ZERO phases as in k_gx. Dynamic shared memory: GROUP
+// StageWarp<T, W> areas.
+template <typename T, int W> struct GxsOcc {
+    static constexpr int blocks = 3;
+};
+template <typename T, int W>
+constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarp<T, W>); }
+
+template <typename T, int W>
+__global__ void __launch_bounds__(32 * GROUP, (GxsOcc<T, W>::blocks))
+k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
+      const int2 *__restrict__ list, int n) {
+    extern __shared__ __align__(16) unsigned char gxs_area[];
+    pdl_wait();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
+    if (*(volatile const int *)&bar->err) return;           // a wait gave up
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * S.xrows;
+        const int64_t r1 = min(S.n, r0 + S.xrows);
+        if (ph == PH_A) {
+            StageWarp<T, W> &sm = reinterpret_cast<StageWarp<T, W> *>(gxs_area)[w];
+            int fail = 0;
+            phase_A_staged<T, sizeof(T) == 4, W>(S, &st[e.x], r0, r1, lane, part, sm,
+                                                 &bar->err, &fail);
+            if (fail && lane == 0) atomicExch(&bar->err, 2);
+        } else if (ph == PH_R) {
+            int bad = 0;
+            phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+        } else {
+            phase_zero<1>(S, r0, r1, lane);
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
 template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
 k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
@@ -1388,6 +1715,7 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
 
 constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
 constexpr int X_CHUNKS_VEC = 8;   // chunks per SpMV work entry, padded scalar rows
+static_assert(X_CHUNKS_VEC * 16 <= XR_MAX, "staged work entries hold at most XR_MAX rows");
 
 // Start of a graph-scheduled solve: every system active, no barrier error.
 __global__ void k_plan_start(GridBar *bar, int n_systems) {
@@ -1406,7 +1734,8 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, GridBar *bar, unsigned
         const unsigned r = bar->rounds + 1;
         bar->rounds = r;
         const int act = *(volatile int *)&bar->active;
-        cudaGraphSetConditional(h, (act > 0 && r < max_rounds) ? 1u : 0u);
+        const int err = *(volatile int *)&bar->err;
+        cudaGraphSetConditional(h, (act > 0 && r < max_rounds && err == 0) ? 1u : 0u);
     }
 }
 }  // namespace cfem
@@ -1451,6 +1780,42 @@ static void glaunch(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned 
     cfg.attrs = at;
     cfg.numAttrs = pdl ? 1 : 0;
     (void)cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// glaunch with dynamic shared memory.
+template <typename... KArgs, typename... Args>
+static void glaunch_smem(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block,
+                         size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    (void)cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// Staging-window sizes of the bulk-staged scalar SpMV per precision:
+// stage 1 = about 4 KB windows (3 blocks of 8 warps fill shared memory),
+// stage 2 = about 2 KB (more L1 left for the gathers of p).
+constexpr int STAGE_W32_1 = 512, STAGE_W64_1 = 352;
+constexpr int STAGE_W32_2 = 256, STAGE_W64_2 = 176;
+
+template <typename T, int W>
+static int gxs_prepare() {
+    const size_t bytes = gxs_smem<T, W>();
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)bytes));
+    // shared-memory share of the unified L1 for three resident blocks
+    int pct = (int)((3 * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+    if (pct > 100) pct = 100;
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   pct));
+    return CFEM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1746,6 +2111,12 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // reduction. The SpMV of the first iteration is bracketed by the
     // timing events when tev is given.
     const bool use_pdl = ctx->pdl != 0;
+    // scalar SpMV: bulk-staged windows (1, 2) or the register path (0)
+    const int stage = ctx->spmv_stage;
+    if (stage == 1 && !la[0].empty()) CFEM_TRY((gxs_prepare<double, STAGE_W64_1>()));
+    if (stage == 2 && !la[0].empty()) CFEM_TRY((gxs_prepare<double, STAGE_W64_2>()));
+    if (stage == 1 && !la[2].empty()) CFEM_TRY((gxs_prepare<float, STAGE_W32_1>()));
+    if (stage == 2 && !la[2].empty()) CFEM_TRY((gxs_prepare<float, STAGE_W32_2>()));
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
         const bool pdl = use_pdl && !t0;
@@ -1766,9 +2137,17 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
-            if (t == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 0 && stage == 1)
+                glaunch_smem(p, k_gxs<double, STAGE_W64_1>, g, 32 * GROUP, gxs_smem<double, STAGE_W64_1>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 0 && stage == 2)
+                glaunch_smem(p, k_gxs<double, STAGE_W64_2>, g, 32 * GROUP, gxs_smem<double, STAGE_W64_2>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 1)
+                glaunch_smem(p, k_gxs<float, STAGE_W32_1>, g, 32 * GROUP, gxs_smem<float, STAGE_W32_1>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 2)
+                glaunch_smem(p, k_gxs<float, STAGE_W32_2>, g, 32 * GROUP, gxs_smem<float, STAGE_W32_2>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 2) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
@@ -1957,6 +2336,8 @@ static int plan_run(cfem_pcg_plan *P, cfem_solve_stats *stats, cudaStream_t s) {
         stats[i].spmv_samples = spmv_samples;
         stats[i].pad2_ = 0;
     }
+    CFEM_CHECK(h_err != 2, CFEM_ERR_TIMEOUT,
+               "solver SpMV bulk-copy wait timed out (device wait bound reached)");
     CFEM_CHECK(h_err == 0, CFEM_ERR_TIMEOUT,
                "solver grid barrier timed out (device wait bound reached)");
     return CFEM_OK;

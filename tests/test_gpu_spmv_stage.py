@@ -1,0 +1,132 @@
+"""Scalar SpMV of the graph scheduler with the matrix streamed through
+shared-memory windows by 1-D bulk copies (staging 1 and 2) against the
+register path (staging 0) and a direct FP64 solve: the same answers, bitwise
+batch independence, rows longer than a window, and CSR arrays that do not
+start on a 16-byte boundary."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    return torch
+
+
+def _hub_matrix(n, hub_degrees, seed):
+    """SPD scalar matrix: a chain Laplacian plus hub nodes each coupled to
+    `deg` random nodes (rows from a few entries up to far longer than a
+    staging window), made strictly diagonally dominant."""
+    rng = np.random.default_rng(seed)
+    r = list(range(n - 1))
+    c = list(range(1, n))
+    w = list(-rng.uniform(0.5, 1.5, n - 1))
+    hubs = rng.choice(n, size=len(hub_degrees), replace=False)
+    for h, deg in zip(hubs, hub_degrees):
+        others = rng.choice(np.setdiff1d(np.arange(n), [h]), size=deg, replace=False)
+        r += [int(h)] * deg
+        c += [int(o) for o in others]
+        w += list(-rng.uniform(0.1, 1.0, deg))
+    off = sp.coo_matrix((w, (r, c)), shape=(n, n)).tocsr()
+    off = off + off.T
+    diag = np.asarray(abs(off).sum(axis=1)).ravel() + rng.uniform(0.5, 2.0, n)
+    A = (off + sp.diags(diag)).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    return A
+
+
+def _offset_copy(torch, arr, dtype, offset):
+    """Device copy of arr starting `offset` elements into a larger buffer
+    (so the data does not start on a 16-byte boundary when offset > 0)."""
+    buf = torch.zeros(arr.size + offset + 4, dtype=dtype, device="cuda")
+    buf[offset:offset + arr.size] = torch.as_tensor(arr, dtype=dtype, device="cuda")
+    return buf[offset:offset + arr.size]
+
+
+def _system(torch, rt, A, b, offset):
+    from cloudfem_b200.device import BlockSystem
+    n = A.shape[0]
+    rp = torch.as_tensor(A.indptr.astype(np.int32), device="cuda")
+    col = _offset_copy(torch, A.indices.astype(np.int32), torch.int32, offset)
+    v64 = _offset_copy(torch, A.data, torch.float64, offset)
+    bb = torch.as_tensor(b, device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s = BlockSystem(rt, n, 1, rp, col, v64, bb, x)
+    if offset:
+        v32 = s.ensure_fp32()
+        s.vals32 = _offset_copy(torch, v32.cpu().numpy(), torch.float32, offset)
+    return s
+
+
+def _solve(rt, systems, mode, rtol, stage):
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import pcg
+    N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_GRAPH))
+    before = rt.get_param(N.PARAM_SPMV_STAGE)
+    try:
+        rt.set_param(N.PARAM_SPMV_STAGE, stage)
+        for s in systems:
+            s.x.zero_()
+        res = pcg(systems, mode, rtol, 20000)
+    finally:
+        rt.set_param(N.PARAM_SPMV_STAGE, before)
+        N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
+    for r in res:
+        assert r.status == N.CFEM_OK, r
+    return res, [s.x.cpu().numpy() for s in systems]
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_staged_spmv_matches_direct_solve(torch, mode):
+    """Hub rows of 200, 400 and 1,500 entries (the last two longer than the
+    FP64 window, the last longer than every window), arrays at 4-, 8- and
+    12-byte offsets: every staging gives the direct solve's answer, and the
+    two staged window sizes agree with the register path."""
+    from cloudfem_b200 import _native as N
+    rt = N.runtime()
+    md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
+    rtol = 1e-12 if mode == "fp64" else 1e-10
+    tol = 1e-9 if mode == "fp64" else 1e-7   # condition number ~1e3
+    for offset in (0, 1, 3):
+        A = _hub_matrix(3000 + 7 * offset, [200, 400, 1500], seed=offset)
+        b = np.random.default_rng(10 + offset).normal(size=A.shape[0])
+        ref = spla.spsolve(A.tocsc(), b)
+        sys_ = _system(torch, rt, A, b, offset)
+        xs = {}
+        for stage in (0, 1, 2):
+            _, (x,) = _solve(rt, [sys_], md, rtol, stage)
+            err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+            assert err <= tol, (offset, stage, err)
+            xs[stage] = x
+        for stage in (1, 2):
+            d = np.linalg.norm(xs[stage] - xs[0]) / np.linalg.norm(xs[0])
+            assert d <= tol, (offset, stage, d)
+
+
+@pytest.mark.parametrize("stage", [1, 2])
+def test_staged_spmv_batch_equals_solo_bitwise(torch, stage):
+    """On the graph scheduler with staged SpMV, each system's answer is
+    bitwise the same alone, in a batch, and on a repeat."""
+    from cloudfem_b200 import _native as N
+    rt = N.runtime()
+    mats = [_hub_matrix(n, degs, seed=n) for n, degs in
+            ((2500, [600]), (1800, []), (4100, [50, 900]))]
+    systems = [_system(torch, rt, A, np.ones(A.shape[0]), off)
+               for A, off in zip(mats, (0, 1, 2))]
+    for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
+        rb, xb = _solve(rt, systems, md, 1e-10, stage)
+        for i, s in enumerate(systems):
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage)
+            assert r[0].iterations == rb[i].iterations
+            assert np.array_equal(x, xb[i]), (md, i)
+        _, xr = _solve(rt, systems, md, 1e-10, stage)
+        for i in range(len(systems)):
+            assert np.array_equal(xr[i], xb[i])
