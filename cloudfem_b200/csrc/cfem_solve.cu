@@ -1179,12 +1179,17 @@ __device__ __forceinline__ bool mbar_test(unsigned long long *m, uint32_t parity
 }
 // Wait for the phase of the given parity to complete; false after 2 s, or
 // at once when another warp has already recorded an error in *err.
+// The clock and the error word are read every 64 tests only, so that a
+// completed phase is seen as soon as possible.
 __device__ bool mbar_wait(unsigned long long *m, uint32_t parity, const int *err) {
     if (mbar_test(m, parity)) return true;
     const unsigned long long t0 = globaltimer();
-    while (!mbar_test(m, parity))
-        if (globaltimer() - t0 > 2000000000ull || *(volatile const int *)err) return false;
-    return true;
+    for (unsigned it = 1;; ++it) {
+        if (mbar_test(m, parity)) return true;
+        if ((it & 63) == 0 &&
+            (globaltimer() - t0 > 2000000000ull || *(volatile const int *)err))
+            return false;
+    }
 }
 // 1-D bulk copy global -> this CTA's shared memory, completing on m.
 // dst and src 16-byte aligned, bytes a non-zero multiple of 16.
