@@ -1028,9 +1028,9 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
                     help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
-    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2],
-                    help="scalar SpMV: 1 bulk-staged 4 KB windows (library default), "
-                         "2 bulk-staged 2 KB windows, 0 register path")
+    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1],
+                    help="scalar SpMV: 1 bulk-staged shared-memory windows (library "
+                         "default), 0 register path")
     args = ap.parse_args()
     global SPMV_STAGE
     SPMV_STAGE = args.spmv_stage

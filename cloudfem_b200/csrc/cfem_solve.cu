@@ -1123,31 +1123,38 @@ __global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
 
 // ---------------------------------------------------------------------------
 // Bulk-staged scalar SpMV (graph scheduler, A phase of scalar systems).
-// A warp owns one work entry of up to XR_MAX rows, whose entries are one
-// contiguous span of the CSR arrays. The warp streams that span through two
-// shared-memory windows of at most W entries with 1-D bulk copies
-// (cp.async.bulk, the TMA engine, completing on a transaction mbarrier):
-// the copy of window k+1 is in flight while the rows of window k are
-// multiplied, so the HBM stream no longer waits on the dependent gathers.
-// Rows read columns and values from shared memory, eight lanes per row
-// (lane s takes entries s, s+8, ...), and gather p through the read-only
-// path. Only the 16-byte aligned interior of a window's span is bulk-copied;
-// its ragged head and tail (under 16 bytes each) are loaded by lanes, so
-// nothing outside the span is read and any 4- or 8-byte aligned array
-// works. A row longer than a window is multiplied by the whole warp
-// straight from global memory. Window bounds depend only on the system's
-// row pointers, so sums are the same alone and in any batch. Every barrier
-// wait is bounded (2 s); on expiry the warp records an error, waits
+// A warp owns one work entry of up to XR_MAX rows. Their units (16-byte
+// groups of four entries) in the unit-padded copy (row i starting at unit
+// (rp[i] + 3 i + 3) / 4, padding entries with column i and value 0) are one
+// contiguous span, which the warp streams through two shared-memory windows
+// of at most W units with 1-D bulk copies (cp.async.bulk, the TMA engine,
+// completing on a transaction mbarrier): the copy of window k+1 is in
+// flight while the rows of window k are multiplied, so the HBM stream no
+// longer waits on the dependent gathers. Every row starts on a unit, so
+// lanes read whole units with 128-bit shared-memory loads and need no
+// per-entry bounds tests; LPR lanes share a row (4 for rows of up to 16
+// entries, 8 above), lane s taking units s, s + LPR, .... Windows hold a
+// whole number of row steps (32 / LPR groups x H rows) except at the end of
+// the work entry. A row longer than a window is multiplied by the whole
+// warp straight from global memory. Window bounds depend only on the
+// system's row pointers, so sums are the same alone and in any batch. Every
+// barrier wait is bounded (2 s); on expiry the warp records an error, waits
 // (bounded) for its other copy and stops.
 constexpr int XR_MAX = 128;    // rows of one staged work entry (X_CHUNKS_VEC * 16)
 
+struct alignas(16) DUnit {     // four FP64 values
+    double2 lo, hi;
+};
+template <typename TV> struct ValUnit;
+template <> struct ValUnit<float> { using type = float4; };
+template <> struct ValUnit<double> { using type = DUnit; };
+
 template <typename TV, int W>
 struct StageWarp {
-    static constexpr int CAP = W + 8;     // entries per window buffer (head/tail slack)
-    int32_t rps[XR_MAX + 4];              // row pointers of the work entry
-    unsigned long long mbar[2];           // one transaction barrier per buffer
-    int32_t c[2][CAP];
-    TV v[2][CAP];
+    int32_t rps[XR_MAX + 4];                    // row pointers of the work entry
+    unsigned long long mbar[2];                 // one transaction barrier per buffer
+    int4 c[2][W];                               // column units
+    typename ValUnit<TV>::type v[2][W];         // value units
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -1178,9 +1185,9 @@ __device__ __forceinline__ bool mbar_test(unsigned long long *m, uint32_t parity
     return done != 0;
 }
 // Wait for the phase of the given parity to complete; false after 2 s, or
-// at once when another warp has already recorded an error in *err.
-// The clock and the error word are read every 64 tests only, so that a
-// completed phase is seen as soon as possible.
+// when another warp has already recorded an error in *err. The clock and
+// the error word are read every 64 tests only, so that a completed phase is
+// seen as soon as possible.
 __device__ bool mbar_wait(unsigned long long *m, uint32_t parity, const int *err) {
     if (mbar_test(m, parity)) return true;
     const unsigned long long t0 = globaltimer();
@@ -1201,102 +1208,86 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         "l"(src), "r"(bytes), "r"(smem_addr(m))
         : "memory");
 }
-// First entry at or after k (last at or before k) whose address is 16-byte
-// aligned; base must be aligned to its element size.
-template <typename E>
-__device__ __forceinline__ int64_t entry_up16(const E *base, int64_t k) {
-    const uintptr_t a = (uintptr_t)(base + k);
-    return k + (int64_t)(((a + 15) & ~(uintptr_t)15) - a) / (int64_t)sizeof(E);
-}
-template <typename E>
-__device__ __forceinline__ int64_t entry_down16(const E *base, int64_t k) {
-    const uintptr_t a = (uintptr_t)(base + k);
-    return k - (int64_t)(a & 15) / (int64_t)sizeof(E);
-}
+
+// First unit of global row i whose entries start at kb (unit-padded copy).
+__device__ __forceinline__ int64_t unit_start(int64_t kb, int64_t i) { return (kb + 3 * i + 3) >> 2; }
 
 // One window: rows [a, b) of the work entry, staged in buffer buf (-1: the
-// single long row a, read from global memory); entry k of the span sits at
-// index k - cb of the column buffer and k - vb of the value buffer.
+// single long row a, read from global memory); unit ub of the copy sits at
+// index 0 of the buffer.
 struct StageWin {
     int a, b, buf;
-    int64_t cb, vb;
+    int64_t ub;
 };
 
 // Open the window starting at row a (warp-uniform; every lane calls): pick
-// its rows, start the bulk copies of its interior on the buffer's barrier
-// and load its head and tail.
-template <typename TV, int W>
-__device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32_t *ci,
-                                               const TV *va, int a, int nr, int lane,
-                                               int &nbuf) {
+// its rows and start the bulk copies of their units on the buffer's barrier.
+// SR: rows per processing step.
+template <typename TV, int W, int SR>
+__device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32_t *ci4,
+                                               const TV *va4, int64_t r0, int a, int nr,
+                                               int lane, int &nbuf) {
     StageWin w;
     w.a = a;
-    const int s0 = sm.rps[a];
-    const int64_t lim = (int64_t)s0 + W;
+    w.ub = unit_start(sm.rps[a], r0 + a);
+    const int64_t lim = w.ub + W;
     int b = a;
     for (int t0 = a + 1; t0 <= nr; t0 += 32) {
         const int t = t0 + lane;
-        // row pointers do not decrease: the rows that fit are a prefix
-        const unsigned m = __ballot_sync(0xffffffffu, t <= nr && sm.rps[t] <= lim);
+        // unit starts do not decrease: the rows that fit are a prefix
+        const unsigned m =
+            __ballot_sync(0xffffffffu, t <= nr && unit_start(sm.rps[t], r0 + t) <= lim);
         if (m) b = t0 + __popc(m) - 1;
         if (m != 0xffffffffu) break;
     }
     if (b == a) {   // row a alone is longer than a window
         w.b = a + 1;
         w.buf = -1;
-        w.cb = w.vb = 0;
         return w;
     }
+    if (b < nr && b - a >= SR) b = a + (b - a) / SR * SR;   // whole steps
     w.b = b;
     w.buf = nbuf;
     nbuf ^= 1;
-    const int s1 = sm.rps[b];
-    constexpr int EC = 4, EV = 16 / (int)sizeof(TV);   // entries per 16 bytes
-    const int64_t ac = entry_up16(ci, s0), av = entry_up16(va, s0);
-    int64_t ec = entry_down16(ci, s1), ev = entry_down16(va, s1);
-    if (ec < ac) ec = ac;   // span without an aligned interior
-    if (ev < av) ev = av;
-    w.cb = ac - EC;
-    w.vb = av - EV;
-    int32_t *cs = sm.c[w.buf];
-    TV *vs = sm.v[w.buf];
-    const uint32_t bc = (uint32_t)(ec - ac) * 4u, bv = (uint32_t)(ev - av) * (uint32_t)sizeof(TV);
+    const uint32_t nu = (uint32_t)(unit_start(sm.rps[b], r0 + b) - w.ub);
     if (lane == 0) {
         // earlier generic reads of this buffer before the async-proxy writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t bc = nu * 16u, bv = nu * 4u * (uint32_t)sizeof(TV);
         mbar_expect(&sm.mbar[w.buf], bc + bv);
-        if (bc) bulk_load(cs + EC, ci + ac, bc, &sm.mbar[w.buf]);
-        if (bv) bulk_load(vs + EV, va + av, bv, &sm.mbar[w.buf]);
+        if (nu) {
+            bulk_load(&sm.c[w.buf][0], ci4 + 4 * w.ub, bc, &sm.mbar[w.buf]);
+            bulk_load(&sm.v[w.buf][0], va4 + 4 * w.ub, bv, &sm.mbar[w.buf]);
+        }
     }
-    // head [s0, min(a16, s1)) and tail [max(e16, a16), s1): < 16 bytes each
-    const int sl = lane & 3;
-    int64_t k = -1;
-    if (lane < 4) k = s0 + sl < ac && s0 + sl < s1 ? s0 + sl : -1;
-    else if (lane < 8) k = ec + sl < s1 ? ec + sl : -1;
-    if (k >= 0) cs[k - w.cb] = __ldg(ci + k);
-    k = -1;
-    if (lane >= 8 && lane < 12) k = s0 + sl < av && s0 + sl < s1 ? s0 + sl : -1;
-    else if (lane >= 12 && lane < 16) k = ev + sl < s1 ? ev + sl : -1;
-    if (k >= 0) vs[k - w.vb] = __ldg(va + k);
     return w;
 }
 
+__device__ __forceinline__ void unit_vals(const float4 &u, float a[4]) {
+    a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w;
+}
+__device__ __forceinline__ void unit_vals(const DUnit &u, double a[4]) {
+    a[0] = u.lo.x; a[1] = u.lo.y; a[2] = u.hi.x; a[3] = u.hi.y;
+}
+
 // q = A p and p.q over rows [r0, r1) of one scalar system (A phase), the
-// matrix streamed through the warp's staging windows. DIFF: the FP32
-// difference-form operator (diagonal slot = row sum), applied as
-// s_i p_i + sum_j a_ij (p_j - p_i).
-template <typename T, bool DIFF, int W>
+// unit-padded matrix streamed through the warp's staging windows. DIFF: the
+// FP32 difference-form operator (diagonal slot = row sum), applied as
+// s_i p_i + sum_j a_ij (p_j - p_i); padding entries (column i, value 0) add
+// nothing either way.
+template <typename T, bool DIFF, int W, int LPR>
 __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
                                int lane, double part[4], StageWarp<T, W> &sm,
                                const int *err, int *fail) {
-    constexpr int H = 2, U = 4;
+    constexpr int NG = 32 / LPR, H = sizeof(T) == 8 ? 1 : 2, SR = NG * H;
+    using VU = typename ValUnit<T>::type;
     const int pbuf = vcgi(&st->pbuf);
     const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
     T *q = (T *)S.q;
-    const T *va = (const T *)S.vsoa;
-    const int32_t *ci = S.ci;
+    const T *va4 = (const T *)S.va4;
+    const int32_t *ci4 = S.ci4;
     const int nr = (int)(r1 - r0);
-    const int sub = lane & 7, grp = lane >> 3;
+    const int sub = lane % LPR, grp = lane / LPR;
     T pq = 0;
     for (int t = lane; t <= nr; t += 32) sm.rps[t] = __ldg(S.rp + r0 + t);
     if (lane == 0) {
@@ -1307,17 +1298,16 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
     __syncwarp();
     int nbuf = 0;
     uint32_t par = 0;   // bit b: parity of buffer b's next phase
-    StageWin w = stage_open(sm, ci, va, 0, nr, lane, nbuf);
+    StageWin w = stage_open<T, W, SR>(sm, ci4, va4, r0, 0, nr, lane, nbuf);
     while (w.a < nr) {
         StageWin nx;
         nx.a = nx.b = nr;
         nx.buf = -1;
-        nx.cb = nx.vb = 0;
-        if (w.b < nr) nx = stage_open(sm, ci, va, w.b, nr, lane, nbuf);
+        nx.ub = 0;
+        if (w.b < nr) nx = stage_open<T, W, SR>(sm, ci4, va4, r0, w.b, nr, lane, nbuf);
         if (w.buf >= 0) {
             const bool ok = mbar_wait(&sm.mbar[w.buf], (par >> w.buf) & 1u, err);
             par ^= 1u << w.buf;
-            __syncwarp();   // head and tail stores of the window visible
             if (!__all_sync(0xffffffffu, ok)) {
                 if (nx.buf >= 0) {   // its own copy still in flight: bounded wait
                     const unsigned long long t0 = globaltimer();
@@ -1328,57 +1318,68 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
                 *fail = 1;
                 break;
             }
-            const int32_t *cs = sm.c[w.buf];
-            const T *vs = sm.v[w.buf];
-            for (int base = w.a; base < w.b; base += 4 * H) {
-                int rl[H], k[H], ke[H];
+            const int4 *cs = sm.c[w.buf];
+            const VU *vs = sm.v[w.buf];
+            for (int base = w.a; base < w.b; base += SR) {
+                int rl[H], u[H], ue[H];
                 T pi[H], acc[H];
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
-                    rl[h] = base + grp + 4 * h;
+                    rl[h] = base + grp + NG * h;
                     const bool valid = rl[h] < w.b;
                     const int rr = valid ? rl[h] : w.a;
-                    k[h] = sm.rps[rr] + sub;
-                    ke[h] = valid ? sm.rps[rr + 1] : 0;
+                    const int kb = sm.rps[rr];
+                    const int len = valid ? sm.rps[rr + 1] - kb : 0;
+                    const int u0 = (int)(unit_start(kb, r0 + rr) - w.ub);
+                    u[h] = u0 + sub;
+                    ue[h] = u0 + ((len + 3) >> 2);
                     pi[h] = __ldg(pv + r0 + rr);
                     acc[h] = 0;
                 }
                 while (true) {
                     bool more = false;
 #pragma unroll
-                    for (int h = 0; h < H; ++h) more |= k[h] < ke[h];
+                    for (int h = 0; h < H; ++h) more |= u[h] < ue[h];
                     if (!more) break;
-                    int32_t c[H][U];
-                    T a[H][U], pj[H][U];
+                    // columns, then the gathers, then the values: fewer
+                    // registers live across the gathers
+                    int4 cc[H];
 #pragma unroll
                     for (int h = 0; h < H; ++h)
-#pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            const int kk = k[h] + 8 * e;
-                            const bool ok2 = kk < ke[h];
-                            c[h][e] = ok2 ? cs[kk - w.cb] : -1;
-                            a[h][e] = ok2 ? vs[kk - w.vb] : (T)0;
-                        }
-#pragma unroll
-                    for (int h = 0; h < H; ++h)
-#pragma unroll
-                        for (int e = 0; e < U; ++e)
-                            pj[h][e] = c[h][e] >= 0 ? __ldg(pv + c[h][e]) : (T)0;
+                        if (u[h] < ue[h]) cc[h] = cs[u[h]];
+                    T pj[H][4];
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
-                        const int64_t row = r0 + rl[h];
+                        const bool on = u[h] < ue[h];
+                        pj[h][0] = on ? __ldg(pv + cc[h].x) : (T)0;
+                        pj[h][1] = on ? __ldg(pv + cc[h].y) : (T)0;
+                        pj[h][2] = on ? __ldg(pv + cc[h].z) : (T)0;
+                        pj[h][3] = on ? __ldg(pv + cc[h].w) : (T)0;
+                    }
+                    VU vv[H];
 #pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            T x = pj[h][e];
-                            if (DIFF) x = (c[h][e] == row) ? pi[h] : x - pi[h];
-                            acc[h] += a[h][e] * x;
+                    for (int h = 0; h < H; ++h)
+                        if (u[h] < ue[h]) vv[h] = vs[u[h]];
+#pragma unroll
+                    for (int h = 0; h < H; ++h) {
+                        if (u[h] < ue[h]) {
+                            T a[4];
+                            unit_vals(vv[h], a);
+                            const int c4[4] = {cc[h].x, cc[h].y, cc[h].z, cc[h].w};
+                            const int row = (int)(r0 + rl[h]);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                T x = pj[h][e];
+                                if (DIFF) x = (c4[e] == row) ? pi[h] : x - pi[h];
+                                acc[h] += a[e] * x;
+                            }
                         }
-                        k[h] += 8 * U;
+                        u[h] += LPR;
                     }
                 }
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
-                    acc[h] = group_sum<8>(acc[h]);
+                    acc[h] = group_sum<LPR>(acc[h]);
                     if (rl[h] < w.b && sub == 0) {
                         q[r0 + rl[h]] = acc[h];
                         pq += pi[h] * acc[h];
@@ -1388,14 +1389,28 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
             __syncwarp();   // reads done before the buffer is refilled
         } else {
             const int64_t row = r0 + w.a;
-            const int kb = sm.rps[w.a], ke = sm.rps[w.a + 1];
+            const int kb = sm.rps[w.a], len = sm.rps[w.a + 1] - kb;
+            const int64_t u0 = unit_start(kb, row), nu = (len + 3) >> 2;
             const T pi = __ldg(pv + row);
             T acc = 0;
-            for (int k = kb + lane; k < ke; k += 32) {
-                const int32_t c = __ldg(ci + k);
-                T x = __ldg(pv + c);
-                if (DIFF) x = (c == row) ? pi : x - pi;
-                acc += __ldg(va + k) * x;
+            for (int64_t uu = lane; uu < nu; uu += 32) {
+                const int4 cc = __ldg((const int4 *)ci4 + u0 + uu);
+                T a[4];
+                if (sizeof(T) == 4) {
+                    const float4 f = __ldg((const float4 *)va4 + u0 + uu);
+                    a[0] = (T)f.x; a[1] = (T)f.y; a[2] = (T)f.z; a[3] = (T)f.w;
+                } else {
+                    const double2 d0 = __ldg((const double2 *)va4 + 2 * (u0 + uu));
+                    const double2 d1 = __ldg((const double2 *)va4 + 2 * (u0 + uu) + 1);
+                    a[0] = (T)d0.x; a[1] = (T)d0.y; a[2] = (T)d1.x; a[3] = (T)d1.y;
+                }
+                const int c4[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    T x = __ldg(pv + c4[e]);
+                    if (DIFF) x = (c4[e] == row) ? pi : x - pi;
+                    acc += a[e] * x;
+                }
             }
             acc = group_sum<32>(acc);
             if (lane == 0) {
@@ -1568,19 +1583,20 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
-// k_gx for scalar systems with the bulk-staged A phase (W entries per
-// window); R and ZERO phases as in k_gx. Dynamic shared memory: GROUP
-// StageWarp<T, W> areas.
-template <typename T, int W> struct GxsOcc {
-    static constexpr int blocks = 3;
-};
-template <typename T, int W>
-constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarp<T, W>); }
+// k_gx for scalar systems with the bulk-staged A phase (windows of W
+// units, LPR lanes per row); R and ZERO phases as in k_gx. Dynamic shared
+// memory: GROUP StageWarp<T, W> areas, about 70 KB, three blocks per SM.
+template <typename T> struct StageUnits;
+template <> struct StageUnits<float> { static constexpr int W = 128; };   // 2 x 4 KB per warp
+template <> struct StageUnits<double> { static constexpr int W = 88; };   // 2 x 4.1 KB per warp
+template <typename T>
+constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarp<T, StageUnits<T>::W>); }
 
-template <typename T, int W>
-__global__ void __launch_bounds__(32 * GROUP, (GxsOcc<T, W>::blocks))
+template <typename T, int LPR>
+__global__ void __launch_bounds__(32 * GROUP, 3)
 k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
       const int2 *__restrict__ list, int n) {
+    constexpr int W = StageUnits<T>::W;
     extern __shared__ __align__(16) unsigned char gxs_area[];
     pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1600,8 +1616,8 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
         if (ph == PH_A) {
             StageWarp<T, W> &sm = reinterpret_cast<StageWarp<T, W> *>(gxs_area)[w];
             int fail = 0;
-            phase_A_staged<T, sizeof(T) == 4, W>(S, &st[e.x], r0, r1, lane, part, sm,
-                                                 &bar->err, &fail);
+            phase_A_staged<T, sizeof(T) == 4, W, LPR>(S, &st[e.x], r0, r1, lane, part, sm,
+                                                      &bar->err, &fail);
             if (fail && lane == 0) atomicExch(&bar->err, 2);
         } else if (ph == PH_R) {
             int bad = 0;
@@ -1804,21 +1820,15 @@ static void glaunch_smem(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsi
     (void)cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// Staging-window sizes of the bulk-staged scalar SpMV per precision:
-// stage 1 = about 4 KB windows (3 blocks of 8 warps fill shared memory),
-// stage 2 = about 2 KB (more L1 left for the gathers of p).
-constexpr int STAGE_W32_1 = 512, STAGE_W64_1 = 352;
-constexpr int STAGE_W32_2 = 256, STAGE_W64_2 = 176;
-
-template <typename T, int W>
+template <typename T, int LPR>
 static int gxs_prepare() {
-    const size_t bytes = gxs_smem<T, W>();
-    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t bytes = gxs_smem<T>();
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, LPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)bytes));
     // shared-memory share of the unified L1 for three resident blocks
     int pct = (int)((3 * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
     if (pct > 100) pct = 100;
-    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, LPR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    pct));
     return CFEM_OK;
 }
@@ -2116,12 +2126,24 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // reduction. The SpMV of the first iteration is bracketed by the
     // timing events when tev is given.
     const bool use_pdl = ctx->pdl != 0;
-    // scalar SpMV: bulk-staged windows (1, 2) or the register path (0)
+    // scalar SpMV: bulk-staged windows (1) or the register path (0); lanes
+    // per row from the mean row length of the list's systems (4 up to 16
+    // entries, whole units of a P1 row; 8 above, Tet10 rows of ~27)
     const int stage = ctx->spmv_stage;
-    if (stage == 1 && !la[0].empty()) CFEM_TRY((gxs_prepare<double, STAGE_W64_1>()));
-    if (stage == 2 && !la[0].empty()) CFEM_TRY((gxs_prepare<double, STAGE_W64_2>()));
-    if (stage == 1 && !la[2].empty()) CFEM_TRY((gxs_prepare<float, STAGE_W32_1>()));
-    if (stage == 2 && !la[2].empty()) CFEM_TRY((gxs_prepare<float, STAGE_W32_2>()));
+    int lpr[4] = {8, 8, 8, 8};
+    for (int t = 0; t < 4; t += 2) {
+        double nz = 0.0, rows = 0.0;
+        for (int i = 0; i < n_systems; ++i)
+            if (hs[i].bs == 1 && (hs[i].mode == CFEM_SOLVE_MIXED) == (t == 2)) {
+                nz += (double)hs[i].nnzb;
+                rows += (double)hs[i].n;
+            }
+        if (rows > 0 && nz <= 16.0 * rows) lpr[t] = 4;
+    }
+    if (stage == 1 && !la[0].empty())
+        CFEM_TRY((lpr[0] == 4 ? gxs_prepare<double, 4>() : gxs_prepare<double, 8>()));
+    if (stage == 1 && !la[2].empty())
+        CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
         const bool pdl = use_pdl && !t0;
@@ -2143,13 +2165,9 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
             if (t == 0 && stage == 1)
-                glaunch_smem(p, k_gxs<double, STAGE_W64_1>, g, 32 * GROUP, gxs_smem<double, STAGE_W64_1>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 0 && stage == 2)
-                glaunch_smem(p, k_gxs<double, STAGE_W64_2>, g, 32 * GROUP, gxs_smem<double, STAGE_W64_2>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+                glaunch_smem(p, lpr[0] == 4 ? k_gxs<double, 4> : k_gxs<double, 8>, g, 32 * GROUP, gxs_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 1)
-                glaunch_smem(p, k_gxs<float, STAGE_W32_1>, g, 32 * GROUP, gxs_smem<float, STAGE_W32_1>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 2 && stage == 2)
-                glaunch_smem(p, k_gxs<float, STAGE_W32_2>, g, 32 * GROUP, gxs_smem<float, STAGE_W32_2>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+                glaunch_smem(p, lpr[2] == 4 ? k_gxs<float, 4> : k_gxs<float, 8>, g, 32 * GROUP, gxs_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);

@@ -173,11 +173,10 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * convergence). PDL: 1 (default) captures the solve graphs' kernels as
  * programmatic dependent launches (launch processing overlaps the previous
  * kernel's drain), 0 as plain launches. SPMV_STAGE: how the graph
- * scheduler's scalar SpMV reads the matrix: 1 (default) streams each work
- * entry's span through shared-memory windows of about 4 KB with 1-D bulk
- * copies (TMA), 2 the same with 2 KB windows, 0 reads a unit-padded copy
- * with vector loads into registers. get returns -1 for an unknown
- * parameter. */
+ * scheduler's scalar SpMV reads its unit-padded copy of the matrix: 1
+ * (default) streams each work entry's span through two shared-memory
+ * windows of about 4 KB per warp with 1-D bulk copies (TMA), 0 loads it into
+ * registers with vector loads. get returns -1 for an unknown parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
