@@ -1102,8 +1102,11 @@ __device__ void phase_A_vec1(const SysDev &S, const SysState *st, int64_t r0,
     part[0] += (double)pq;
 }
 
-// Unit-padded copy of a scalar CSR matrix for phase_A_vec1 / phase_R_vec1:
-// one warp per row, lanes writing consecutive entries.
+// Unit-padded copy of a scalar CSR matrix for phase_A_vec1, phase_R_vec1
+// and phase_A_staged: one warp per row, lanes writing consecutive entries.
+// The diagonal entry, when the row has one, moves to the row's first slot
+// (the others keep their order): the staged difference-form SpMV takes the
+// row sum from there instead of testing every column against the row.
 template <typename T>
 __global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
                        const int32_t *__restrict__ ci, const T *__restrict__ v,
@@ -1114,9 +1117,17 @@ __global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
         const int64_t kb = rp[i], len = rp[i + 1] - kb;
         const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
         const int64_t m = ((len + 3) >> 2) * 4;
+        int64_t dpos = -1;   // position of the diagonal entry
+        for (int64_t t0 = 0; t0 < len && dpos < 0; t0 += 32) {
+            const unsigned hit =
+                __ballot_sync(0xffffffffu, t0 + lane < len && ci[kb + t0 + lane] == (int32_t)i);
+            if (hit) dpos = t0 + __ffs(hit) - 1;
+        }
         for (int64_t t = lane; t < m; t += 32) {
-            ci4[o + t] = t < len ? ci[kb + t] : (int32_t)i;
-            v4[o + t] = t < len ? v[kb + t] : (T)0;
+            // slot t <- entry src: diagonal first, then the others in order
+            const int64_t src = dpos < 0 ? t : (t == 0 ? dpos : (t <= dpos ? t - 1 : t));
+            ci4[o + t] = t < len ? ci[kb + src] : (int32_t)i;
+            v4[o + t] = t < len ? v[kb + src] : (T)0;
         }
     }
 }
@@ -1151,7 +1162,8 @@ template <> struct ValUnit<double> { using type = DUnit; };
 
 template <typename TV, int W>
 struct StageWarp {
-    int32_t rps[XR_MAX + 4];                    // row pointers of the work entry
+    int2 row[XR_MAX + 4];                       // per row: first unit (from the
+                                                // entry's first), unit count
     unsigned long long mbar[2];                 // one transaction barrier per buffer
     int4 c[2][W];                               // column units
     typename ValUnit<TV>::type v[2][W];         // value units
@@ -1213,30 +1225,28 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 __device__ __forceinline__ int64_t unit_start(int64_t kb, int64_t i) { return (kb + 3 * i + 3) >> 2; }
 
 // One window: rows [a, b) of the work entry, staged in buffer buf (-1: the
-// single long row a, read from global memory); unit ub of the copy sits at
-// index 0 of the buffer.
+// single long row a, read from global memory); unit ub (counted from the
+// entry's first unit) sits at index 0 of the buffer.
 struct StageWin {
-    int a, b, buf;
-    int64_t ub;
+    int a, b, buf, ub;
 };
 
 // Open the window starting at row a (warp-uniform; every lane calls): pick
 // its rows and start the bulk copies of their units on the buffer's barrier.
-// SR: rows per processing step.
+// e0: the entry's first unit in the copy; SR: rows per processing step.
 template <typename TV, int W, int SR>
 __device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32_t *ci4,
-                                               const TV *va4, int64_t r0, int a, int nr,
+                                               const TV *va4, int64_t e0, int a, int nr,
                                                int lane, int &nbuf) {
     StageWin w;
     w.a = a;
-    w.ub = unit_start(sm.rps[a], r0 + a);
-    const int64_t lim = w.ub + W;
+    w.ub = sm.row[a].x;
+    const int lim = w.ub + W;
     int b = a;
     for (int t0 = a + 1; t0 <= nr; t0 += 32) {
         const int t = t0 + lane;
         // unit starts do not decrease: the rows that fit are a prefix
-        const unsigned m =
-            __ballot_sync(0xffffffffu, t <= nr && unit_start(sm.rps[t], r0 + t) <= lim);
+        const unsigned m = __ballot_sync(0xffffffffu, t <= nr && sm.row[t].x <= lim);
         if (m) b = t0 + __popc(m) - 1;
         if (m != 0xffffffffu) break;
     }
@@ -1249,15 +1259,16 @@ __device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32
     w.b = b;
     w.buf = nbuf;
     nbuf ^= 1;
-    const uint32_t nu = (uint32_t)(unit_start(sm.rps[b], r0 + b) - w.ub);
+    const uint32_t nu = (uint32_t)(sm.row[b].x - w.ub);
     if (lane == 0) {
         // earlier generic reads of this buffer before the async-proxy writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const uint32_t bc = nu * 16u, bv = nu * 4u * (uint32_t)sizeof(TV);
         mbar_expect(&sm.mbar[w.buf], bc + bv);
         if (nu) {
-            bulk_load(&sm.c[w.buf][0], ci4 + 4 * w.ub, bc, &sm.mbar[w.buf]);
-            bulk_load(&sm.v[w.buf][0], va4 + 4 * w.ub, bv, &sm.mbar[w.buf]);
+            const int64_t u = e0 + w.ub;
+            bulk_load(&sm.c[w.buf][0], ci4 + 4 * u, bc, &sm.mbar[w.buf]);
+            bulk_load(&sm.v[w.buf][0], va4 + 4 * u, bv, &sm.mbar[w.buf]);
         }
     }
     return w;
@@ -1272,9 +1283,11 @@ __device__ __forceinline__ void unit_vals(const DUnit &u, double a[4]) {
 
 // q = A p and p.q over rows [r0, r1) of one scalar system (A phase), the
 // unit-padded matrix streamed through the warp's staging windows. DIFF: the
-// FP32 difference-form operator (diagonal slot = row sum), applied as
-// s_i p_i + sum_j a_ij (p_j - p_i); padding entries (column i, value 0) add
-// nothing either way.
+// FP32 difference-form operator, q_i = s_i p_i + sum_j a_ij (p_j - p_i) with
+// the row sum s_i in the diagonal slot, which the padded copy puts first in
+// the row: every slot is applied as a (p_j - p_i) (the diagonal then adds
+// nothing) and the lane holding the row's first unit adds s_i p_i. Padding
+// slots (column i, value 0) add nothing either way.
 template <typename T, bool DIFF, int W, int LPR>
 __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
                                int lane, double part[4], StageWarp<T, W> &sm,
@@ -1288,8 +1301,13 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
     const int32_t *ci4 = S.ci4;
     const int nr = (int)(r1 - r0);
     const int sub = lane % LPR, grp = lane / LPR;
+    const int64_t e0 = unit_start(__ldg(S.rp + r0), r0);   // the entry's first unit
     T pq = 0;
-    for (int t = lane; t <= nr; t += 32) sm.rps[t] = __ldg(S.rp + r0 + t);
+    for (int t = lane; t <= nr; t += 32) {
+        const int64_t kb = __ldg(S.rp + r0 + t);
+        const int len = t < nr ? __ldg(S.rp + r0 + t + 1) - (int)kb : 0;
+        sm.row[t] = make_int2((int)(unit_start(kb, r0 + t) - e0), (len + 3) >> 2);
+    }
     if (lane == 0) {
         mbar_init(&sm.mbar[0]);
         mbar_init(&sm.mbar[1]);
@@ -1298,13 +1316,13 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
     __syncwarp();
     int nbuf = 0;
     uint32_t par = 0;   // bit b: parity of buffer b's next phase
-    StageWin w = stage_open<T, W, SR>(sm, ci4, va4, r0, 0, nr, lane, nbuf);
+    StageWin w = stage_open<T, W, SR>(sm, ci4, va4, e0, 0, nr, lane, nbuf);
     while (w.a < nr) {
         StageWin nx;
         nx.a = nx.b = nr;
         nx.buf = -1;
         nx.ub = 0;
-        if (w.b < nr) nx = stage_open<T, W, SR>(sm, ci4, va4, r0, w.b, nr, lane, nbuf);
+        if (w.b < nr) nx = stage_open<T, W, SR>(sm, ci4, va4, e0, w.b, nr, lane, nbuf);
         if (w.buf >= 0) {
             const bool ok = mbar_wait(&sm.mbar[w.buf], (par >> w.buf) & 1u, err);
             par ^= 1u << w.buf;
@@ -1322,20 +1340,20 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
             const VU *vs = sm.v[w.buf];
             for (int base = w.a; base < w.b; base += SR) {
                 int rl[H], u[H], ue[H];
-                T pi[H], acc[H];
+                T pi[H], acc[H], dg[H];
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
                     rl[h] = base + grp + NG * h;
                     const bool valid = rl[h] < w.b;
                     const int rr = valid ? rl[h] : w.a;
-                    const int kb = sm.rps[rr];
-                    const int len = valid ? sm.rps[rr + 1] - kb : 0;
-                    const int u0 = (int)(unit_start(kb, r0 + rr) - w.ub);
-                    u[h] = u0 + sub;
-                    ue[h] = u0 + ((len + 3) >> 2);
+                    const int2 ri = sm.row[rr];
+                    u[h] = ri.x - w.ub + sub;
+                    ue[h] = valid ? ri.x - w.ub + ri.y : 0;
                     pi[h] = __ldg(pv + r0 + rr);
                     acc[h] = 0;
+                    dg[h] = 0;
                 }
+                bool first = true;
                 while (true) {
                     bool more = false;
 #pragma unroll
@@ -1365,20 +1383,18 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
                         if (u[h] < ue[h]) {
                             T a[4];
                             unit_vals(vv[h], a);
-                            const int c4[4] = {cc[h].x, cc[h].y, cc[h].z, cc[h].w};
-                            const int row = (int)(r0 + rl[h]);
+                            if (DIFF && first && sub == 0) dg[h] = a[0];
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                T x = pj[h][e];
-                                if (DIFF) x = (c4[e] == row) ? pi[h] : x - pi[h];
-                                acc[h] += a[e] * x;
-                            }
+                            for (int e = 0; e < 4; ++e)
+                                acc[h] += a[e] * (DIFF ? pj[h][e] - pi[h] : pj[h][e]);
                         }
                         u[h] += LPR;
                     }
+                    first = false;
                 }
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
+                    if (DIFF) acc[h] += dg[h] * pi[h];   // s_i p_i, lane sub == 0 only
                     acc[h] = group_sum<LPR>(acc[h]);
                     if (rl[h] < w.b && sub == 0) {
                         q[r0 + rl[h]] = acc[h];
@@ -1389,8 +1405,7 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
             __syncwarp();   // reads done before the buffer is refilled
         } else {
             const int64_t row = r0 + w.a;
-            const int kb = sm.rps[w.a], len = sm.rps[w.a + 1] - kb;
-            const int64_t u0 = unit_start(kb, row), nu = (len + 3) >> 2;
+            const int64_t u0 = e0 + sm.row[w.a].x, nu = sm.row[w.a].y;
             const T pi = __ldg(pv + row);
             T acc = 0;
             for (int64_t uu = lane; uu < nu; uu += 32) {
@@ -1406,11 +1421,8 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
                 }
                 const int c4[4] = {cc.x, cc.y, cc.z, cc.w};
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    T x = __ldg(pv + c4[e]);
-                    if (DIFF) x = (c4[e] == row) ? pi : x - pi;
-                    acc += a[e] * x;
-                }
+                for (int e = 0; e < 4; ++e) acc += a[e] * (DIFF ? __ldg(pv + c4[e]) - pi : __ldg(pv + c4[e]));
+                if (DIFF && uu == 0) acc += a[0] * pi;   // the diagonal slot, first
             }
             acc = group_sum<32>(acc);
             if (lane == 0) {
@@ -1588,7 +1600,7 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
 // memory: GROUP StageWarp<T, W> areas, about 70 KB, three blocks per SM.
 template <typename T> struct StageUnits;
 template <> struct StageUnits<float> { static constexpr int W = 128; };   // 2 x 4 KB per warp
-template <> struct StageUnits<double> { static constexpr int W = 88; };   // 2 x 4.1 KB per warp
+template <> struct StageUnits<double> { static constexpr int W = 84; };   // 2 x 3.9 KB per warp
 template <typename T>
 constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarp<T, StageUnits<T>::W>); }
 
