@@ -1160,13 +1160,13 @@ template <typename TV> struct ValUnit;
 template <> struct ValUnit<float> { using type = float4; };
 template <> struct ValUnit<double> { using type = DUnit; };
 
-template <typename TV, int W>
+template <typename TV, int W, int NB>
 struct StageWarp {
     int2 row[XR_MAX + 4];                       // per row: first unit (from the
                                                 // entry's first), unit count
-    unsigned long long mbar[2];                 // one transaction barrier per buffer
-    int4 c[2][W];                               // column units
-    typename ValUnit<TV>::type v[2][W];         // value units
+    unsigned long long mbar[NB];                // one transaction barrier per buffer
+    int4 c[NB][W];                              // column units
+    typename ValUnit<TV>::type v[NB][W];        // value units
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -1234,8 +1234,8 @@ struct StageWin {
 // Open the window starting at row a (warp-uniform; every lane calls): pick
 // its rows and start the bulk copies of their units on the buffer's barrier.
 // e0: the entry's first unit in the copy; SR: rows per processing step.
-template <typename TV, int W, int SR>
-__device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32_t *ci4,
+template <typename TV, int W, int NB, int SR>
+__device__ __forceinline__ StageWin stage_open(StageWarp<TV, W, NB> &sm, const int32_t *ci4,
                                                const TV *va4, int64_t e0, int a, int nr,
                                                int lane, int &nbuf) {
     StageWin w;
@@ -1258,7 +1258,7 @@ __device__ __forceinline__ StageWin stage_open(StageWarp<TV, W> &sm, const int32
     if (b < nr && b - a >= SR) b = a + (b - a) / SR * SR;   // whole steps
     w.b = b;
     w.buf = nbuf;
-    nbuf ^= 1;
+    nbuf = nbuf + 1 == NB ? 0 : nbuf + 1;   // buffers in turn: the oldest is free
     const uint32_t nu = (uint32_t)(sm.row[b].x - w.ub);
     if (lane == 0) {
         // earlier generic reads of this buffer before the async-proxy writes
@@ -1288,11 +1288,11 @@ __device__ __forceinline__ void unit_vals(const DUnit &u, double a[4]) {
 // the row: every slot is applied as a (p_j - p_i) (the diagonal then adds
 // nothing) and the lane holding the row's first unit adds s_i p_i. Padding
 // slots (column i, value 0) add nothing either way.
-template <typename T, bool DIFF, int W, int LPR>
+template <typename T, bool DIFF, int W, int NB, int H, int LPR>
 __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
-                               int lane, double part[4], StageWarp<T, W> &sm,
+                               int lane, double part[4], StageWarp<T, W, NB> &sm,
                                const int *err, int *fail) {
-    constexpr int NG = 32 / LPR, H = sizeof(T) == 8 ? 1 : 2, SR = NG * H;
+    constexpr int NG = 32 / LPR, SR = NG * H;
     using VU = typename ValUnit<T>::type;
     const int pbuf = vcgi(&st->pbuf);
     const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
@@ -1309,30 +1309,42 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
         sm.row[t] = make_int2((int)(unit_start(kb, r0 + t) - e0), (len + 3) >> 2);
     }
     if (lane == 0) {
-        mbar_init(&sm.mbar[0]);
-        mbar_init(&sm.mbar[1]);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) mbar_init(&sm.mbar[b]);
         mbar_init_fence();
     }
     __syncwarp();
     int nbuf = 0;
     uint32_t par = 0;   // bit b: parity of buffer b's next phase
-    StageWin w = stage_open<T, W, SR>(sm, ci4, va4, e0, 0, nr, lane, nbuf);
-    while (w.a < nr) {
-        StageWin nx;
-        nx.a = nx.b = nr;
-        nx.buf = -1;
-        nx.ub = 0;
-        if (w.b < nr) nx = stage_open<T, W, SR>(sm, ci4, va4, e0, w.b, nr, lane, nbuf);
+    // windows in order: wq[0] is multiplied while the copies of wq[1..NB-1]
+    // are in flight
+    StageWin wq[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int a = k == 0 ? 0 : wq[k - 1].b;
+        if (a < nr) {
+            wq[k] = stage_open<T, W, NB, SR>(sm, ci4, va4, e0, a, nr, lane, nbuf);
+        } else {
+            wq[k].a = wq[k].b = nr;
+            wq[k].buf = -1;
+            wq[k].ub = 0;
+        }
+    }
+    while (wq[0].a < nr) {
+        const StageWin w = wq[0];
         if (w.buf >= 0) {
             const bool ok = mbar_wait(&sm.mbar[w.buf], (par >> w.buf) & 1u, err);
             par ^= 1u << w.buf;
             if (!__all_sync(0xffffffffu, ok)) {
-                if (nx.buf >= 0) {   // its own copy still in flight: bounded wait
-                    const unsigned long long t0 = globaltimer();
-                    while (!mbar_test(&sm.mbar[nx.buf], (par >> nx.buf) & 1u) &&
-                           globaltimer() - t0 < 2000000000ull) {
+                // the other copies still in flight: bounded waits
+#pragma unroll
+                for (int k = 1; k < NB; ++k)
+                    if (wq[k].buf >= 0) {
+                        const unsigned long long t0 = globaltimer();
+                        while (!mbar_test(&sm.mbar[wq[k].buf], (par >> wq[k].buf) & 1u) &&
+                               globaltimer() - t0 < 2000000000ull) {
+                        }
                     }
-                }
                 *fail = 1;
                 break;
             }
@@ -1430,7 +1442,15 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
                 pq += pi * acc;
             }
         }
-        w = nx;
+#pragma unroll
+        for (int k = 0; k + 1 < NB; ++k) wq[k] = wq[k + 1];
+        if (wq[NB - 2].b < nr) {
+            wq[NB - 1] = stage_open<T, W, NB, SR>(sm, ci4, va4, e0, wq[NB - 2].b, nr, lane, nbuf);
+        } else {
+            wq[NB - 1].a = wq[NB - 1].b = nr;
+            wq[NB - 1].buf = -1;
+            wq[NB - 1].ub = 0;
+        }
     }
     part[0] += (double)pq;
 }
@@ -1598,17 +1618,24 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
 // k_gx for scalar systems with the bulk-staged A phase (windows of W
 // units, LPR lanes per row); R and ZERO phases as in k_gx. Dynamic shared
 // memory: GROUP StageWarp<T, W> areas, about 70 KB, three blocks per SM.
+// W units per window, NB windows per warp, H rows per lane group and step,
+// BLOCKS resident blocks per SM.
 template <typename T> struct StageUnits;
-template <> struct StageUnits<float> { static constexpr int W = 128; };   // 2 x 4 KB per warp
-template <> struct StageUnits<double> { static constexpr int W = 84; };   // 2 x 3.9 KB per warp
+template <> struct StageUnits<float> {     // 2 x 4 KB windows per warp
+    static constexpr int W = 128, NB = 2, H = 2, BLOCKS = 3;
+};
+template <> struct StageUnits<double> {    // 2 x 3.9 KB windows per warp
+    static constexpr int W = 84, NB = 2, H = 1, BLOCKS = 3;
+};
 template <typename T>
-constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarp<T, StageUnits<T>::W>); }
+using StageWarpOf = StageWarp<T, StageUnits<T>::W, StageUnits<T>::NB>;
+template <typename T>
+constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarpOf<T>); }
 
 template <typename T, int LPR>
-__global__ void __launch_bounds__(32 * GROUP, 3)
+__global__ void __launch_bounds__(32 * GROUP, StageUnits<T>::BLOCKS)
 k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
       const int2 *__restrict__ list, int n) {
-    constexpr int W = StageUnits<T>::W;
     extern __shared__ __align__(16) unsigned char gxs_area[];
     pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1626,10 +1653,11 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
-            StageWarp<T, W> &sm = reinterpret_cast<StageWarp<T, W> *>(gxs_area)[w];
+            using SU = StageUnits<T>;
+            StageWarpOf<T> &sm = reinterpret_cast<StageWarpOf<T> *>(gxs_area)[w];
             int fail = 0;
-            phase_A_staged<T, sizeof(T) == 4, W, LPR>(S, &st[e.x], r0, r1, lane, part, sm,
-                                                      &bar->err, &fail);
+            phase_A_staged<T, sizeof(T) == 4, SU::W, SU::NB, SU::H, LPR>(
+                S, &st[e.x], r0, r1, lane, part, sm, &bar->err, &fail);
             if (fail && lane == 0) atomicExch(&bar->err, 2);
         } else if (ph == PH_R) {
             int bad = 0;
@@ -1837,8 +1865,9 @@ static int gxs_prepare() {
     const size_t bytes = gxs_smem<T>();
     CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, LPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)bytes));
-    // shared-memory share of the unified L1 for three resident blocks
-    int pct = (int)((3 * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+    // shared-memory share of the unified L1 for the resident blocks
+    constexpr int nb = StageUnits<T>::BLOCKS;
+    int pct = (int)((nb * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
     if (pct > 100) pct = 100;
     CFEM_CUDA(cudaFuncSetAttribute(k_gxs<T, LPR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    pct));
