@@ -510,11 +510,11 @@ def run_batched_heat(args, rank, world, local_rank):
     if spmv_ms > 0:
         ach = spmv_b / (spmv_ms * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": "k_gx (batched PCG SpMV phase over all systems: q = A p, p update, p.q)",
+            "kernel": "k_gxs (batched PCG SpMV phase over all systems, matrix bulk-staged through shared memory: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": spmv_ms,
-            "traffic": _profiled_traffic("k_gx_batched_tet10_heat",
+            "traffic": _profiled_traffic("k_gxs_batched_tet10_heat",
                                          "fp32" if args.precision == "mixed" else "fp64"),
         }
     if world == 1 and not args.no_cpu_baseline:
@@ -681,7 +681,7 @@ def run_transient_heat(args, rank, world, local_rank):
     if spmv:
         ach = spmv_b / (float(np.mean(spmv)) * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": "k_gx (scalar PCG SpMV phase: q = A p, p.q)",
+            "kernel": "k_gxs (scalar PCG SpMV phase, matrix bulk-staged through shared memory: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": float(np.mean(spmv)), "traffic": None,
