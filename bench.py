@@ -899,6 +899,13 @@ def run_serving(args, rank, world, local_rank):
             runs.append(srv.serve(fresh()))
     launches = rt.launches() - l0
     mixed_sol = {r.id: r.result for r in stream}
+    # give the resident server's device meshes (up to the HBM budget) back
+    # before the comparison paths build their own
+    del srv
+    import gc
+    gc.collect()
+    torch.cuda.empty_cache()
+    rt.trim()
 
     # plain FP64 GPU path: one request at a time, unbatched, FP64, to the
     # same tolerance, on the first requests of the stream; accuracy of the
