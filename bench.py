@@ -901,6 +901,7 @@ def run_serving(args, rank, world, local_rank):
     mixed_sol = {r.id: r.result for r in stream}
     # give the resident server's device meshes (up to the HBM budget) back
     # before the comparison paths build their own
+    workers = srv.workers
     del srv
     import gc
     gc.collect()
@@ -941,7 +942,7 @@ def run_serving(args, rank, world, local_rank):
         "config": {
             "workload": f"serving_stream_{len(stream)}_requests_lambda200",
             "mix": "60% P1 heat / 25% Tet10 heat / 15% Tet10 elasticity",
-            "dof_range": [1e3, 2e6], "hbm_budget_gb": 150, "workers": srv.workers,
+            "dof_range": [1e3, 2e6], "hbm_budget_gb": 150, "workers": workers,
             "rtol": args.serve_rtol,
             "requests": len(stream), "solved_dofs": med["solved_dofs"],
             "p50_ms": med["p50_ms"], "p99_ms": med["p99_ms"], "max_ms": med["max_ms"],
