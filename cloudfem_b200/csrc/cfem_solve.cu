@@ -82,6 +82,11 @@ struct SysDev {
     const int32_t *ci4;
     const void *va4;
     const double *va4d;   // FP64 values in the same layout (== va4 in FP64 mode)
+    // bs 3, graph scheduler with the staged SpMV: block rows padded to whole
+    // units of 4 blocks, row i starting at unit (rp[i] + 3 i + 3) / 4
+    // (padding: column i, zero block); working-precision values, 9 per slot
+    const int32_t *c3;
+    const void *v3;
     // graph scheduler: rows per SpMV-phase work entry, and entry count
     int32_t xrows, nxe;
 };
@@ -1455,6 +1460,203 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
     part[0] += (double)pq;
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-staged 3x3-block SpMV (graph scheduler, A phase of 3x3 systems).
+// Working copy: block rows padded to whole units of 4 blocks, row i starting
+// at unit (rp[i] + 3 i + 3) / 4 (padding: column i, zero block), columns in
+// one array and row-major block values (9 per slot) in another, so a work
+// entry's rows are one contiguous span of units. Block rows of an elasticity
+// pattern run from 10 to 65 blocks (76 B each in FP64), so windows cannot
+// hold whole rows within the shared memory three blocks per SM leave;
+// instead the span is cut into fixed windows of W units, streamed through
+// two buffers with 1-D bulk copies (the next window in flight while the
+// current one is used), and a row may straddle windows: the warp takes one
+// block row at a time, lane l the row's blocks l, l+32, ... (two in flight
+// in FP32, one in FP64 within 80 registers), and carries
+// its three sums in registers from one window to the next. The new
+// direction p = zeta z + beta p_old is formed at every gathered block (as
+// the register path does) and written for the row's own DOFs. Waits are
+// bounded as in the scalar staged SpMV.
+constexpr int XR3 = 8;    // block rows of one 3x3 work entry (one chunk)
+
+template <typename TV, int W>
+struct Stage3Warp {
+    int2 row[XR3 + 4];                // per row: first slot (from the entry's first), blocks
+    unsigned long long mbar[2];       // one transaction barrier per buffer
+    int4 c[2][W];                     // block columns, 4 per unit
+    TV v[2][W * 36];                  // block values, 36 per unit
+};
+
+// Padded 3x3 working copy (one warp per block row, consecutive writes).
+template <typename T>
+__global__ void k_pad3(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                       const T *__restrict__ v, int32_t *__restrict__ c3, T *__restrict__ v3) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const int64_t kb = rp[i], len = rp[i + 1] - kb;
+        const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
+        const int64_t m = ((len + 3) >> 2) * 4;
+        for (int64_t t = lane; t < m; t += 32) c3[o + t] = t < len ? ci[kb + t] : (int32_t)i;
+        for (int64_t t = lane; t < 9 * m; t += 32) v3[9 * o + t] = t < 9 * len ? v[9 * kb + t] : (T)0;
+    }
+}
+
+// Start the copy of window k (units [e0 + k W, min(e0 + (k+1) W, e1))) into
+// buffer k & 1; lane 0 only.
+template <typename TV, int W>
+__device__ __forceinline__ void stage3_issue(Stage3Warp<TV, W> &sm, const int32_t *c3,
+                                             const TV *v3, int64_t e0, int64_t e1, int k) {
+    const int b = k & 1;
+    const int64_t u0 = e0 + (int64_t)k * W;
+    const int64_t u1 = min(e1, u0 + W);
+    const uint32_t nu = (uint32_t)(u1 - u0);
+    const uint32_t bc = nu * 16u, bv = nu * 36u * (uint32_t)sizeof(TV);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(&sm.mbar[b], bc + bv);
+    if (nu) {
+        bulk_load(&sm.c[b][0], c3 + 4 * u0, bc, &sm.mbar[b]);
+        bulk_load(&sm.v[b][0], v3 + 36 * u0, bv, &sm.mbar[b]);
+    }
+}
+
+// q = A p, p = zeta z + beta p_old written for the rows, and p.q over block
+// rows [r0, r1) (at most XR3) of one 3x3 system. DIFF: the FP32
+// difference-form operator (off-diagonal blocks applied to p_j - p_i).
+template <typename T, bool DIFF, int W>
+__device__ void phase_A3_staged(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
+                                int lane, double part[4], Stage3Warp<T, W> &sm,
+                                const int *err, int *fail) {
+    constexpr int HB = sizeof(T) == 8 ? 1 : 2;   // blocks per lane in flight
+    const T beta = (T)vcg(&st->beta);
+    const T zeta = (T)vcg(&st->zeta);
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
+    T *pout = (T *)(pbuf ? S.p0 : S.p1);
+    const T *z = (const T *)S.z;
+    T *q = (T *)S.q;
+    const int32_t *c3 = S.c3;
+    const T *v3 = (const T *)S.v3;
+    const int nr = (int)(r1 - r0);
+    const int64_t e0 = unit_start(__ldg(S.rp + r0), r0);   // the entry's first unit
+    const int64_t e1 = unit_start(__ldg(S.rp + r1), r1);   // the next entry's first
+    const int nwin = (int)((e1 - e0 + W - 1) / W);
+    for (int t = lane; t < nr; t += 32) {
+        const int64_t kb = __ldg(S.rp + r0 + t);
+        const int len = __ldg(S.rp + r0 + t + 1) - (int)kb;
+        sm.row[t] = make_int2((int)(4 * (unit_start(kb, r0 + t) - e0)), len);
+    }
+    if (lane == 0) {
+        mbar_init(&sm.mbar[0]);
+        mbar_init(&sm.mbar[1]);
+        mbar_init_fence();
+        if (nwin > 0) stage3_issue(sm, c3, v3, e0, e1, 0);
+        if (nwin > 1) stage3_issue(sm, c3, v3, e0, e1, 1);
+    }
+    __syncwarp();
+    // window k sits in buffer k & 1 and is that buffer's (k >> 1)-th use:
+    // its barrier phase has parity (k >> 1) & 1
+    int cur = 0;        // window in use
+    bool ok = true;
+    if (nwin > 0) ok = mbar_wait(&sm.mbar[0], 0u, err);
+    ok = __all_sync(0xffffffffu, ok);
+    T pq = 0;
+    for (int t = 0; t < nr && ok; ++t) {
+        const int64_t i = r0 + t;
+        const int2 ri = sm.row[t];
+        T pi[3], acc[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pi[c] = zeta * __ldg(z + 3 * i + c) + beta * __ldg(pin + 3 * i + c);
+            acc[c] = 0;
+        }
+        int done = 0;   // blocks of the row already multiplied
+        while (true) {
+            const int wlo = 4 * W * cur;
+            const int tend = min(ri.y, wlo + 4 * W - ri.x);   // row blocks in this window
+            const int32_t *cs = (const int32_t *)sm.c[cur & 1];
+            const T *vs = sm.v[cur & 1];
+            for (int b0 = lane; b0 < tend; b0 += 32 * HB) {
+                // HB blocks per lane in flight: b0, b0 + 32, ...
+                int col[HB], sl[HB];
+                bool on[HB];
+#pragma unroll
+                for (int h = 0; h < HB; ++h) {
+                    const int b = b0 + 32 * h;
+                    on[h] = b >= done && b < tend;
+                    sl[h] = ri.x + b - wlo;
+                    col[h] = on[h] ? cs[sl[h]] : (int)i;
+                }
+                T pj[HB][3];
+#pragma unroll
+                for (int h = 0; h < HB; ++h)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        pj[h][d] = on[h] ? zeta * __ldg(z + 3 * (int64_t)col[h] + d) +
+                                               beta * __ldg(pin + 3 * (int64_t)col[h] + d)
+                                         : (T)0;
+#pragma unroll
+                for (int h = 0; h < HB; ++h) {
+                    if (!on[h]) continue;
+                    if (DIFF) {
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                            pj[h][d] = (col[h] == (int)i) ? pi[d] : pj[h][d] - pi[d];
+                    }
+                    const T *a = vs + 9 * sl[h];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) acc[c] += a[3 * c + d] * pj[h][d];
+                }
+            }
+            done = max(done, tend);
+            if (done >= ri.y) break;
+            // the row goes on in the next window
+            __syncwarp();   // reads of this buffer done before it is refilled
+            if (lane == 0 && cur + 2 < nwin) stage3_issue(sm, c3, v3, e0, e1, cur + 2);
+            ++cur;
+            bool okw = false;
+            if (cur < nwin) okw = mbar_wait(&sm.mbar[cur & 1], (uint32_t)(cur >> 1) & 1u, err);
+            if (!__all_sync(0xffffffffu, okw)) {
+                ok = false;
+                break;
+            }
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] = group_sum<32>(acc[c]);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                pout[3 * i + c] = pi[c];
+                q[3 * i + c] = acc[c];
+                pq += pi[c] * acc[c];
+            }
+        }
+    }
+    if (ok) {
+        // window cur + 1 was issued and may hold only gap units: it must
+        // have landed before the warp's shared memory is released
+        if (cur + 1 < nwin) {
+            const bool okw =
+                mbar_wait(&sm.mbar[(cur + 1) & 1], (uint32_t)((cur + 1) >> 1) & 1u, err);
+            if (!__all_sync(0xffffffffu, okw)) *fail = 1;
+        }
+    } else {
+        // windows cur (whose wait gave up) and cur + 1 may still be in
+        // flight: bounded waits, then report
+        for (int k = cur; k < nwin && k <= cur + 1; ++k) {
+            const unsigned long long t0 = globaltimer();
+            while (!mbar_test(&sm.mbar[k & 1], (uint32_t)(k >> 1) & 1u) &&
+                   globaltimer() - t0 < 2000000000ull) {
+            }
+        }
+        *fail = 1;
+    }
+    part[0] += (double)pq;
+}
+
 // Entry-major working-precision copy of block values (AoS -> SoA).
 template <typename TI, typename TO, int B2>
 __global__ void k_to_soa(int64_t nnzb, const TI *__restrict__ in, TO *__restrict__ out) {
@@ -1669,6 +1871,53 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
+// k_gx for 3x3 systems with the bulk-staged A phase; R and ZERO phases as
+// in k_gx. Dynamic shared memory: GROUP Stage3Warp<T, W3> areas, about
+// 68 KB, three blocks per SM.
+template <typename T> struct Stage3Units;
+template <> struct Stage3Units<float> { static constexpr int W = 26; };    // 2 x 3.9 KB per warp
+template <> struct Stage3Units<double> { static constexpr int W = 14; };   // 2 x 4.1 KB per warp
+template <typename T>
+using Stage3WarpOf = Stage3Warp<T, Stage3Units<T>::W>;
+template <typename T>
+constexpr size_t gxs3_smem() { return (size_t)GROUP * sizeof(Stage3WarpOf<T>); }
+
+template <typename T>
+__global__ void __launch_bounds__(32 * GROUP, 3)
+k_gxs3(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
+       const int2 *__restrict__ list, int n) {
+    extern __shared__ __align__(16) unsigned char gxs_area[];
+    pdl_wait();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
+    if (*(volatile const int *)&bar->err) return;           // a wait gave up
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * S.xrows;
+        const int64_t r1 = min(S.n, r0 + S.xrows);
+        if (ph == PH_A) {
+            Stage3WarpOf<T> &sm = reinterpret_cast<Stage3WarpOf<T> *>(gxs_area)[w];
+            int fail = 0;
+            phase_A3_staged<T, sizeof(T) == 4, Stage3Units<T>::W>(S, &st[e.x], r0, r1, lane,
+                                                                   part, sm, &bar->err, &fail);
+            if (fail && lane == 0) atomicExch(&bar->err, 2);
+        } else if (ph == PH_R) {
+            int bad = 0;
+            phase_R<T, 3, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+        } else {
+            phase_zero<3>(S, r0, r1, lane);
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
 template <typename T, int BS>
 __global__ void __launch_bounds__(32 * GROUP)
 k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
@@ -1860,6 +2109,18 @@ static void glaunch_smem(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsi
     (void)cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+template <typename T>
+static int gxs3_prepare() {
+    const size_t bytes = gxs3_smem<T>();
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)bytes));
+    int pct = (int)((3 * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+    if (pct > 100) pct = 100;
+    CFEM_CUDA(cudaFuncSetAttribute(k_gxs3<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   pct));
+    return CFEM_OK;
+}
+
 template <typename T, int LPR>
 static int gxs_prepare() {
     const size_t bytes = gxs_smem<T>();
@@ -1923,7 +2184,15 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
     for (int i = 0; i < P->n_systems; ++i) {
         SysDev &S = P->hs[i];
-        if (S.bs == 3) {
+        if (S.bs == 3 && S.c3) {
+            const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
+            if (S.mode == CFEM_SOLVE_MIXED)
+                CFEM_LAUNCH(k_pad3<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
+                            (int32_t *)S.c3, (float *)S.v3);
+            else
+                CFEM_LAUNCH(k_pad3<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
+                            (int32_t *)S.c3, (double *)S.v3);
+        } else if (S.bs == 3 && S.vsoa) {
             if (S.mode == CFEM_SOLVE_MIXED)
                 CFEM_LAUNCH((k_to_soa<float, float, 9>), grid_for(S.nnzb, 256), 256, 0,
                             s, S.nnzb, S.v32, (float *)S.vsoa);
@@ -2043,7 +2312,6 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                        align256(S.ntiles * 4 * sizeof(double)) +
                        align256(S.ntiles * sizeof(unsigned)) +
                        align256(S.nchunksB * 4 * sizeof(double));
-        if (L.bs == 3) copy_bytes += align256((size_t)S.nnzb * 9 * ts);
         n_chunks_b += S.nchunksB;
         if (L.max_iter > max_iter) max_iter = L.max_iter;
     }
@@ -2065,14 +2333,23 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     P->persistent = persistent;
     P->grid = grid;
-    // Scalar systems on the graph scheduler read a unit-padded copy.
+    // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
+    // systems a padded block copy (staged SpMV) or an entry-major copy.
+    const bool stage3 = ctx->spmv_stage == 1;
     if (!persistent)
-        for (int i = 0; i < n_systems; ++i)
+        for (int i = 0; i < n_systems; ++i) {
+            const size_t ts = (hs[i].mode == CFEM_SOLVE_MIXED) ? 4 : 8;
             if (hs[i].bs == 1) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 8) +
                               (hs[i].mode == CFEM_SOLVE_MIXED ? align256(ne * 4) : 0);
+            } else if (stage3) {
+                const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
+                copy_bytes += align256(ne * 4) + align256(ne * 9 * ts);
+            } else {
+                copy_bytes += align256((size_t)hs[i].nnzb * 9 * ts);
             }
+        }
     const size_t list_a = n_chunks + (size_t)GROUP * n_systems;
     const size_t list_b = n_chunks_b + (size_t)GROUP * n_systems;
     copy_bytes += align256(n_systems * sizeof(SysDev)) + align256(n_chunks * sizeof(int32_t)) +
@@ -2100,7 +2377,13 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         S.tcnt = (unsigned *)take_s(S.ntiles * sizeof(unsigned));
         S.partialB = (double *)take_s(S.nchunksB * 4 * sizeof(double));
         if (S.bs == 3) {
-            S.vsoa = take_c((size_t)S.nnzb * 9 * ts);
+            if (!persistent && stage3) {
+                const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
+                S.c3 = (const int32_t *)take_c(ne * 4);
+                S.v3 = take_c(ne * 9 * ts);
+            } else if (!persistent) {
+                S.vsoa = take_c((size_t)S.nnzb * 9 * ts);
+            }
         } else {
             S.vsoa = (S.mode == CFEM_SOLVE_MIXED) ? (const void *)S.v32 : (const void *)S.v64;
             if (!persistent) {
@@ -2116,6 +2399,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         // (measured 1.8x faster than one chunk on the batched heat meshes; 3x3
         // systems keep one chunk: fewer, longer warps measured slower there).
         S.xrows = (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;
+        CFEM_CHECK(!S.c3 || S.xrows <= XR3, CFEM_ERR_UNSUPPORTED,
+                   "staged 3x3 work entries hold at most %d block rows", XR3);
         S.nxe = (int32_t)((S.n + S.xrows - 1) / S.xrows);
     }
     P->d_st = (SysState *)take_s(n_systems * sizeof(SysState));
@@ -2185,6 +2470,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         CFEM_TRY((lpr[0] == 4 ? gxs_prepare<double, 4>() : gxs_prepare<double, 8>()));
     if (stage == 1 && !la[2].empty())
         CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
+    if (stage == 1 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
+    if (stage == 1 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
         const bool pdl = use_pdl && !t0;
@@ -2210,9 +2497,13 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (t == 2 && stage == 1)
                 glaunch_smem(p, lpr[2] == 4 ? k_gxs<float, 4> : k_gxs<float, 8>, g, 32 * GROUP, gxs_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 1) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 1)
+                glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 0) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 3) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 1)
+                glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 0) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
         if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));
