@@ -1036,9 +1036,10 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
                     help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
-    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1],
-                    help="scalar SpMV: 1 bulk-staged shared-memory windows (library "
-                         "default), 0 register path")
+    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2],
+                    help="SpMV: 1 scalar rows bulk-staged through shared memory, 3x3 "
+                         "blocks in registers (library default); 2 both staged; 0 "
+                         "both in registers")
     args = ap.parse_args()
     global SPMV_STAGE
     SPMV_STAGE = args.spmv_stage

@@ -75,7 +75,7 @@ struct cfem_ctx {
     int p1_threads = 128;              // P1 element kernels, threads per block
     int graph_iters = 2;               // iterations per solve-loop body
     int pdl = 1;                       // dependent launches in solve graphs
-    int spmv_stage = 1;                // scalar SpMV: 0 registers, 1 bulk-staged windows
+    int spmv_stage = 1;                // SpMV: 0 registers, 1 staged scalar rows, 2 also 3x3
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // SpMV timing

@@ -2335,7 +2335,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     P->grid = grid;
     // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
     // systems a padded block copy (staged SpMV) or an entry-major copy.
-    const bool stage3 = ctx->spmv_stage == 1;
+    const bool stage3 = ctx->spmv_stage == 2;
     if (!persistent)
         for (int i = 0; i < n_systems; ++i) {
             const size_t ts = (hs[i].mode == CFEM_SOLVE_MIXED) ? 4 : 8;
@@ -2452,7 +2452,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // reduction. The SpMV of the first iteration is bracketed by the
     // timing events when tev is given.
     const bool use_pdl = ctx->pdl != 0;
-    // scalar SpMV: bulk-staged windows (1) or the register path (0); lanes
+    // scalar SpMV: bulk-staged windows (1, 2) or the register path (0); 3x3
+    // SpMV: bulk-staged (2) or the register path (0, 1); lanes
     // per row from the mean row length of the list's systems (4 up to 16
     // entries, whole units of a P1 row; 8 above, Tet10 rows of ~27)
     const int stage = ctx->spmv_stage;
@@ -2466,12 +2467,12 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             }
         if (rows > 0 && nz <= 16.0 * rows) lpr[t] = 4;
     }
-    if (stage == 1 && !la[0].empty())
+    if (stage >= 1 && !la[0].empty())
         CFEM_TRY((lpr[0] == 4 ? gxs_prepare<double, 4>() : gxs_prepare<double, 8>()));
-    if (stage == 1 && !la[2].empty())
+    if (stage >= 1 && !la[2].empty())
         CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
-    if (stage == 1 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
-    if (stage == 1 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
+    if (stage == 2 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
+    if (stage == 2 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
         const bool pdl = use_pdl && !t0;
@@ -2492,18 +2493,18 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
-            if (t == 0 && stage == 1)
+            if (t == 0 && stage >= 1)
                 glaunch_smem(p, lpr[0] == 4 ? k_gxs<double, 4> : k_gxs<double, 8>, g, 32 * GROUP, gxs_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 2 && stage == 1)
+            if (t == 2 && stage >= 1)
                 glaunch_smem(p, lpr[2] == 4 ? k_gxs<float, 4> : k_gxs<float, 8>, g, 32 * GROUP, gxs_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage == 1)
+            if (t == 1 && stage == 2)
                 glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage == 0) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage < 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage == 1)
+            if (t == 3 && stage == 2)
                 glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage == 0) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage < 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
         if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));

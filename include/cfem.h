@@ -173,10 +173,12 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * convergence). PDL: 1 (default) captures the solve graphs' kernels as
  * programmatic dependent launches (launch processing overlaps the previous
  * kernel's drain), 0 as plain launches. SPMV_STAGE: how the graph
- * scheduler's scalar SpMV reads its unit-padded copy of the matrix: 1
- * (default) streams each work entry's span through two shared-memory
- * windows of about 4 KB per warp with 1-D bulk copies (TMA), 0 loads it into
- * registers with vector loads. get returns -1 for an unknown parameter. */
+ * scheduler's SpMV reads its padded working copy of the matrix: 1 (default)
+ * streams each scalar work entry's span through two shared-memory windows
+ * of about 4 KB per warp with 1-D bulk copies (TMA) and loads 3x3 blocks
+ * into registers, 2 streams 3x3 blocks through shared memory too (slower on
+ * the elasticity beam: kept for tuning), 0 loads both into registers. get
+ * returns -1 for an unknown parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);

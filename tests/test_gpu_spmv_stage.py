@@ -1,8 +1,9 @@
-"""Scalar SpMV of the graph scheduler with the matrix streamed through
-shared-memory windows by 1-D bulk copies (staging 1) against the register
-path (staging 0) and a direct FP64 solve: the same answers, bitwise batch
-independence, rows longer than a window, short (P1-like, 4 lanes per row)
-and long (8 lanes) rows, and CSR arrays that do not start on a 16-byte
+"""SpMV of the graph scheduler with the matrix streamed through
+shared-memory windows by 1-D bulk copies (staging 1: scalar rows; 2: also
+3x3 blocks) against the register path (staging 0) and a direct FP64 solve:
+the same answers, bitwise batch independence, rows longer than a window,
+short (P1-like, 4 lanes per row) and long (8 lanes) rows, 3x3 rows that
+straddle windows, and CSR arrays that do not start on a 16-byte
 boundary."""
 
 import numpy as np
@@ -172,17 +173,17 @@ def _elastic_system(torch, nx, ny, nz, seed):
 
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
 def test_staged_3x3_spmv_matches_register_path(torch, mode):
-    """3x3-block systems on the graph scheduler: the staged SpMV (rows that
-    straddle windows, 65-block vertex rows) and the register path reach the
-    same answer, and the staged one repeats bitwise."""
+    """3x3-block systems on the graph scheduler: the staged SpMV (staging
+    2: rows that straddle windows, 65-block vertex rows) and the register
+    path reach the same answer, and the staged one repeats bitwise."""
     from cloudfem_b200 import _native as N
     dm, sysm = _elastic_system(torch, 10, 3, 3, seed=1)
     rt = dm.rt
     md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
     rtol = 1e-11 if mode == "fp64" else 1e-10
     _, (x0,) = _solve(rt, [sysm], md, rtol, 0)
-    r1, (x1,) = _solve(rt, [sysm], md, rtol, 1)
-    _, (x1b,) = _solve(rt, [sysm], md, rtol, 1)
+    r1, (x1,) = _solve(rt, [sysm], md, rtol, 2)
+    _, (x1b,) = _solve(rt, [sysm], md, rtol, 2)
     d = np.linalg.norm(x1 - x0) / np.linalg.norm(x0)
     assert d <= (1e-8 if mode == "fp64" else 1e-7), d
     assert np.array_equal(x1, x1b)
@@ -196,8 +197,8 @@ def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch):
     rt = built[0][0].rt
     systems = [s for _, s in built]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, 1)
+        rb, xb = _solve(rt, systems, md, 1e-10, 2)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, 1)
+            r, (x,) = _solve(rt, [s], md, 1e-10, 2)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
