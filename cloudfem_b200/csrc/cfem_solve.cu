@@ -1341,12 +1341,15 @@ __device__ void phase_A_staged(const SysDev &S, const SysState *st, int64_t r0, 
             const bool ok = mbar_wait(&sm.mbar[w.buf], (par >> w.buf) & 1u, err);
             par ^= 1u << w.buf;
             if (!__all_sync(0xffffffffu, ok)) {
-                // the other copies still in flight: bounded waits
+                // this window's copy and the later ones may still be in
+                // flight: bounded waits (this window's parity bit has
+                // already been advanced)
 #pragma unroll
-                for (int k = 1; k < NB; ++k)
+                for (int k = 0; k < NB; ++k)
                     if (wq[k].buf >= 0) {
+                        const uint32_t ph = ((par >> wq[k].buf) & 1u) ^ (k == 0 ? 1u : 0u);
                         const unsigned long long t0 = globaltimer();
-                        while (!mbar_test(&sm.mbar[wq[k].buf], (par >> wq[k].buf) & 1u) &&
+                        while (!mbar_test(&sm.mbar[wq[k].buf], ph) &&
                                globaltimer() - t0 < 2000000000ull) {
                         }
                     }
