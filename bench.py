@@ -957,7 +957,9 @@ def run_serving(args, rank, world, local_rank):
         },
         "e2e": {"value": world * e2e["dof_per_s"], "unit": "DOF/s",
                 "p50_ms": e2e["p50_ms"], "p99_ms": e2e["p99_ms"],
-                "h2d_bytes_per_step": int(sum(r.mesh.nodes.nbytes + np.asarray(r.mesh.elements).nbytes
+                # nodes in FP64 and connectivity as the int32 the device
+                # copy holds (the host converts before the copy)
+                "h2d_bytes_per_step": int(sum(r.mesh.nodes.nbytes + 4 * np.asarray(r.mesh.elements).size
                                               for r in stream)),
                 "d2h_bytes_per_step": int(sum(r.dofs * 8 for r in stream)),
                 "note": "new server: every mesh crosses with its request"},
