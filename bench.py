@@ -41,7 +41,7 @@ BC = {"xmin": (0.0, 0.0, 0.0)}
 TRACTION = {"xmax": (0.0, 0.0, -1e6)}
 BEAM = dict(xlim=(0.0, 2.0), ylim=(0.0, 0.25), zlim=(0.0, 0.25))
 FULL = (80, 10, 10)
-CPU_SAMPLE = (40, 5, 5)
+CPU_SAMPLE = (48, 6, 6)   # about 12 s of one SuperLU solve on 16 host cores
 RTOL = 1e-10
 L2_FLUSH_BYTES = 256 << 20
 
@@ -546,7 +546,7 @@ def run_batched_heat(args, rank, world, local_rank):
     return out
 
 
-def cpu_baseline_batched_heat(ns, ks, cap_n=7, count=12):
+def cpu_baseline_batched_heat(ns, ks, cap_n=7, count=24):
     """Oracle (NumPy + SuperLU) on the first `count` draws with n <= cap_n."""
     from oracle import cfem_oracle as O
     bc = {s: 0.0 for s in O.FACE_NAMES}
