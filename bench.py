@@ -751,6 +751,20 @@ def _av_kw():
                 J_s=av_js, boundary=["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"])
 
 
+def cpu_baseline_av(nb=8):
+    """Oracle (NumPy + SuperLU) phasor A-V solve on a box of nb^3 cells."""
+    from oracle import cfem_oracle as O
+    mo = O.box_mesh_tet10(nb, nb, nb)
+    t0 = time.perf_counter()
+    O.solve_eddy_current_tet10(mo, **_av_kw())
+    dt = time.perf_counter() - t0
+    fb = len(np.unique(np.concatenate([mo.boundaries[f] for f in _av_kw()["boundary"]])))
+    ub = 3 * (mo.n_nodes - fb)
+    return {"value": ub / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"box {nb}^3 (~{ub} A unknowns), SuperLU"}
+
+
 def run_av(args, rank, world, local_rank):
     import torch
 
@@ -803,18 +817,33 @@ def run_av(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        from oracle import cfem_oracle as O
-        nb = 8
-        mo = O.box_mesh_tet10(nb, nb, nb)
-        t0 = time.perf_counter()
-        O.solve_eddy_current_tet10(mo, **_av_kw())
-        dt = time.perf_counter() - t0
-        fb = len(np.unique(np.concatenate([mo.boundaries[f] for f in _av_kw()["boundary"]])))
-        ub = 3 * (mo.n_nodes - fb)
-        out["cpu_baseline"] = {"value": ub / dt, "unit": "DOF/s", "cores": os.cpu_count(),
-                               "kind": "port", "seconds": dt,
-                               "sample": f"box {nb}^3 (~{ub} A unknowns), SuperLU"}
+        out["cpu_baseline"] = cpu_baseline_av()
     return out
+
+
+AVT_STEPS = 50
+
+
+def _avt_kw(steps=AVT_STEPS):
+    return dict(nu=1.0 / (4e-7 * np.pi), sigma=AV_SIGMA, t_end=steps * 1e-4, dt=1e-4,
+                method="cn", J_s=lambda x, y, z: np.real(av_js(x, y, z)),
+                time_scale=lambda t: np.sin(2 * np.pi * 500.0 * t),
+                boundary=["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"])
+
+
+def cpu_baseline_avt(nb=8, steps=AVT_STEPS):
+    """Oracle transient A-V march (one LU, then the steps) on nb^3 cells."""
+    from oracle import cfem_oracle as O
+    kw = _avt_kw(steps)
+    mo = O.box_mesh_tet10(nb, nb, nb)
+    t0 = time.perf_counter()
+    O.transient_eddy_current_tet10(mo, **kw)
+    dt = time.perf_counter() - t0
+    fb = len(np.unique(np.concatenate([mo.boundaries[f] for f in kw["boundary"]])))
+    ub = 3 * (mo.n_nodes - fb)
+    return {"value": ub * steps / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"box {nb}^3, {steps} CN steps, one LU"}
 
 
 def run_avt(args, rank, world, local_rank):
@@ -831,12 +860,8 @@ def run_avt(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     rt = N.runtime(local_rank)
-    n, steps = args.av_n, 50
-
-    kw = dict(nu=1.0 / (4e-7 * np.pi), sigma=AV_SIGMA, t_end=steps * 1e-4, dt=1e-4,
-              method="cn", J_s=lambda x, y, z: np.real(av_js(x, y, z)),
-              time_scale=lambda t: np.sin(2 * np.pi * 500.0 * t),
-              boundary=["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"])
+    n, steps = args.av_n, AVT_STEPS
+    kw = _avt_kw(steps)
     mesh = box_mesh_tet10(n, n, n)
     for _ in range(args.warmup):
         em.transient_eddy_current_tet10(mesh, precision=args.precision, rtol=1e-10, **kw)
@@ -874,22 +899,62 @@ def run_avt(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        from oracle import cfem_oracle as O
-        nb = 8
-        mo = O.box_mesh_tet10(nb, nb, nb)
-        t0 = time.perf_counter()
-        O.transient_eddy_current_tet10(mo, **kw)
-        dt = time.perf_counter() - t0
-        fb = len(np.unique(np.concatenate([mo.boundaries[f] for f in kw["boundary"]])))
-        ub = 3 * (mo.n_nodes - fb)
-        out["cpu_baseline"] = {"value": ub * steps / dt, "unit": "DOF/s",
-                               "cores": os.cpu_count(), "kind": "port", "seconds": dt,
-                               "sample": f"box {nb}^3, {steps} CN steps, one LU"}
+        out["cpu_baseline"] = cpu_baseline_avt(steps=steps)
     return out
 
 
 # ---------------------------------------------------- serving a request stream
 SERVE_REQUESTS = 200
+
+
+def _cell_coef(mesh, k_elem):
+    """A per-element coefficient of a box mesh (6 tets per hex cell, cells
+    in k, j, i order, unit cell width 1 / ny as the request stream builds
+    them) as the callable(x, y, z) the reference's API takes: the value of
+    the hex cell holding the point (centroids and Keast points are interior,
+    so the lookup is exact)."""
+    corners = np.asarray(mesh.nodes)[np.unique(np.asarray(mesh.elements)[:, :4])]
+    nx, ny, nz = (len(np.unique(np.round(corners[:, d], 9))) - 1 for d in range(3))
+    lo = corners.min(axis=0)
+    hi = corners.max(axis=0)
+    kc = np.asarray(k_elem, dtype=float)[::6].reshape(nz, ny, nx)
+
+    def k(x, y, z):
+        i = np.clip(((np.asarray(x) - lo[0]) / (hi[0] - lo[0]) * nx).astype(int), 0, nx - 1)
+        j = np.clip(((np.asarray(y) - lo[1]) / (hi[1] - lo[1]) * ny).astype(int), 0, ny - 1)
+        kk = np.clip(((np.asarray(z) - lo[2]) / (hi[2] - lo[2]) * nz).astype(int), 0, nz - 1)
+        return kc[kk, j, i]
+    return k
+
+
+def cpu_baseline_serving(count=12, cap_dofs=6e3, seed=7):
+    """Oracle (NumPy + SuperLU, the reference's one-request-at-a-time path)
+    on the first `count` requests of the seeded stream drawn with at most
+    `cap_dofs` DOFs; DOF/s over their free DOFs. The cap keeps SuperLU
+    within memory: the reference's Dirichlet step stores the cleared
+    columns as explicit zeros (a dense free x fixed block), which at 25 k
+    P1 DOFs already exhausts its workspace here."""
+    from cloudfem_b200 import serve
+    from oracle import cfem_oracle as O
+    stream = serve.make_stream(SERVE_REQUESTS, rate=200.0, seed=seed, max_dofs=cap_dofs)
+    picked = stream[:count]
+    free, kinds, t0 = 0, {}, time.perf_counter()
+    for r in picked:
+        m = O.Mesh(r.mesh.nodes, r.mesh.elements, r.mesh.boundaries)
+        if r.kind == "t10_elast":
+            O.solve_elasticity_tet10(m, r.E, r.nu, bc={c: (0.0, 0.0, 0.0) for c in r.clamp},
+                                     traction=r.traction)
+        else:
+            solve = O.solve_p1_poisson if r.kind == "p1_heat" else O.solve_tet10_poisson
+            solve(m, k=_cell_coef(r.mesh, r.k), f=r.f, bc=r.bc)
+        free += serve.free_dofs(r)
+        kinds[r.kind] = kinds.get(r.kind, 0) + 1
+    dt = time.perf_counter() - t0
+    mix = ", ".join(f"{v} {k}" for k, v in sorted(kinds.items()))
+    return {"value": free / dt, "unit": "DOF/s", "cores": os.cpu_count(),
+            "kind": "port", "seconds": dt,
+            "sample": f"the first {len(picked)} requests of the seeded stream drawn with at most "
+                      f"{int(cap_dofs)} DOFs ({mix}; {free} free DOFs), one solve each"}
 
 
 def run_serving(args, rank, world, local_rank):
@@ -969,7 +1034,7 @@ def run_serving(args, rank, world, local_rank):
     med_dps, e2e_dps = -neg[0], -neg[1]
     if rank != 0:
         return None
-    return {
+    out = {
         "metric": METRIC, "value": world * med_dps, "unit": "DOF/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": float(np.mean([d["span_s"] for d in runs])) * 1e3,
@@ -1003,6 +1068,9 @@ def run_serving(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_serving()
+    return out
 
 
 def run_reference(args, rank):
@@ -1016,6 +1084,12 @@ def run_reference(args, rank):
             c = cpu_baseline_batched_heat(*draw)
         elif args.workload == "transient-heat":
             c = cpu_baseline_transient_heat()
+        elif args.workload == "serving":
+            c = cpu_baseline_serving()
+        elif args.workload == "av-phasor":
+            c = cpu_baseline_av()
+        elif args.workload == "av-transient":
+            c = cpu_baseline_avt()
         else:
             c = cpu_baseline()
         if i >= args.warmup:
@@ -1029,9 +1103,12 @@ def run_reference(args, rank):
         "warmup": args.warmup,
         "ms_per_step": float(np.mean([c["seconds"] for c in per])) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "c128" if args.workload == "av-phasor" else "f64", "data": "synthetic",
         "config": {"workload": {"batched-heat": "batched_tet10_heat_512_meshes_n4to24",
                                 "transient-heat": f"transient_p1_heat_cn_box_{TRANSIENT_N}cubed_{TRANSIENT_STEPS}_steps",
+                                "serving": f"serving_stream_{SERVE_REQUESTS}_requests_lambda200",
+                                "av-phasor": f"phasor_av_tet10_box_{AV_N}cubed",
+                                "av-transient": f"transient_av_tet10_box_{AV_N}cubed_{AVT_STEPS}_cn_steps",
                                 }.get(args.workload, "tet10_elasticity_beam_80x10x10"),
                    "sample": c["sample"]},
         "cpu_baseline": c,

@@ -308,11 +308,14 @@ def _cells_for(kind, dofs, aspect):
 
 def make_stream(n_requests, rate=200.0, mix=(0.60, 0.25, 0.15),
                 dof_range=(1e3, 2e6), aspect_range=(1.0, 4.0), sigma=0.5,
-                seed=0, mesh_cache=None):
+                seed=0, mesh_cache=None, max_dofs=None):
     """Seeded request stream: Poisson arrivals, kind mix, log-uniform DOF
     counts, random box aspect ratios, lognormal coefficients (per hex cell
     for heat, one E per elasticity request). Meshes with the same cells are
-    shared (a client resubmitting one geometry)."""
+    shared (a client resubmitting one geometry). max_dofs: keep only the
+    requests drawn with at most that many DOFs; every random draw is still
+    made, so the kept requests are exactly those of the full stream (and
+    no mesh is built for the others)."""
     from .mesh import box_mesh, box_mesh_tet10
     rng = np.random.default_rng(seed)
     cache = {} if mesh_cache is None else mesh_cache
@@ -324,15 +327,19 @@ def make_stream(n_requests, rate=200.0, mix=(0.60, 0.25, 0.15),
         dofs = float(np.exp(rng.uniform(np.log(dof_range[0]), np.log(dof_range[1]))))
         aspect = float(rng.uniform(*aspect_range))
         nx, ny, nz = _cells_for(kind, dofs, aspect)
+        if kind == "t10_elast":
+            coef = float(210e9 * rng.lognormal(0.0, sigma))
+        else:
+            coef = rng.lognormal(0.0, sigma, nx * ny * nz)
+        if max_dofs is not None and dofs > max_dofs:
+            continue
         key = (kind != "p1_heat", nx, ny, nz)
         if key not in cache:
             lim = dict(xlim=(0.0, nx / max(ny, 1)), ylim=(0.0, 1.0), zlim=(0.0, 1.0))
             cache[key] = (box_mesh_tet10 if key[0] else box_mesh)(nx, ny, nz, **lim)
         mesh = cache[key]
         if kind == "t10_elast":
-            E = float(210e9 * rng.lognormal(0.0, sigma))
-            out.append(Request(i, kind, mesh, t, E=E, nu=0.3))
+            out.append(Request(i, kind, mesh, t, E=coef, nu=0.3))
         else:
-            kc = rng.lognormal(0.0, sigma, nx * ny * nz)
-            out.append(Request(i, kind, mesh, t, k=np.repeat(kc, 6), f=1.0))
+            out.append(Request(i, kind, mesh, t, k=np.repeat(coef, 6), f=1.0))
     return out

@@ -53,3 +53,21 @@ def test_batch_dof_cap():
     srv = _server(1e12, max_batch_dofs=3 * reqs[0].dofs)
     batch, _ = srv._take_batch(list(reqs), 1e12)
     assert sum(r.dofs for r in batch) <= 3 * reqs[0].dofs
+
+
+def test_stream_cap_keeps_the_full_streams_requests():
+    """make_stream(max_dofs=...) keeps a subset of the full stream's
+    requests, unchanged (same ids, kinds, arrivals, coefficients, meshes)."""
+    import numpy as np
+    from cloudfem_b200 import serve
+    full = {r.id: r for r in serve.make_stream(40, seed=7, dof_range=(1e3, 3e4))}
+    kept = serve.make_stream(40, seed=7, dof_range=(1e3, 3e4), max_dofs=5e3)
+    assert 0 < len(kept) < len(full)
+    for r in kept:
+        f = full[r.id]
+        assert (r.kind, r.arrival, r.mesh.n_nodes) == (f.kind, f.arrival, f.mesh.n_nodes)
+        if r.kind == "t10_elast":
+            assert r.E == f.E
+        else:
+            assert np.array_equal(r.k, f.k)
+        assert r.dofs < 4 * 5e3
