@@ -13,7 +13,6 @@ max_iter : iteration cap (default grows with the system size).
 """
 
 import threading
-import warnings
 
 import numpy as np
 
@@ -44,15 +43,17 @@ def solver_mode(precision, rtol):
 
 
 def accept(res, rtol, what):
-    """Raise unless the solve converged (a stall within 10x of the target
-    at the FP64 round-off floor is accepted with a warning)."""
+    """Raise RuntimeError unless the solve converged.
+
+    The reference raises RuntimeError when its solve fails
+    (cloudfem/physics/em3d_tet10.py:360-367). A solve that stopped short of
+    its target - iteration cap, or no progress over several true-residual
+    replacements - is reported the same way, with the residual it reached
+    (rtol is named in the message); it is never returned as a result.
+    """
     if res.status == N.CFEM_OK:
         return
-    if res.status == N.CFEM_ERR_NOT_CONVERGED and res.relres <= 10.0 * rtol:
-        warnings.warn(f"{what}: stopped at relative residual "
-                      f"{res.relres:.2e} (target {rtol:.1e})", RuntimeWarning)
-        return
-    raise_for(res, what)
+    raise_for(res, f"{what} (target relative residual {rtol:.1e})")
 
 
 def solve_block(dm, bs, vals, rhs, fixed_idx, fixed_val, precision="fp64",

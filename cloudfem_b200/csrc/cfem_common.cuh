@@ -76,6 +76,8 @@ struct cfem_ctx {
     int graph_iters = 2;               // iterations per solve-loop body
     int pdl = 1;                       // dependent launches in solve graphs
     int spmv_stage = 1;                // SpMV: 0 registers, 1 staged scalar rows, 2 also 3x3
+    int barrier_timeout_us = 4000000;  // persistent grid-barrier wait limit
+    int barrier_hold = 0;              // phantom barrier arrivals (fault injection)
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // SpMV timing

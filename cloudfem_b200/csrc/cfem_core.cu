@@ -236,6 +236,16 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
                        "SpMV staging must be 0, 1 or 2 (got %d)", value);
             ctx->spmv_stage = value;
             return CFEM_OK;
+        case CFEM_PARAM_BARRIER_TIMEOUT_US:
+            CFEM_CHECK(value >= 1 && value <= 60000000, CFEM_ERR_INVALID,
+                       "grid-barrier wait limit must be 1 us .. 60 s (got %d us)", value);
+            ctx->barrier_timeout_us = value;
+            return CFEM_OK;
+        case CFEM_PARAM_BARRIER_HOLD:
+            CFEM_CHECK(value == 0 || value == 1, CFEM_ERR_INVALID,
+                       "phantom barrier arrivals must be 0 or 1 (got %d)", value);
+            ctx->barrier_hold = value;
+            return CFEM_OK;
         default:
             return fail(CFEM_ERR_INVALID, "unknown parameter %d", param);
     }
@@ -249,6 +259,8 @@ int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
         case CFEM_PARAM_GRAPH_ITERS: return ctx->graph_iters;
         case CFEM_PARAM_PDL: return ctx->pdl;
         case CFEM_PARAM_SPMV_STAGE: return ctx->spmv_stage;
+        case CFEM_PARAM_BARRIER_TIMEOUT_US: return ctx->barrier_timeout_us;
+        case CFEM_PARAM_BARRIER_HOLD: return ctx->barrier_hold;
         default: return -1;
     }
 }

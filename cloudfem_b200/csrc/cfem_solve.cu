@@ -26,6 +26,7 @@
 // convergence norm.
 #include "cfem_common.cuh"
 
+#include <cuda.h>
 #include <math.h>
 #include <string.h>
 
@@ -47,7 +48,6 @@ constexpr int MAX_STALL = 8;
 // a few eps * sum_j |a_ij x_j|; a residual at that level cannot be reduced
 // or even measured further, so it counts as converged.
 constexpr double FLOOR_C = 16.0 * 2.220446049250313e-16;
-constexpr unsigned long long BARRIER_TIMEOUT_NS = 4000000000ull;  // 4 s
 constexpr int BAR_GROUP = 16;              // blocks per first-level counter
 constexpr int BAR_MAX_GROUPS = 64;
 
@@ -140,7 +140,11 @@ __device__ __forceinline__ unsigned atom_add_acqrel(unsigned *p, unsigned v) {
 
 // Bounded two-level software grid barrier over co-resident blocks
 // (cooperative launch). Returns false when a block gave up waiting.
-__device__ bool grid_sync(GridBar *bar) {
+// `timeout_ns` bounds each wait (CFEM_PARAM_BARRIER_TIMEOUT_US); `hold`
+// phantom blocks are counted as still to arrive (CFEM_PARAM_BARRIER_HOLD,
+// fault injection for the host's timeout path: with hold > 0 no wait can
+// complete, so every block gives up at the limit and the launch returns).
+__device__ bool grid_sync(GridBar *bar, unsigned long long timeout_ns, unsigned hold) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *vgen = &bar->gen;
@@ -156,7 +160,7 @@ __device__ bool grid_sync(GridBar *bar) {
         if (atomicAdd(&bar->grp[grp][0], 1u) == gsize - 1) {
             atomicExch(&bar->grp[grp][0], 0u);
             __threadfence();
-            if (atomicAdd(&bar->top, 1u) == ngrp - 1) {
+            if (atomicAdd(&bar->top, 1u) == ngrp - 1 + hold) {
                 atomicExch(&bar->top, 0u);
                 __threadfence();
                 atomicAdd(&bar->gen, 1u);
@@ -169,7 +173,7 @@ __device__ bool grid_sync(GridBar *bar) {
             while (ld_acquire(&bar->gen) == g) {
                 if ((++spins & 1023u) == 0) {
                     if (*verr) break;
-                    if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+                    if (globaltimer() - t0 > timeout_ns) {
                         atomicExch(&bar->err, 1);
                         break;
                     }
@@ -881,7 +885,8 @@ k_pcg_init(const SysDev *__restrict__ sys, SysState *st,
 __global__ void __launch_bounds__(SOLVE_THREADS, 1)
 k_pcg_persistent(const SysDev *__restrict__ sys, SysState *st,
                  const int32_t *__restrict__ chunk_sys, int n_chunks,
-                 GridBar *bar, int max_steps) {
+                 GridBar *bar, int max_steps, unsigned long long timeout_ns,
+                 unsigned hold) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -889,7 +894,7 @@ k_pcg_persistent(const SysDev *__restrict__ sys, SysState *st,
     for (int step = 0; step < max_steps; ++step) {
         for (int c = gw; c < n_chunks; c += nw)
             dispatch<RUN_ALL>(sys, st, bar, chunk_sys, c, lane);
-        if (!grid_sync(bar)) return;
+        if (!grid_sync(bar, timeout_ns, hold)) return;
         if (*(volatile int *)&bar->active <= 0) return;
     }
 }
@@ -2155,6 +2160,8 @@ struct cfem_pcg_plan {
     int max_iter = 1;
     bool persistent = true;
     int grid = 1;
+    unsigned long long bar_timeout_ns = 4000000000ull;   // grid-barrier wait limit
+    unsigned bar_hold = 0;                               // phantom arrivals (tests)
     int per_iter = 0;
     std::vector<cfem::SysDev> hs;
     char *ws_copy = nullptr;      // system table, lists, working matrix copies
@@ -2336,6 +2343,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     P->persistent = persistent;
     P->grid = grid;
+    P->bar_timeout_ns = 1000ull * (unsigned long long)ctx->barrier_timeout_us;
+    P->bar_hold = (unsigned)ctx->barrier_hold;
     // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
     // systems a padded block copy (staged SpMV) or an entry-major copy.
     const bool stage3 = ctx->spmv_stage == 2;
@@ -2617,7 +2626,8 @@ static int plan_run(cfem_pcg_plan *P, cfem_solve_stats *stats, cudaStream_t s) {
     }
     if (P->persistent) {
         void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&P->d_chunks,
-                        (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
+                        (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps,
+                        (void *)&P->bar_timeout_ns, (void *)&P->bar_hold};
         CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(P->grid),
                                               dim3(SOLVE_THREADS), args, 0, w));
         g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -2777,23 +2787,44 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;   // 32 MiB
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch per device. In host code the array's
-// name is only a host-side stand-in, so the address is looked up once per
-// device with that device current and passed to the kernels.
-static void *g_noalloc_addr[64] = {nullptr};
+// Device address of g_noalloc_scratch per CUDA context. In host code the
+// array's name is only a host-side stand-in, so the address is looked up with
+// the device (and its context) current the first time a context calls, and
+// passed to the kernels. Keyed on the current driver context, so a caller
+// that makes its own (non-primary) context current gets that context's copy
+// of the array.
+struct NoallocAddr {
+    CUcontext cu;
+    void *addr;
+};
+static std::vector<NoallocAddr> g_noalloc_addr;
 static std::mutex g_noalloc_mu;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
 
-static int noalloc_scratch(int device, void **out) {
+static int noalloc_scratch(void **out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    CFEM_CHECK(device >= 0 && device < 64, CFEM_ERR_INVALID,
-               "device %d out of range for the allocation-free solver", device);
-    if (!g_noalloc_addr[device]) {
-        void *p = nullptr;
-        CFEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        CFEM_CHECK(p != nullptr, CFEM_ERR_CUDA, "scratch symbol has no address");
-        g_noalloc_addr[device] = p;
+    static CtxGetCurrentFn get_current = nullptr;
+    if (!get_current) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        CFEM_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        CFEM_CHECK(fn && q == cudaDriverEntryPointSuccess, CFEM_ERR_CUDA,
+                   "driver entry point cuCtxGetCurrent not found");
+        get_current = (CtxGetCurrentFn)fn;
     }
-    *out = g_noalloc_addr[device];
+    CUcontext cu = nullptr;
+    CFEM_CHECK(get_current(&cu) == CUDA_SUCCESS && cu, CFEM_ERR_CUDA,
+               "no current CUDA context");
+    for (const NoallocAddr &e : g_noalloc_addr)
+        if (e.cu == cu) {
+            *out = e.addr;
+            return CFEM_OK;
+        }
+    void *p = nullptr;
+    CFEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    CFEM_CHECK(p != nullptr, CFEM_ERR_CUDA, "scratch symbol has no address");
+    g_noalloc_addr.push_back({cu, p});
+    *out = p;
     return CFEM_OK;
 }
 
@@ -2862,7 +2893,7 @@ extern "C" int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *L,
                need, NOALLOC_SCRATCH_BYTES);
 
     void *base = nullptr;
-    CFEM_TRY(noalloc_scratch(ctx->device, &base));
+    CFEM_TRY(noalloc_scratch(&base));
     char *ws = (char *)base;
     // Every call reuses the array: clear all of it that this call uses
     // (state, tickets, chunk table, p buffers) before the launch.
@@ -2899,8 +2930,11 @@ extern "C" int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *L,
     int max_steps = 3 * L->max_iter + 16;
     CFEM_LAUNCH(k_pcg_init, grid_for((int64_t)n_chunks * 32, 256), 256, 0, s,
                 d_sys, d_st, d_chunks, n_chunks, d_bar);
+    unsigned long long bar_timeout_ns = 1000ull * (unsigned long long)ctx->barrier_timeout_us;
+    unsigned bar_hold = (unsigned)ctx->barrier_hold;
     void *args[] = {(void *)&d_sys, (void *)&d_st, (void *)&d_chunks,
-                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps};
+                    (void *)&n_chunks, (void *)&d_bar, (void *)&max_steps,
+                    (void *)&bar_timeout_ns, (void *)&bar_hold};
     CFEM_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg_persistent, dim3(grid),
                                           dim3(SOLVE_THREADS), args, 0, s));
     g_launches.fetch_add(1, std::memory_order_relaxed);

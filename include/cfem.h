@@ -177,10 +177,18 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * streams each scalar work entry's span through two shared-memory windows
  * of about 4 KB per warp with 1-D bulk copies (TMA) and loads 3x3 blocks
  * into registers, 2 streams 3x3 blocks through shared memory too (slower on
- * the elasticity beam: kept for tuning), 0 loads both into registers. get
- * returns -1 for an unknown parameter. */
+ * the elasticity beam: kept for tuning), 0 loads both into registers.
+ * BARRIER_TIMEOUT_US: how long (microseconds, 1 .. 60e6; default 4e6) a
+ * block of the persistent scheduler waits at its grid barrier before it
+ * gives up; the solve then ends with CFEM_ERR_TIMEOUT and the context stays
+ * usable. BARRIER_HOLD: fault injection for that path (0 default, or 1):
+ * the barrier counts one phantom block that never arrives, so every wait
+ * runs to the limit; no other waits of the library are affected. Both are
+ * read when a solve plan is created. get returns -1 for an unknown
+ * parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
-       CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5 };
+       CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5, CFEM_PARAM_BARRIER_TIMEOUT_US = 6,
+       CFEM_PARAM_BARRIER_HOLD = 7 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */
@@ -389,12 +397,18 @@ CFEM_API int cfem_cocg_solve(cfem_ctx *ctx, int64_t n, const int32_t *d_indptr,
  * synchronisation. The solver workspace is a fixed file-scope device array
  * of cfem_pcg_noalloc_capacity() bytes (32 MiB), held by every GPU that
  * loads the library until the process exits; systems that need more are
- * rejected with CFEM_ERR_INVALID. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture. Every call reuses the same array and clears it
- * first: calls that overlap on the GPU (other streams, other threads) race
- * and must be serialised by the caller. stats->kernel_ms is 0 (no timing
- * events are created). Otherwise identical to cfem_pcg_solve. Synchronises. */
+ * rejected with CFEM_ERR_INVALID. The first call in each CUDA context looks
+ * up the array's device address (cudaGetSymbolAddress) and keeps it for
+ * that context, so make that first call before any stream capture, and do
+ * not reset the device (cudaDeviceReset) after it. Every call reuses the
+ * same array and clears it first: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.
+ * It always runs the persistent scheduler (one cooperative launch, the
+ * grid strided over the row chunks when they exceed one resident wave):
+ * the context's scheduler, SpMV staging and tuned solve-loop parameters have
+ * no effect (its grid-barrier wait limit does), and stats->kernel_ms and
+ * stats->spmv_ms are 0 (no timing events are created). The arithmetic is
+ * that of cfem_pcg_solve on the persistent scheduler. Synchronises. */
 CFEM_API size_t cfem_pcg_noalloc_capacity(void);
 CFEM_API int cfem_pcg_solve_noalloc(cfem_ctx *ctx, const cfem_linsys *system,
                                     cfem_solve_stats *stats, void *stream);

@@ -21,6 +21,14 @@ def golden():
         return {k: z[k] for k in z.files}
 
 
+@pytest.fixture(scope="session")
+def config_golden():
+    """Reference outputs on the benchmark configurations (make_config_golden.py)."""
+    path = os.path.join(ROOT, "tests", "golden", "config_fixtures.npz")
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
 def golden_csr(golden, name):
     import scipy.sparse as sp
     shape = tuple(int(v) for v in golden[name + "__shape"])
@@ -68,3 +76,56 @@ def assert_close(a, b, rtol=1e-12, what=""):
     scale = max(float(np.abs(b).max(initial=0.0)), 1e-300)
     err = float(np.abs(a - b).max(initial=0.0)) / scale
     assert err <= rtol, f"{what}: rel err {err:.3e} > {rtol:.1e}"
+
+
+# Entry-wise tolerance of matrix values. Each entry is a sum of element
+# contributions; summed in another order it differs by a few ulps of the
+# largest contribution, so an entry that cancels to (near) zero cannot be
+# compared relative to itself. Entries are held to rtol of their own
+# magnitude, with a floor of CANCEL_EPS times the largest entry of their row.
+CANCEL_EPS = 64 * np.finfo(float).eps
+
+
+def assert_csr_entrywise(A, B, rtol=1e-12, what="CSR"):
+    """Bit-exact indptr / indices; every value within rtol of itself (floor:
+    CANCEL_EPS of its row's largest entry). Returns (max entry-relative
+    error over entries above the floor, count of entries at the floor)."""
+    A = A.tocsr()
+    B = B.tocsr()
+    assert A.shape == B.shape, f"{what}: shape {A.shape} vs {B.shape}"
+    np.testing.assert_array_equal(np.asarray(A.indptr, np.int64),
+                                  np.asarray(B.indptr, np.int64))
+    np.testing.assert_array_equal(np.asarray(A.indices, np.int64),
+                                  np.asarray(B.indices, np.int64))
+    absb = np.abs(B.data)
+    rows = np.repeat(np.arange(B.shape[0]), np.diff(B.indptr))
+    rowmax = np.zeros(B.shape[0])
+    np.maximum.at(rowmax, rows, absb)
+    floor = CANCEL_EPS * rowmax[rows]
+    diff = np.abs(A.data - B.data)
+    bad = diff > rtol * absb + floor
+    assert not bad.any(), (
+        f"{what}: {int(bad.sum())} entries differ beyond {rtol:.0e} "
+        f"(worst {float((diff / np.maximum(absb, 1e-300)).max()):.3e})")
+    big = absb > floor / rtol
+    worst = float((diff[big] / absb[big]).max(initial=0.0))
+    return worst, int((~big).sum())
+
+
+def assert_entrywise(a, b, rtol=1e-12, what="vector"):
+    """Every entry within rtol of itself, floor CANCEL_EPS of the largest."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    assert a.shape == b.shape, f"{what}: shape {a.shape} vs {b.shape}"
+    floor = CANCEL_EPS * float(np.abs(b).max(initial=0.0))
+    diff = np.abs(a - b)
+    bad = diff > rtol * np.abs(b) + floor
+    assert not bad.any(), f"{what}: {int(bad.sum())} entries beyond {rtol:.0e}"
+
+
+def rel_err(a, b):
+    """max |a - b| / max |b| (the solution error measure of the tests)."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    return float(np.abs(a - b).max(initial=0.0)) / max(
+        float(np.abs(b).max(initial=0.0)), 1e-300)

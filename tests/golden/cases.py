@@ -100,3 +100,64 @@ def avt_js(x, y, z):
 
 def avt_scale(t):
     return np.sin(2.0 * np.pi * 250.0 * t)
+
+
+# ------------------------------------------------ configuration-scale cases
+# These reproduce the benchmark configurations (or seeded subsets of them)
+# at sizes the reference finishes in seconds to minutes; their reference
+# answers are in config_fixtures.npz (make_config_golden.py).
+
+# C1: P1 steady heat, unit cube 20^3 Kuhn box, k = 1, f = 3 pi^2 sin sin sin
+# at centroids, T = 0 on all six faces
+C1_N = 20
+
+# C3: seeded Tet10 unit cubes, lognormal(0, 1) conductivity per hex cell,
+# f = 1, T = 0 on all faces; the reference is run on the small ones
+C3_SEED = 11
+C3_GOLDEN_NS = (4, 5, 6, 8)
+
+
+def c3_draw(ns, seed=C3_SEED):
+    """One lognormal(0, 1) conductivity per hex cell (cell order k, j, i)."""
+    rng = np.random.default_rng(seed)
+    return [rng.lognormal(0.0, 1.0, int(n) ** 3) for n in ns]
+
+
+def c3_cell_fn(n, kc):
+    """Per-cell conductivity as a callable k(x, y, z) of the unit cube,
+    the form the reference's API takes (Keast points are interior, so every
+    point of an element looks up its own cell)."""
+    kc3 = np.asarray(kc).reshape(n, n, n)
+
+    def k(x, y, z):
+        i = np.minimum((np.asarray(x) * n).astype(int), n - 1)
+        j = np.minimum((np.asarray(y) * n).astype(int), n - 1)
+        kk = np.minimum((np.asarray(z) * n).astype(int), n - 1)
+        return kc3[kk, j, i]
+    return k
+
+
+# C4: P1 transient heat, Crank-Nicolson, Robin on all faces, Gaussian source
+# at the centre, at n = 32 for 20 steps of 1 s
+C4_N = 32
+C4_STEPS = 20
+C4 = dict(k=45.0, rho_cp=3.6e6, t0=20.0, h=25.0, t_inf=20.0, q0=1e7,
+          sigma=0.1, dt=1.0)
+
+
+def c4_source(x, y, z):
+    r2 = ((np.asarray(x) - 0.5) ** 2 + (np.asarray(y) - 0.5) ** 2
+          + (np.asarray(z) - 0.5) ** 2)
+    return C4["q0"] * np.exp(-r2 / (2.0 * C4["sigma"] ** 2))
+
+
+def c4_robin():
+    return {f: (C4["h"], C4["t_inf"]) for f in FACES}
+
+
+# C2 at quarter resolution: Tet10 cantilever 2.0 x 0.25 x 0.25 m, 40 x 5 x 5
+# cells, clamped at x = 0, 1 MPa traction in -z on x = 2
+C2Q_BOX = (40, 5, 5, (0.0, 2.0), (0.0, 0.25), (0.0, 0.25))
+C2_E, C2_NU = 210e9, 0.3
+C2_BC = {"xmin": (0.0, 0.0, 0.0)}
+C2_TRACTION = {"xmax": (0.0, 0.0, -1e6)}

@@ -227,4 +227,6 @@ def main(ref_path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the CloudFEM checkout>")
+    main(sys.argv[1])
