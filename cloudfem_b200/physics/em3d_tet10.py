@@ -14,6 +14,17 @@ Drop-in for the assembly of cloudfem/physics/em3d_tet10.py:
   symmetric positive definite scaling of the step matrix and one device
   PCG solve (one graph launch) per step; ``transient_joule_power_tet10``
   (:665-692) vectorised.
+* ``solve_eddy_current_nonlinear_tet10`` (:849-982): the secant B-H Picard
+  loop, K rebuilt on the device from the updated per-element reluctivity
+  each iteration and each linear phasor solve by device COCG warm-started
+  from the previous iterate; ``bh_secant_mu_r`` (:716-743) is the model
+  curve.
+* Post-processing the reference's other modules import
+  (``induction3d_tet10.py:101-104``, ``inductance.py:22-24``):
+  ``element_flux_density_tet10`` (:378-390), ``total_joule_power_tet10``
+  (:393-419), ``source_complex_power_tet10`` (:422-451) and
+  ``magnetic_energy_tet10`` (:695-713), vectorised over elements on the host
+  (``magnetic_energy_tet10`` assembles K on the device when not given).
 
 Element matrices are computed by warp-per-element kernels (Keast-5
 gradients staged in shared memory) and summed into the node pattern by the
@@ -41,6 +52,9 @@ from ..device import DeviceMesh, centroids, evaluate, ptr
 MU0 = 4e-7 * np.pi
 
 __all__ = ["assemble_tet10_av", "solve_eddy_current_tet10",
+           "element_flux_density_tet10", "total_joule_power_tet10",
+           "source_complex_power_tet10", "magnetic_energy_tet10",
+           "bh_secant_mu_r", "solve_eddy_current_nonlinear_tet10",
            "transient_eddy_current_tet10", "transient_joule_power_tet10", "MU0"]
 
 
@@ -271,11 +285,15 @@ def solve_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, omega=0.0,
 
 def _solve_phasor_with_K_tet10(mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s,
                                boundary, a_bc, permc_spec=None, *, rtol=1e-10,
-                               max_iter=None):
+                               max_iter=None, dm=None, js_rhs=None, x0=None):
     """One linear phasor solve with a given curl-curl block K
     (em3d_tet10.py:774-846, used by the nonlinear Picard loop, :938): block
     system with the V rows scaled by 1/(i w), source load, Dirichlet
-    elimination as the reference, device COCG; returns (a, v)."""
+    elimination as the reference, device COCG; returns (a, v).
+
+    Keyword-only extras for repeated solves on one mesh: dm (its
+    DeviceMesh), js_rhs (the A-block source load, computed once), x0 (a
+    previous (a, v) used as the initial guess)."""
     import torch
     n = mesh.n_nodes
     n_v = len(v_nodes)
@@ -283,8 +301,10 @@ def _solve_phasor_with_K_tet10(mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s
     A_sys = sp.bmat([[K + 1j * w * M, Gs], [Gs.T, S * (1.0 / (1j * w))]],
                     format="csr")
     rhs = np.zeros(3 * n + n_v, dtype=complex)
-    dm = DeviceMesh(mesh)
-    if J_s is not None:
+    dm = dm if dm is not None else DeviceMesh(mesh)
+    if js_rhs is not None:
+        rhs[:3 * n] += js_rhs
+    elif J_s is not None:
         rhs[:3 * n] += _js_load(mesh, dm, J_s)
     fixed = {}
     if B_applied is not None:
@@ -314,7 +334,12 @@ def _solve_phasor_with_K_tet10(mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s
     d_ix = torch.from_numpy(A2.indices.astype(np.int32)).to(dev)
     d_a = torch.from_numpy(np.ascontiguousarray(A2.data, dtype=np.complex128).view(np.float64)).to(dev)
     d_b = torch.from_numpy(np.ascontiguousarray(rhs2, dtype=np.complex128).view(np.float64)).to(dev)
-    d_x = torch.zeros(2 * n2, dtype=torch.float64, device=dev)
+    if x0 is None:
+        d_x = torch.zeros(2 * n2, dtype=torch.float64, device=dev)
+    else:
+        guess = np.concatenate([np.asarray(x0[0], dtype=complex).ravel(),
+                                np.asarray(x0[1], dtype=complex)[v_nodes]])[keep]
+        d_x = torch.from_numpy(np.ascontiguousarray(guess).view(np.float64)).to(dev)
     st = N.SolveStats()
     # COCG with Jacobi needed ~6,400 iterations at 37 k unknowns (box 10^3)
     mi = max_iter if max_iter is not None else max(5000, 50 * int(np.sqrt(n2)))
@@ -346,6 +371,200 @@ def last_solve_info():
     """COCG iterations, relative residual and device time of the last
     solve_eddy_current_tet10."""
     return dict(_last_info)
+
+
+# ------------------------------------------------------ post-processing
+
+def _corner_geometry(mesh):
+    """Connectivity (M, 10), corner Jacobians (M, 3, 3) (columns p_k - p_0,
+    as element_operators builds them, tet10.py:103-126) and volumes."""
+    els = np.asarray(mesh.elements, dtype=np.int64)
+    p = np.asarray(mesh.nodes, dtype=float)[els[:, :4]]
+    J = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]], axis=2)
+    return els, J, np.abs(np.linalg.det(J)) / 6.0
+
+
+def _keast_operators(mesh):
+    """Per element at the Keast-5 points: G (M, 5, 10, 3), N (5, 10),
+    xq (M, 5, 3), weights (5,), volumes (M,), connectivity."""
+    from ..fem.tet10 import quadrature, shape_functions
+    els, J, vol = _corner_geometry(mesh)
+    Lq, wq = quadrature()
+    Nq, dN = shape_functions(Lq)
+    dxi = np.stack([dN[..., 1] - dN[..., 0], dN[..., 2] - dN[..., 0],
+                    dN[..., 3] - dN[..., 0]], axis=-1)          # (5, 10, 3)
+    G = np.einsum("qpk,ekl->eqpl", dxi, np.linalg.inv(J))
+    xq = np.einsum("qc,ecx->eqx", Lq, np.asarray(mesh.nodes, dtype=float)[els[:, :4]])
+    return G, Nq, xq, wq, vol, els
+
+
+def element_flux_density_tet10(mesh, a):
+    """B = curl A at every element centroid [T], (M, 3) complex
+    (em3d_tet10.py:378-390): B = sum_p grad N_p x a_p with the gradients
+    at the centroid (the first Keast point)."""
+    from ..fem.tet10 import shape_functions
+    a = np.asarray(a, dtype=complex).reshape(-1, 3)
+    els, J, _ = _corner_geometry(mesh)
+    _, dN = shape_functions(np.full(4, 0.25))
+    dxi = np.stack([dN[:, 1] - dN[:, 0], dN[:, 2] - dN[:, 0],
+                    dN[:, 3] - dN[:, 0]], axis=-1)              # (10, 3)
+    G0 = np.einsum("pk,ekl->epl", dxi, np.linalg.inv(J))        # (M, 10, 3)
+    return np.cross(G0, a[els]).sum(axis=1)
+
+
+def total_joule_power_tet10(mesh, a, v, sigma, omega):
+    """Time-averaged Joule power [W] of a phasor field and the per-element
+    heating density [W/m^3] (em3d_tet10.py:393-419): E = -i w A - grad V is
+    quadratic per element, so with nodal values E_p and the exact Tet10
+    mass matrix, P_e = sigma_e V_e / 2 sum_pq M_ref[p, q] Re(E_p . E_q*).
+    Returns (P_total, Q_elem); Q is 0 where sigma is 0."""
+    from ..fem.tet10 import _MASS_REF
+    a = np.asarray(a, dtype=complex).reshape(-1, 3)
+    v = np.asarray(v, dtype=complex)
+    sig_e = _element_values(mesh, sigma)
+    on = sig_e > 0.0
+    Q = np.zeros(len(sig_e))
+    if not on.any():
+        return 0.0, Q
+    sub = types.SimpleNamespace(nodes=mesh.nodes, elements=np.asarray(mesh.elements)[on])
+    els, _, vol = _corner_geometry(sub)
+    grads = _nodal_gradients_all(sub)                           # (m, 10, 10, 3)
+    Ep = -1j * float(omega) * a[els] - np.einsum("epjx,ej->epx", grads, v[els])
+    re = np.real(np.einsum("epm,eqm->epq", Ep, Ep.conj()))
+    P_e = 0.5 * sig_e[on] * vol * np.einsum("pq,epq->e", _MASS_REF, re)
+    Q[on] = P_e / vol
+    vols_all = _corner_geometry(mesh)[2]
+    return float(np.sum(Q * vols_all)), Q
+
+
+def source_complex_power_tet10(mesh, a, v, J_s, omega):
+    """Complex power delivered by the imposed current [VA]
+    (em3d_tet10.py:422-451): S = -1/2 sum_e V_e sum_q w_q J_s(x_q)* . E(x_q)
+    with the discrete E = -i w A - grad V at the Keast points."""
+    a = np.asarray(a, dtype=complex).reshape(-1, 3)
+    v = np.asarray(v, dtype=complex)
+    G, Nq, xq, wq, vol, els = _keast_operators(mesh)
+    flat = xq.reshape(-1, 3)
+    Jq = np.array([np.asarray(J_s(x, y, z), dtype=complex).ravel()
+                   for x, y, z in flat]).reshape(xq.shape[0], xq.shape[1], 3)
+    Eq = (-1j * float(omega) * np.einsum("qp,epm->eqm", Nq, a[els])
+          - np.einsum("eqjm,ej->eqm", G, v[els]))
+    S = np.sum(vol * np.einsum("q,eqm,eqm->e", wq, Jq.conj(), Eq))
+    return -0.5 * complex(S)
+
+
+def magnetic_energy_tet10(mesh, a, nu=1.0 / MU0, K=None):
+    """Time-averaged stored magnetic energy [J] of a phasor A field,
+    W = Re(a^H K a) / 4 with the assembled curl-curl matrix
+    (em3d_tet10.py:695-713); K is assembled on the device when not given."""
+    a = np.asarray(a, dtype=complex).reshape(-1, 3).ravel()
+    if K is None:
+        K = assemble_tet10_av(mesh, nu=nu)[0]
+    return 0.25 * float(np.real(np.vdot(a, K @ a)))
+
+
+def bh_secant_mu_r(Hmag, bsat=1.9, mu_mag0=200.0):
+    """Secant relative permeability of the analytic magnetisation curve
+    M(H) = Ms tanh(H / H_ref), Ms = bsat / mu0, H_ref = Ms / mu_mag0
+    (em3d_tet10.py:716-743): mu_r = 1 + mu_mag0 tanh(h) / h, h = |H| / H_ref,
+    with the series 1 - h^2 / 3 for tanh(h) / h below h = 1e-6."""
+    H = np.asarray(Hmag, dtype=float)
+    if mu_mag0 == 0.0:
+        return np.ones_like(H)
+    Ms = float(bsat) / MU0
+    h = np.abs(H) / (Ms / float(mu_mag0))
+    ratio = np.where(h > 1.0e-6, np.tanh(h) / np.maximum(h, 1.0e-300), 1.0 - h * h / 3.0)
+    return 1.0 + float(mu_mag0) * ratio
+
+
+def _as_fn(q):
+    return q if callable(q) else (lambda x, y, z, _q=q: _q)
+
+
+def solve_eddy_current_nonlinear_tet10(mesh, nu=1.0 / MU0, sigma=0.0, omega=0.0,
+                                       B_applied=None, J_s=None, boundary=None,
+                                       a_bc=None, gauge_eps=1e-6, permc_spec=None,
+                                       iron=None, bsat=1.9, mu_mag0=200.0,
+                                       mu_init=None, tol=1e-3, max_iter=50,
+                                       relax=0.5, *, rtol=1e-10, cocg_max_iter=None):
+    """Nonlinear (secant B-H) phasor A-V solve by Picard iteration
+    (em3d_tet10.py:849-982); returns (a, v, info) as the reference does.
+
+    The sigma blocks (M, G, S) are assembled once; every iteration rebuilds
+    K on the device from the per-element reluctivity (the same mesh pattern,
+    no pattern rebuild), solves the phasor system by device COCG to rtol,
+    warm-started from the previous iterate, and relaxes nu of the iron
+    elements towards the curve's secant value at |H| = nu |B| (centroid B).
+    Convergence: relative change of |B| over the iron elements (all
+    elements without iron) below tol; info carries iterations, converged,
+    rel_dB, P (Joule power per solve), mu_r_elem, nu_elem, B_elem,
+    iron_mask, relax and tol. permc_spec is accepted and has no effect.
+    """
+    if omega <= 0:
+        raise ValueError("omega must be positive (phasor eddy-current "
+                         "solve; omega = 0 magnetostatics is out of scope)")
+    if B_applied is None and J_s is None:
+        raise ValueError("no excitation: pass B_applied (background "
+                         "field) or J_s (imposed current density)")
+    if tol <= 0:
+        raise ValueError("tol must be positive")
+    if max_iter < 1:
+        raise ValueError("max_iter must be >= 1")
+    if not (0.0 < relax <= 1.0):
+        raise ValueError("relax must be in (0, 1]")
+    _, M, Gs, S, v_nodes, sig_e, conducting = assemble_tet10_av(
+        mesh, nu=1.0, sigma=sigma, gauge_eps=gauge_eps)
+    if not conducting.any():
+        raise ValueError("no conducting elements (sigma > 0) in mesh")
+    nu_e = _element_values(mesh, nu)
+    if iron is None:
+        iron_mask = np.zeros(len(nu_e), dtype=bool)
+    else:
+        fn = _as_fn(iron)
+        cen = centroids(np.asarray(mesh.nodes, dtype=float), np.asarray(mesh.elements))
+        iron_mask = np.array([bool(fn(x, y, z)) for x, y, z in cen], dtype=bool)
+    mu_r0 = (1.0 + float(mu_mag0)) if mu_init is None else float(mu_init)
+    nu_e[iron_mask] = 1.0 / (MU0 * mu_r0)
+
+    dm = DeviceMesh(mesh)
+    js_rhs = _js_load(mesh, dm, J_s) if J_s is not None else None
+    sel = iron_mask if iron_mask.any() else slice(None)
+    hist_rel, hist_P, cocg_iters = [], [], []
+    B_prev = None
+    converged = False
+    a = v = B = None
+    it = 0
+    for it in range(1, max_iter + 1):
+        K = _curl_curl(dm, nu_e)
+        a, v = _solve_phasor_with_K_tet10(
+            mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s, boundary, a_bc,
+            permc_spec, rtol=rtol, max_iter=cocg_max_iter, dm=dm, js_rhs=js_rhs,
+            x0=None if a is None else (a, v))
+        cocg_iters.append(_last_info["iterations"])
+        B = element_flux_density_tet10(mesh, a)
+        B_amp = np.sqrt(np.sum(np.abs(B) ** 2, axis=1))
+        hist_P.append(total_joule_power_tet10(mesh, a, v, sigma, omega)[0])
+        if B_prev is not None:
+            denom = max(float(np.linalg.norm(B_amp[sel])), 1e-300)
+            rel = float(np.linalg.norm(B_amp[sel] - B_prev[sel]) / denom)
+            hist_rel.append(rel)
+            if rel < tol:
+                converged = True
+                break
+        if it == max_iter:
+            break
+        B_prev = B_amp
+        if iron_mask.any():
+            mu_t = bh_secant_mu_r(B_amp[iron_mask] * nu_e[iron_mask], bsat=bsat,
+                                  mu_mag0=mu_mag0)
+            nu_e[iron_mask] = ((1.0 - relax) * nu_e[iron_mask]
+                               + relax / (MU0 * mu_t))
+    info = {"iterations": it, "converged": converged,
+            "rel_dB": np.array(hist_rel), "P": np.array(hist_P),
+            "mu_r_elem": 1.0 / (MU0 * nu_e), "nu_elem": nu_e.copy(),
+            "B_elem": B, "iron_mask": iron_mask, "relax": relax, "tol": tol,
+            "cocg_iterations": np.array(cocg_iters)}
+    return a, v, info
 
 
 # ------------------------------------------------------ transient (theta)

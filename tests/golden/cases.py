@@ -161,3 +161,23 @@ C2Q_BOX = (40, 5, 5, (0.0, 2.0), (0.0, 0.25), (0.0, 0.25))
 C2_E, C2_NU = 210e9, 0.3
 C2_BC = {"xmin": (0.0, 0.0, 0.0)}
 C2_TRACTION = {"xmax": (0.0, 0.0, -1e6)}
+
+
+# nonlinear (secant B-H) phasor A-V: iron and conductor in x < 0.5, a
+# background field strong enough to saturate part of the iron
+AVN_N = 3
+AVN_OMEGA = 2.0 * np.pi * 50.0
+AVN_B = (0.0, 0.0, 2.5)
+AVN_KW = dict(tol=1e-3, max_iter=40, relax=0.8)
+
+
+def avn_sigma(x, y, z):
+    return 2.0e6 if x < 0.5 else 0.0
+
+
+def avn_iron(x, y, z):
+    return x < 0.5
+
+
+# B-H curve sample points [A/m], including the small-h series branch
+BH_H = np.array([0.0, 1e-9, 1.0, 30.0, 500.0, 3e3, 2e4, 1e5, 1e6])

@@ -209,6 +209,30 @@ def main(ref_path):
                                        boundary=list(C.FACES))
     put("avp_a", a)
     put("avp_v", v)
+    # post-processing of the phasor field (em3d_tet10.py:378-451, 695-713)
+    put("avp_B", em.element_flux_density_tet10(mp, a))
+    P, Q = em.total_joule_power_tet10(mp, a, v, C.AVP_SIGMA, C.AVP_OMEGA)
+    put("avp_P", np.array(P))
+    put("avp_Q", Q)
+    put("avp_S", np.array(em.source_complex_power_tet10(mp, a, v, C.avp_js,
+                                                         C.AVP_OMEGA)))
+    put("avp_Wm", np.array(em.magnetic_energy_tet10(mp, a, nu=C.nu_fn)))
+    put("bh_mu_r", em.bh_secant_mu_r(C.BH_H))
+    put("bh_mu_r_soft", em.bh_secant_mu_r(C.BH_H, bsat=1.2, mu_mag0=50.0))
+
+    # ---------------- Tet10 nonlinear (secant B-H) phasor A-V ----------------
+    mn = box_mesh_tet10(C.AVN_N, C.AVN_N, C.AVN_N)
+    a, v, info = em.solve_eddy_current_nonlinear_tet10(
+        mn, sigma=C.avn_sigma, omega=C.AVN_OMEGA, B_applied=C.AVN_B,
+        iron=C.avn_iron, boundary=list(C.FACES), **C.AVN_KW)
+    put("avn_a", a)
+    put("avn_v", v)
+    put("avn_iterations", np.array(info["iterations"]))
+    put("avn_converged", np.array(info["converged"]))
+    put("avn_rel_dB", info["rel_dB"])
+    put("avn_P", info["P"])
+    put("avn_mu_r", info["mu_r_elem"])
+    put("avn_B", info["B_elem"])
 
     # ---------------- Tet10 A-V transient (theta method, LU) ----------------
     mt = box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)

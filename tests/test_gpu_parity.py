@@ -275,3 +275,34 @@ def test_av_transient_golden(cf, golden, precision):
     for k in ("a_end", "v_end"):
         ref = golden["avt_" + k]
         assert np.linalg.norm(r[k] - ref) <= tol * np.linalg.norm(ref)
+
+
+def test_av_magnetic_energy_golden(cf, golden):
+    """W_m = Re(a^H K a)/4 with K assembled on the device."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    m = cf.mesh.box_mesh_tet10(C.AVP_N, C.AVP_N, C.AVP_N)
+    W = em.magnetic_energy_tet10(m, golden["avp_a"], nu=C.nu_fn)
+    Wg = float(golden["avp_Wm"])
+    assert abs(W - Wg) <= 1e-12 * abs(Wg)
+
+
+def test_av_nonlinear_picard_golden(cf, golden):
+    """Secant B-H Picard loop (K rebuilt on the device each iteration,
+    device COCG per linear solve) against the reference's SuperLU loop:
+    same iteration count and convergence flag; fields, power history and
+    permeabilities within the linear solves' accuracy."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    g = golden
+    m = cf.mesh.box_mesh_tet10(C.AVN_N, C.AVN_N, C.AVN_N)
+    a, v, info = em.solve_eddy_current_nonlinear_tet10(
+        m, sigma=C.avn_sigma, omega=C.AVN_OMEGA, B_applied=C.AVN_B,
+        iron=C.avn_iron, boundary=list(C.FACES), **C.AVN_KW)
+    assert info["iterations"] == int(g["avn_iterations"])
+    assert info["converged"] == bool(g["avn_converged"])
+    tol = 1e-8
+    assert np.linalg.norm(a - g["avn_a"]) <= tol * np.linalg.norm(g["avn_a"])
+    assert np.linalg.norm(v - g["avn_v"]) <= tol * np.linalg.norm(g["avn_v"])
+    assert_close(info["P"], g["avn_P"], tol, "power history")
+    assert_close(info["mu_r_elem"], g["avn_mu_r"], tol, "mu_r")
+    assert_close(np.abs(info["B_elem"]), np.abs(g["avn_B"]), tol, "|B|")
+    assert np.abs(info["rel_dB"] - g["avn_rel_dB"]).max() <= 1e-6 * g["avn_rel_dB"].max()
