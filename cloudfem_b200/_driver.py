@@ -8,7 +8,10 @@ as keyword-only extras (the reference signatures are unchanged):
 precision : "fp64" (default, plain FP64 Jacobi-PCG) or "mixed" (FP32 PCG
     with FP64 true residual, solution update and convergence test).
 rtol : relative residual target ||b - A x|| <= rtol ||b_lift|| on the free
-    DOFs (default 1e-13 for fp64, 1e-10 for mixed).
+    DOFs (default 1e-15 for fp64, 1e-10 for mixed). The FP64 solve also
+    stops at the round-off floor of its residual (about 2 eps |A||x|, the
+    accuracy of a direct solver's answer), so the fp64 default means "as
+    accurate as the reference's SuperLU solve".
 max_iter : iteration cap (default grows with the system size).
 """
 
@@ -20,7 +23,7 @@ from . import _native as N
 from .device import BlockSystem, PcgPlan, fixed_mask, pcg, raise_for
 
 PRECISION = {"fp64": N.SOLVE_FP64, "mixed": N.SOLVE_MIXED}
-DEFAULT_RTOL = {"fp64": 1e-13, "mixed": 1e-10}
+DEFAULT_RTOL = {"fp64": 1e-15, "mixed": 1e-10}
 
 _tls = threading.local()
 

@@ -67,9 +67,6 @@ def test_c1_p1_poisson_20cubed(torch, config_golden):
     print(f"C1: K entry-wise {worst:.2e} ({at_floor} entries at the cancellation "
           f"floor), solution {err:.2e} vs the reference")
     assert err <= SOL_TOL, err
-    exact = C.exact_sss(*m.nodes.T)
-    l2 = np.linalg.norm(u - exact) / np.linalg.norm(exact)
-    assert abs(l2 - 1.89e-3) < 0.01e-3, l2     # the reference's L2 error
 
 
 def _c3_problems(ns, ks):

@@ -21,6 +21,7 @@ import cases as C
 pytestmark = pytest.mark.gpu
 
 SOL_RTOL = 1e-10
+MIXED_RTOL = 1e-8
 
 
 @pytest.fixture(scope="module")
@@ -173,8 +174,11 @@ def test_noalloc_strided_grid_matches_allocating_solver(torch, mode_name):
         x = sys_.x.cpu().numpy()
         assert st.iterations == r_pers.iterations
         assert np.array_equal(x, x_pers), f"call {call}"
+        # another scheduler sums in another order: the suite's tolerance
+        # for the precision (FP64 1e-10, mixed 1e-8)
+        tol = SOL_RTOL if mode_name == "fp64" else MIXED_RTOL
         err = np.abs(x - x_auto).max() / np.abs(x_auto).max()
-        assert err <= SOL_RTOL, f"call {call}: rel diff {err:.3e}"
+        assert err <= tol, f"call {call}: rel diff {err:.3e}"
     assert _pool_reserved(rt, 2 ** 64 - 1) == before, "the library allocated"
 
 
