@@ -67,6 +67,14 @@ def _set_scheduler(rt, name):
         rt.set_param(N.PARAM_SPMV_STAGE, SPMV_STAGE)
 
 
+def _scalar_spmv_kernel(rt):
+    """Name of the scalar SpMV-phase kernel the context's staging selects."""
+    from cloudfem_b200 import _native as N
+    stage = rt.get_param(N.PARAM_SPMV_STAGE)
+    return {0: "k_gx (register path)", 3: "k_gxl (sliced ELL, one row per lane)"}.get(
+        stage, "k_gxs (matrix bulk-staged through shared memory)")
+
+
 def _barrier(world):
     """Every rank at the same point with its GPU idle: before and after each
     timed region (on one process only the device synchronisation)."""
@@ -563,7 +571,7 @@ def run_batched_heat(args, rank, world, local_rank):
     if spmv_ms > 0:
         ach = spmv_b / (spmv_ms * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": "k_gxs (batched PCG SpMV phase over all systems, matrix bulk-staged through shared memory: q = A p, p.q)",
+            "kernel": _scalar_spmv_kernel(rt) + " (batched PCG SpMV phase over all systems: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": spmv_ms,
@@ -758,7 +766,7 @@ def run_transient_heat(args, rank, world, local_rank):
     if spmv:
         ach = spmv_b / (float(np.mean(spmv)) * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": "k_gxs (scalar PCG SpMV phase, matrix bulk-staged through shared memory: q = A p, p.q)",
+            "kernel": _scalar_spmv_kernel(rt) + " (scalar PCG SpMV phase: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": float(np.mean(spmv)), "traffic": None,
@@ -1202,10 +1210,11 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
                     help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
-    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2],
+    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2, 3],
                     help="SpMV: 1 scalar rows bulk-staged through shared memory, 3x3 "
-                         "blocks in registers (library default); 2 both staged; 0 "
-                         "both in registers")
+                         "blocks in registers; 2 both staged; 0 both in registers; 3 "
+                         "scalar rows in the sliced-ELL layout (one row per lane), 3x3 "
+                         "blocks in registers (default: the library's)")
     args = ap.parse_args()
     global SPMV_STAGE
     SPMV_STAGE = args.spmv_stage

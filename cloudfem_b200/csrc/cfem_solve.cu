@@ -26,6 +26,7 @@
 // convergence norm.
 #include "cfem_common.cuh"
 
+#include <cub/device/device_scan.cuh>
 #include <cuda.h>
 #include <math.h>
 #include <string.h>
@@ -95,6 +96,16 @@ struct SysDev {
     const void *v3;
     // graph scheduler: rows per SpMV-phase work entry, and entry count
     int32_t xrows, nxe;
+    // bs 1, graph scheduler with the sliced-ELL SpMV (SpMV staging 3):
+    // work entries of SELL_ROWS rows sorted by length into slices of 32 rows,
+    // slot k of slice lane l at soff[slice] + 32 k + l (slot 0: the diagonal
+    // entry, or the row sum of the FP32 difference form); sperm: the entry's
+    // row (0..SELL_ROWS-1) at each sorted position
+    const int32_t *scol;
+    const void *sval;
+    const int64_t *soff;
+    const uint8_t *sperm;
+    int32_t sell;
 };
 
 struct SysState {
@@ -2042,6 +2053,195 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Sliced-ELL scalar SpMV (graph scheduler, A phase of scalar systems at SpMV
+// staging 3). A work entry is SELL_ROWS consecutive rows of one system,
+// sorted by length (longest first, ties in row order) and cut into slices
+// of 32 rows; a slice stores its rows' entries slot-major (slot k of all 32
+// rows, then slot k + 1), padded to its longest row with (own row, 0). One
+// lane owns one row: the column and value loads of a warp are two coalesced
+// 128-byte (FP32) lines per slot, read with no L1 allocation so that the
+// gathered p stays in L1, and a row needs no cross-lane reduction. Slot 0
+// holds the diagonal (FP64) or the FP32 difference form's row sum s_i, which
+// is applied to p_i; the other slots a_ij (p_j - p_i) in the difference form,
+// a_ij p_j otherwise (padding adds nothing either way). Sorting within
+// SELL_ROWS rows keeps the padding of Tet10 patterns near 3 % (slices of
+// unsorted rows: 14 %). The layout depends only on the system's pattern, so
+// sums are the same alone and in any batch.
+constexpr int SELL_ROWS = 256;
+constexpr int SELL_SLICES = SELL_ROWS / 32;
+constexpr int SELL_BLOCKS = 4;     // resident blocks of k_gxl per SM
+
+__device__ __forceinline__ int32_t ld_stream(const int32_t *p) {
+    int32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *p) {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double *p) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+// Sort each work entry's rows by stored length (the diagonal counted once
+// even when absent: it gets its own slot) and write the slice sizes
+// (32 x longest row, 0 for slices of padding rows only).
+__global__ void __launch_bounds__(SELL_ROWS)
+k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+            uint8_t *__restrict__ perm, int64_t *__restrict__ sizes) {
+    __shared__ int len[SELL_ROWS];
+    const int t = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
+    const int64_t row = r0 + t;
+    int L = 0;
+    if (row < n) {
+        const int32_t kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
+        bool diag = false;
+        for (int32_t k = kb; k < ke; ++k) diag |= __ldg(ci + k) == (int32_t)row;
+        L = ke - kb + (diag ? 0 : 1);
+    }
+    len[t] = L;
+    __syncthreads();
+    int rank = 0;
+    for (int u = 0; u < SELL_ROWS; ++u) {
+        const int Lu = len[u];
+        rank += (Lu > L || (Lu == L && u < t)) ? 1 : 0;
+    }
+    perm[r0 + rank] = (uint8_t)t;
+    if ((rank & 31) == 0) sizes[(int64_t)blockIdx.x * SELL_SLICES + (rank >> 5)] = 32 * (int64_t)L;
+}
+
+// Fill the slices from the CSR: position t of entry blockIdx.x (slice t/32,
+// lane t%32) holds row r0 + perm[t]: the diagonal first, then the other
+// entries in column order, then padding.
+template <typename T>
+__global__ void __launch_bounds__(SELL_ROWS)
+k_sell_fill(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+            const T *__restrict__ v, const uint8_t *__restrict__ perm,
+            const int64_t *__restrict__ soff, int32_t *__restrict__ scol, T *__restrict__ sval) {
+    const int t = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
+    const int64_t sl = (int64_t)blockIdx.x * SELL_SLICES + (t >> 5);
+    const int64_t base = soff[sl];
+    const int w = (int)((soff[sl + 1] - base) >> 5);
+    if (w == 0) return;
+    const int64_t row = r0 + perm[r0 + t];
+    const bool valid = row < n;
+    const int32_t kb = valid ? __ldg(rp + row) : 0, len = valid ? __ldg(rp + row + 1) - kb : 0;
+    int dpos = -1;
+    for (int k = 0; k < len; ++k)
+        if (__ldg(ci + kb + k) == (int32_t)row) { dpos = k; break; }
+    const int32_t own = valid ? (int32_t)row : (int32_t)r0;
+    int64_t o = base + (t & 31);
+    // slot 0: the diagonal (value 0 if the pattern has none)
+    scol[o] = own;
+    sval[o] = dpos >= 0 ? v[kb + dpos] : (T)0;
+    int k = 1;
+    for (int e = 0; e < len; ++e) {
+        if (e == dpos) continue;
+        o += 32;
+        scol[o] = __ldg(ci + kb + e);
+        sval[o] = v[kb + e];
+        ++k;
+    }
+    for (; k < w; ++k) {
+        o += 32;
+        scol[o] = own;
+        sval[o] = (T)0;
+    }
+}
+
+// q = A p and p.q over the rows of one work entry (A phase).
+template <typename T, bool DIFF>
+__device__ __forceinline__ void phase_A_sell(const SysDev &S, const SysState *st, int64_t ent,
+                                             int lane, double part[4]) {
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
+    T *q = (T *)S.q;
+    const int32_t *scol = S.scol;
+    const T *sval = (const T *)S.sval;
+    const int64_t r0 = ent * SELL_ROWS;
+    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    T pq = 0;
+    for (int s = 0; s < SELL_SLICES && s * 32 < nr; ++s) {
+        const int64_t sl = ent * SELL_SLICES + s;
+        const int64_t base = __ldg(S.soff + sl);
+        const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+        const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
+        const bool valid = rl < nr;
+        const int64_t row = r0 + rl;
+        const T pi = valid ? __ldg(pv + row) : (T)0;
+        const int32_t *cp = scol + base + lane;
+        const T *vp = sval + base + lane;
+        T acc = ld_stream(vp) * pi;
+        // U slots in flight per lane: their column and value loads first,
+        // then the gathers
+        constexpr int U = 8;
+        int k = 1;
+        for (; k + U <= w; k += U) {
+            int32_t c[U];
+            T a[U], g[U];
+#pragma unroll
+            for (int j = 0; j < U; ++j) c[j] = ld_stream(cp + 32 * (k + j));
+#pragma unroll
+            for (int j = 0; j < U; ++j) a[j] = ld_stream(vp + 32 * (k + j));
+#pragma unroll
+            for (int j = 0; j < U; ++j) g[j] = __ldg(pv + c[j]);
+#pragma unroll
+            for (int j = 0; j < U; ++j) acc += a[j] * (DIFF ? g[j] - pi : g[j]);
+        }
+        for (; k < w; ++k) {
+            const int32_t c = ld_stream(cp + 32 * k);
+            const T a = ld_stream(vp + 32 * k);
+            const T g = __ldg(pv + c);
+            acc += a * (DIFF ? g - pi : g);
+        }
+        if (valid) {
+            q[row] = acc;
+            pq += pi * acc;
+        }
+    }
+    part[0] += (double)pq;
+}
+
+// k_gx for scalar systems with the sliced-ELL A phase (work entries of
+// SELL_ROWS rows); R and ZERO phases on the same rows from the unit-padded
+// copy, as in k_gxs.
+template <typename T>
+__global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
+k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
+      const int2 *__restrict__ list, int n) {
+    pdl_wait();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * S.xrows;
+        const int64_t r1 = min(S.n, r0 + S.xrows);
+        if (ph == PH_A) {
+            phase_A_sell<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
+        } else if (ph == PH_R) {
+            int bad = 0;
+            phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+        } else {
+            phase_zero<1>(S, r0, r1, lane);
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
 constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
 constexpr int X_CHUNKS_VEC = 8;   // chunks per SpMV work entry, padded scalar rows
 static_assert(X_CHUNKS_VEC * 16 <= XR_MAX, "staged work entries hold at most XR_MAX rows");
@@ -2177,6 +2377,8 @@ struct cfem_pcg_plan {
     std::vector<cfem::SysDev> hs;
     char *ws_copy = nullptr;      // system table, lists, working matrix copies
     char *ws_state = nullptr;     // vectors, partials, states, barrier
+    char *ws_smeta = nullptr;     // sliced-ELL row orders and slice offsets
+    char *ws_sdata = nullptr;     // sliced-ELL columns and values
     size_t state_bytes = 0;
     cfem::SysDev *d_sys = nullptr;
     cfem::SysState *d_st = nullptr;
@@ -2222,12 +2424,82 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
                             s, S.nnzb, S.v64, (double *)S.vsoa);
         } else if (S.vec4) {
             const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
-            if (S.mode == CFEM_SOLVE_MIXED)
+            if (S.sell) {
+                if (S.mode == CFEM_SOLVE_MIXED)
+                    CFEM_LAUNCH(k_sell_fill<float>, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp,
+                                S.ci, S.v32, S.sperm, S.soff, (int32_t *)S.scol, (float *)S.sval);
+                else
+                    CFEM_LAUNCH(k_sell_fill<double>, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp,
+                                S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
+            } else if (S.mode == CFEM_SOLVE_MIXED)
                 CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
                             (int32_t *)S.ci4, (float *)S.va4);
             CFEM_LAUNCH(k_pad4<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
                         (int32_t *)S.ci4, (double *)S.va4d);
         }
+    }
+    return CFEM_OK;
+}
+
+// Sliced-ELL layout of every scalar system flagged `sell`: row orders and
+// slice offsets (k_sell_rank, then an exclusive scan of the slice sizes),
+// then room for the columns and values (filled by plan_copies).
+static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
+    size_t meta = 0;
+    int64_t max_sl = 0;
+    for (const SysDev &S : P->hs)
+        if (S.sell) {
+            const int64_t nsl = (int64_t)S.nxe * SELL_SLICES;
+            meta += align256((size_t)S.nxe * SELL_ROWS) + 2 * align256((nsl + 1) * 8);
+            max_sl = std::max(max_sl, nsl + 1);
+        }
+    if (!meta) return CFEM_OK;
+    size_t scan_bytes = 0;
+    CFEM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int64_t *)nullptr,
+                                            (int64_t *)nullptr, max_sl, s));
+    CFEM_TRY(tmp_alloc(&P->ws_smeta, meta, s));
+    char *scan_tmp = nullptr;
+    CFEM_TRY(tmp_alloc(&scan_tmp, scan_bytes, s));
+    size_t o = 0;
+    std::vector<int64_t> totals(P->hs.size(), 0);
+    std::vector<int64_t *> sizes_of(P->hs.size(), nullptr);
+    for (size_t i = 0; i < P->hs.size(); ++i) {
+        SysDev &S = P->hs[i];
+        if (!S.sell) continue;
+        const int64_t nsl = (int64_t)S.nxe * SELL_SLICES;
+        uint8_t *perm = (uint8_t *)(P->ws_smeta + o);
+        o += align256((size_t)S.nxe * SELL_ROWS);
+        int64_t *sizes = (int64_t *)(P->ws_smeta + o);
+        o += align256((nsl + 1) * 8);
+        int64_t *soff = (int64_t *)(P->ws_smeta + o);
+        o += align256((nsl + 1) * 8);
+        CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
+        CFEM_LAUNCH(k_sell_rank, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes);
+        CFEM_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, sizes, soff, nsl + 1, s));
+        CFEM_CUDA(cudaMemcpyAsync(&totals[i], soff + nsl, sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, s));
+        S.sperm = perm;
+        S.soff = soff;
+    }
+    tmp_free(scan_tmp, s);
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    size_t data = 0;
+    for (size_t i = 0; i < P->hs.size(); ++i) {
+        const SysDev &S = P->hs[i];
+        if (!S.sell) continue;
+        const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
+        data += align256((size_t)totals[i] * 4) + align256((size_t)totals[i] * ts);
+    }
+    CFEM_TRY(tmp_alloc(&P->ws_sdata, data, s));
+    o = 0;
+    for (size_t i = 0; i < P->hs.size(); ++i) {
+        SysDev &S = P->hs[i];
+        if (!S.sell) continue;
+        const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
+        S.scol = (const int32_t *)(P->ws_sdata + o);
+        o += align256((size_t)totals[i] * 4);
+        S.sval = P->ws_sdata + o;
+        o += align256((size_t)totals[i] * ts);
     }
     return CFEM_OK;
 }
@@ -2245,6 +2517,8 @@ static void plan_free(cfem_pcg_plan *P) {
     if (P->w) {
         if (P->ws_copy) cudaFreeAsync(P->ws_copy, P->w);
         if (P->ws_state) cudaFreeAsync(P->ws_state, P->w);
+        if (P->ws_smeta) cudaFreeAsync(P->ws_smeta, P->w);
+        if (P->ws_sdata) cudaFreeAsync(P->ws_sdata, P->w);
         cudaStreamSynchronize(P->w);
     }
     for (int i = 0; i < 4; ++i)
@@ -2359,13 +2633,14 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
     // systems a padded block copy (staged SpMV) or an entry-major copy.
     const bool stage3 = ctx->spmv_stage == 2;
+    const bool sell = ctx->spmv_stage == 3;   // sliced-ELL scalar SpMV
     if (!persistent)
         for (int i = 0; i < n_systems; ++i) {
             const size_t ts = (hs[i].mode == CFEM_SOLVE_MIXED) ? 4 : 8;
             if (hs[i].bs == 1) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 8) +
-                              (hs[i].mode == CFEM_SOLVE_MIXED ? align256(ne * 4) : 0);
+                              (hs[i].mode == CFEM_SOLVE_MIXED && !sell ? align256(ne * 4) : 0);
             } else if (stage3) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 9 * ts);
@@ -2413,15 +2688,17 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                 const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
                 S.ci4 = (const int32_t *)take_c(ne * 4);
                 S.va4d = (const double *)take_c(ne * 8);
-                S.va4 = (S.mode == CFEM_SOLVE_MIXED) ? take_c(ne * 4) : (const void *)S.va4d;
+                S.va4 = (S.mode == CFEM_SOLVE_MIXED) ? (sell ? nullptr : take_c(ne * 4))
+                                                     : (const void *)S.va4d;
                 S.vec4 = 1;
+                S.sell = sell ? 1 : 0;
             }
         }
         // Scalar rows from the padded copy: eight chunks per SpMV work entry,
         // so a warp's set-up (work entry, system, state) is paid per 128 rows
         // (measured 1.8x faster than one chunk on the batched heat meshes; 3x3
         // systems keep one chunk: fewer, longer warps measured slower there).
-        S.xrows = (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;
+        S.xrows = S.sell ? SELL_ROWS : (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;
         CFEM_CHECK(!S.c3 || S.xrows <= XR3, CFEM_ERR_UNSUPPORTED,
                    "staged 3x3 work entries hold at most %d block rows", XR3);
         S.nxe = (int32_t)((S.n + S.xrows - 1) / S.xrows);
@@ -2432,6 +2709,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     P->d_chunks = (int32_t *)take_c(n_chunks * sizeof(int32_t));
     int2 *d_lista = (int2 *)take_c(list_a * sizeof(int2));
     int2 *d_listb = (int2 *)take_c(list_b * sizeof(int2));
+    if (sell) CFEM_TRY(sell_layout(P, s));
     CFEM_TRY(plan_copies(P, s));
     CFEM_CUDA(cudaMemcpyAsync(P->d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
@@ -2490,9 +2768,9 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             }
         if (rows > 0 && nz <= 16.0 * rows) lpr[t] = 4;
     }
-    if (stage >= 1 && !la[0].empty())
+    if ((stage == 1 || stage == 2) && !la[0].empty())
         CFEM_TRY((lpr[0] == 4 ? gxs_prepare<double, 4>() : gxs_prepare<double, 8>()));
-    if (stage >= 1 && !la[2].empty())
+    if ((stage == 1 || stage == 2) && !la[2].empty())
         CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
     if (stage == 2 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
     if (stage == 2 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
@@ -2516,18 +2794,20 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
-            if (t == 0 && stage >= 1)
+            if (t == 0 && stage == 3) glaunch(p, k_gxl<double>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 3) glaunch(p, k_gxl<float>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 0 && (stage == 1 || stage == 2))
                 glaunch_smem(p, lpr[0] == 4 ? k_gxs<double, 4> : k_gxs<double, 8>, g, 32 * GROUP, gxs_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 2 && stage >= 1)
+            if (t == 2 && (stage == 1 || stage == 2))
                 glaunch_smem(p, lpr[2] == 4 ? k_gxs<float, 4> : k_gxs<float, 8>, g, 32 * GROUP, gxs_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage == 2)
                 glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage < 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage != 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage == 2)
                 glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage < 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage != 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
         if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));

@@ -1,6 +1,8 @@
 """SpMV of the graph scheduler with the matrix streamed through
 shared-memory windows by 1-D bulk copies (staging 1: scalar rows; 2: also
-3x3 blocks) against the register path (staging 0) and a direct FP64 solve:
+3x3 blocks) or in the sliced-ELL layout (staging 3: scalar rows, one row
+per lane, slices of 32 length-sorted rows) against the register path
+(staging 0) and a direct FP64 solve:
 the same answers, bitwise batch independence, rows longer than a window,
 short (P1-like, 4 lanes per row) and long (8 lanes) rows, 3x3 rows that
 straddle windows, and CSR arrays that do not start on a 16-byte
@@ -119,22 +121,23 @@ def test_staged_spmv_matches_direct_solve(torch, mode):
         ref = spla.spsolve(A.tocsc(), b)
         sys_ = _system(torch, rt, A, b, offset)
         xs = {}
-        for stage in (0, 1):
+        for stage in (0, 1, 3):
             _, (x,) = _solve(rt, [sys_], md, rtol, stage)
             err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
             assert err <= tol, (offset, stage, err)
             xs[stage] = x
-        d = np.linalg.norm(xs[1] - xs[0]) / np.linalg.norm(xs[0])
-        assert d <= tol, (offset, d)
+        for stage in (1, 3):
+            d = np.linalg.norm(xs[stage] - xs[0]) / np.linalg.norm(xs[0])
+            assert d <= tol, (offset, stage, d)
 
 
+@pytest.mark.parametrize("stage", [1, 3])
 @pytest.mark.parametrize("rows", ["long", "short"])
-def test_staged_spmv_batch_equals_solo_bitwise(torch, rows):
-    """On the graph scheduler with staged SpMV, each system's answer is
-    bitwise the same alone, in a batch, and on a repeat, with 8 lanes per
-    row (mean row above 16 entries) and with 4."""
+def test_staged_spmv_batch_equals_solo_bitwise(torch, rows, stage):
+    """On the graph scheduler with staged (1) or sliced-ELL (3) SpMV, each
+    system's answer is bitwise the same alone, in a batch, and on a repeat,
+    with 8 lanes per row (mean row above 16 entries) and with 4."""
     from cloudfem_b200 import _native as N
-    stage = 1
     rt = N.runtime()
     if rows == "long":
         mats = [_dense_band(n, 14, seed=n) for n in (2500, 1800, 4100)]
