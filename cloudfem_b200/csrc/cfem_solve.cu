@@ -2071,6 +2071,9 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
 constexpr int SELL_ROWS = 256;
 constexpr int SELL_SLICES = SELL_ROWS / 32;
 constexpr int SELL_BLOCKS = 4;     // resident blocks of k_gxl per SM
+__host__ __device__ inline int64_t sell_windows(int64_t n) {
+    return (n + SELL_ROWS - 1) / SELL_ROWS;
+}
 
 __device__ __forceinline__ int32_t ld_stream(const int32_t *p) {
     int32_t v;
@@ -2156,20 +2159,128 @@ k_sell_fill(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
     }
 }
 
-// q = A p and p.q over the rows of one work entry (A phase).
+// 3x3 blocks: as k_sell_fill, with the slot's 9 values (row-major block)
+// in 9 planes of 32 lanes: value e of slot k of a slice at
+// 9 soff[slice] + (9 k + e) 32 + lane.
+template <typename T>
+__global__ void __launch_bounds__(SELL_ROWS)
+k_sell_fill3(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+             const T *__restrict__ v, const uint8_t *__restrict__ perm,
+             const int64_t *__restrict__ soff, int32_t *__restrict__ scol, T *__restrict__ sval) {
+    const int t = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
+    const int64_t sl = (int64_t)blockIdx.x * SELL_SLICES + (t >> 5);
+    const int64_t base = soff[sl];
+    const int w = (int)((soff[sl + 1] - base) >> 5);
+    if (w == 0) return;
+    const int64_t row = r0 + perm[r0 + t];
+    const bool valid = row < n;
+    const int32_t kb = valid ? __ldg(rp + row) : 0, len = valid ? __ldg(rp + row + 1) - kb : 0;
+    int dpos = -1;
+    for (int k = 0; k < len; ++k)
+        if (__ldg(ci + kb + k) == (int32_t)row) { dpos = k; break; }
+    const int32_t own = valid ? (int32_t)row : (int32_t)r0;
+    const int lane = t & 31;
+    T *vb = sval + 9 * base + lane;
+    auto put = [&](int k, int32_t c, int64_t src) {
+        scol[base + 32 * k + lane] = c;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) vb[(int64_t)(9 * k + e) * 32] = src >= 0 ? v[src * 9 + e] : (T)0;
+    };
+    put(0, own, dpos >= 0 ? (int64_t)kb + dpos : -1);
+    int k = 1;
+    for (int e = 0; e < len; ++e) {
+        if (e == dpos) continue;
+        put(k++, __ldg(ci + kb + e), (int64_t)kb + e);
+    }
+    for (; k < w; ++k) put(k, own, -1);
+}
+
+// q = A p and p.q over the 32 block rows of slice sl of a 3x3 system (A
+// phase), one block row per lane. As the register path does, the new
+// direction p = zeta z + beta p_old is formed at every gathered block and
+// written for the lane's own row (3x3 systems have no separate direction
+// launch). DIFF: slot 0 holds the FP32 block row sum S_i, applied to p_i,
+// the other slots A_ij (p_j - p_i).
 template <typename T, bool DIFF>
-__device__ __forceinline__ void phase_A_sell(const SysDev &S, const SysState *st, int64_t ent,
+__device__ __forceinline__ void phase_A_sell3(const SysDev &S, const SysState *st, int64_t sl,
+                                              int lane, double part[4]) {
+    const T beta = (T)vcg(&st->beta);
+    const T zeta = (T)vcg(&st->zeta);
+    const int pbuf = vcgi(&st->pbuf);
+    const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
+    T *pout = (T *)(pbuf ? S.p0 : S.p1);
+    const T *z = (const T *)S.z;
+    T *q = (T *)S.q;
+    const int64_t r0 = (sl / SELL_SLICES) * SELL_ROWS;
+    const int s = (int)(sl % SELL_SLICES);
+    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    T pq = 0;
+    if (s * 32 < nr) {
+        const int64_t base = __ldg(S.soff + sl);
+        const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+        const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
+        const bool valid = rl < nr;
+        const int64_t row = valid ? r0 + rl : r0;
+        T pi[3], acc[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pi[c] = zeta * __ldg(z + row * 3 + c) + beta * __ldg(pin + row * 3 + c);
+            acc[c] = 0;
+        }
+        const int32_t *cp = S.scol + base + lane;
+        const T *vp = (const T *)S.sval + 9 * base + lane;
+        {   // slot 0: the diagonal block (FP32: the block row sum)
+            T a[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a[e] = ld_stream(vp + 32 * e);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[c] += a[c * 3 + d] * pi[d];
+        }
+        for (int k = 1; k < w; ++k) {
+            const int64_t j = ld_stream(cp + 32 * k);
+            T a[9], pj[3];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a[e] = ld_stream(vp + 32 * (9 * k + e));
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pj[d] = zeta * __ldg(z + j * 3 + d) + beta * __ldg(pin + j * 3 + d);
+                if (DIFF) pj[d] -= pi[d];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[c] += a[c * 3 + d] * pj[d];
+        }
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int64_t i = row * 3 + c;
+                pout[i] = pi[c];
+                q[i] = acc[c];
+                pq += pi[c] * acc[c];
+            }
+        }
+    }
+    part[0] += (double)pq;
+}
+
+// q = A p and p.q over the 32 rows of slice sl (A phase).
+template <typename T, bool DIFF>
+__device__ __forceinline__ void phase_A_sell(const SysDev &S, const SysState *st, int64_t sl,
                                              int lane, double part[4]) {
     const int pbuf = vcgi(&st->pbuf);
     const T *pv = (const T *)(pbuf ? S.p0 : S.p1);   // this iteration's p (k_gp)
     T *q = (T *)S.q;
     const int32_t *scol = S.scol;
     const T *sval = (const T *)S.sval;
-    const int64_t r0 = ent * SELL_ROWS;
+    const int64_t r0 = (sl / SELL_SLICES) * SELL_ROWS;   // the slice's window
+    const int s = (int)(sl % SELL_SLICES);
     const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
     T pq = 0;
-    for (int s = 0; s < SELL_SLICES && s * 32 < nr; ++s) {
-        const int64_t sl = ent * SELL_SLICES + s;
+    if (s * 32 < nr) {
         const int64_t base = __ldg(S.soff + sl);
         const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
         const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
@@ -2209,9 +2320,10 @@ __device__ __forceinline__ void phase_A_sell(const SysDev &S, const SysState *st
     part[0] += (double)pq;
 }
 
-// k_gx for scalar systems with the sliced-ELL A phase (work entries of
-// SELL_ROWS rows); R and ZERO phases on the same rows from the unit-padded
-// copy, as in k_gxs.
+// k_gx for scalar systems with the sliced-ELL A phase: one slice of 32
+// rows per warp (work entries of 32 rows, so the GROUP warps of a block
+// cover one window of SELL_ROWS rows); R and ZERO phases on the entry's rows
+// from the unit-padded copy, as in k_gxs.
 template <typename T>
 __global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
 k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
@@ -2242,9 +2354,43 @@ k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
+// k_gx for 3x3 systems with the sliced-ELL A phase (one block row per
+// lane, one slice per warp); R and ZERO phases on the entry's block rows
+// as in k_gx.
+template <typename T>
+__global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
+k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
+       const int2 *__restrict__ list, int n) {
+    pdl_wait();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
+        const int64_t r0 = (int64_t)e.y * S.xrows;
+        const int64_t r1 = min(S.n, r0 + S.xrows);
+        if (ph == PH_A) {
+            phase_A_sell3<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
+        } else if (ph == PH_R) {
+            int bad = 0;
+            phase_R<T, 3, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+        } else {
+            phase_zero<3>(S, r0, r1, lane);
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
 constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
 constexpr int X_CHUNKS_VEC = 8;   // chunks per SpMV work entry, padded scalar rows
 static_assert(X_CHUNKS_VEC * 16 <= XR_MAX, "staged work entries hold at most XR_MAX rows");
+static_assert(SELL_SLICES == GROUP, "a block of k_gxl covers one sliced-ELL window");
 
 // Start of a graph-scheduled solve: every system active, no barrier error.
 __global__ void k_plan_start(GridBar *bar, int n_systems) {
@@ -2407,7 +2553,14 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
     for (int i = 0; i < P->n_systems; ++i) {
         SysDev &S = P->hs[i];
-        if (S.bs == 3 && S.c3) {
+        if (S.bs == 3 && S.sell) {
+            if (S.mode == CFEM_SOLVE_MIXED)
+                CFEM_LAUNCH(k_sell_fill3<float>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n,
+                            S.rp, S.ci, S.v32, S.sperm, S.soff, (int32_t *)S.scol, (float *)S.sval);
+            else
+                CFEM_LAUNCH(k_sell_fill3<double>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n,
+                            S.rp, S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
+        } else if (S.bs == 3 && S.c3) {
             const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
             if (S.mode == CFEM_SOLVE_MIXED)
                 CFEM_LAUNCH(k_pad3<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
@@ -2426,10 +2579,10 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
             const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
             if (S.sell) {
                 if (S.mode == CFEM_SOLVE_MIXED)
-                    CFEM_LAUNCH(k_sell_fill<float>, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp,
+                    CFEM_LAUNCH(k_sell_fill<float>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n, S.rp,
                                 S.ci, S.v32, S.sperm, S.soff, (int32_t *)S.scol, (float *)S.sval);
                 else
-                    CFEM_LAUNCH(k_sell_fill<double>, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp,
+                    CFEM_LAUNCH(k_sell_fill<double>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n, S.rp,
                                 S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
             } else if (S.mode == CFEM_SOLVE_MIXED)
                 CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
@@ -2449,8 +2602,8 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     int64_t max_sl = 0;
     for (const SysDev &S : P->hs)
         if (S.sell) {
-            const int64_t nsl = (int64_t)S.nxe * SELL_SLICES;
-            meta += align256((size_t)S.nxe * SELL_ROWS) + 2 * align256((nsl + 1) * 8);
+            const int64_t nsl = sell_windows(S.n) * SELL_SLICES;
+            meta += align256((size_t)nsl * 32) + 2 * align256((nsl + 1) * 8);
             max_sl = std::max(max_sl, nsl + 1);
         }
     if (!meta) return CFEM_OK;
@@ -2466,15 +2619,15 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     for (size_t i = 0; i < P->hs.size(); ++i) {
         SysDev &S = P->hs[i];
         if (!S.sell) continue;
-        const int64_t nsl = (int64_t)S.nxe * SELL_SLICES;
+        const int64_t nw = sell_windows(S.n), nsl = nw * SELL_SLICES;
         uint8_t *perm = (uint8_t *)(P->ws_smeta + o);
-        o += align256((size_t)S.nxe * SELL_ROWS);
+        o += align256((size_t)nsl * 32);
         int64_t *sizes = (int64_t *)(P->ws_smeta + o);
         o += align256((nsl + 1) * 8);
         int64_t *soff = (int64_t *)(P->ws_smeta + o);
         o += align256((nsl + 1) * 8);
         CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
-        CFEM_LAUNCH(k_sell_rank, (unsigned)S.nxe, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes);
+        CFEM_LAUNCH(k_sell_rank, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes);
         CFEM_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, sizes, soff, nsl + 1, s));
         CFEM_CUDA(cudaMemcpyAsync(&totals[i], soff + nsl, sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, s));
@@ -2488,7 +2641,7 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
         const SysDev &S = P->hs[i];
         if (!S.sell) continue;
         const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
-        data += align256((size_t)totals[i] * 4) + align256((size_t)totals[i] * ts);
+        data += align256((size_t)totals[i] * 4) + align256((size_t)totals[i] * S.bs * S.bs * ts);
     }
     CFEM_TRY(tmp_alloc(&P->ws_sdata, data, s));
     o = 0;
@@ -2499,7 +2652,7 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
         S.scol = (const int32_t *)(P->ws_sdata + o);
         o += align256((size_t)totals[i] * 4);
         S.sval = P->ws_sdata + o;
-        o += align256((size_t)totals[i] * ts);
+        o += align256((size_t)totals[i] * S.bs * S.bs * ts);
     }
     return CFEM_OK;
 }
@@ -2644,6 +2797,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             } else if (stage3) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 9 * ts);
+            } else if (sell) {
+                // sliced-ELL copy allocated by sell_layout
             } else {
                 copy_bytes += align256((size_t)hs[i].nnzb * 9 * ts);
             }
@@ -2679,6 +2834,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                 const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
                 S.c3 = (const int32_t *)take_c(ne * 4);
                 S.v3 = take_c(ne * 9 * ts);
+            } else if (!persistent && sell) {
+                S.sell = 1;
             } else if (!persistent) {
                 S.vsoa = take_c((size_t)S.nnzb * 9 * ts);
             }
@@ -2698,7 +2855,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         // so a warp's set-up (work entry, system, state) is paid per 128 rows
         // (measured 1.8x faster than one chunk on the batched heat meshes; 3x3
         // systems keep one chunk: fewer, longer warps measured slower there).
-        S.xrows = S.sell ? SELL_ROWS : (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;
+        S.xrows = S.sell ? 32 : (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;   // 32: one slice
         CFEM_CHECK(!S.c3 || S.xrows <= XR3, CFEM_ERR_UNSUPPORTED,
                    "staged 3x3 work entries hold at most %d block rows", XR3);
         S.nxe = (int32_t)((S.n + S.xrows - 1) / S.xrows);
@@ -2803,11 +2960,13 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage == 2)
                 glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage != 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 3) glaunch(p, k_gxl3<double>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage < 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage == 2)
                 glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage != 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 3) glaunch(p, k_gxl3<float>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage < 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }
         if (t1) CFEM_CUDA(cudaEventRecordWithFlags(t1, cs, cudaEventRecordExternal));

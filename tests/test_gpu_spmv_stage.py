@@ -174,34 +174,37 @@ def _elastic_system(torch, nx, ny, nz, seed):
                            vals, rhs, x, mask)
 
 
+@pytest.mark.parametrize("stage", [2, 3])
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
-def test_staged_3x3_spmv_matches_register_path(torch, mode):
+def test_staged_3x3_spmv_matches_register_path(torch, mode, stage):
     """3x3-block systems on the graph scheduler: the staged SpMV (staging
-    2: rows that straddle windows, 65-block vertex rows) and the register
-    path reach the same answer, and the staged one repeats bitwise."""
+    2: rows that straddle windows, 65-block vertex rows) or the sliced-ELL
+    one (staging 3: one block row per lane) and the register path reach the
+    same answer, and the other path repeats bitwise."""
     from cloudfem_b200 import _native as N
     dm, sysm = _elastic_system(torch, 10, 3, 3, seed=1)
     rt = dm.rt
     md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
     rtol = 1e-11 if mode == "fp64" else 1e-10
     _, (x0,) = _solve(rt, [sysm], md, rtol, 0)
-    r1, (x1,) = _solve(rt, [sysm], md, rtol, 2)
-    _, (x1b,) = _solve(rt, [sysm], md, rtol, 2)
+    r1, (x1,) = _solve(rt, [sysm], md, rtol, stage)
+    _, (x1b,) = _solve(rt, [sysm], md, rtol, stage)
     d = np.linalg.norm(x1 - x0) / np.linalg.norm(x0)
     assert d <= (1e-8 if mode == "fp64" else 1e-7), d
     assert np.array_equal(x1, x1b)
 
 
-def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch):
+@pytest.mark.parametrize("stage", [2, 3])
+def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage):
     """Each 3x3 system's answer is bitwise the same alone and in a batch
-    with the staged SpMV, in both precisions."""
+    with the staged or sliced-ELL SpMV, in both precisions."""
     from cloudfem_b200 import _native as N
     built = [_elastic_system(torch, nx, 3, 3, seed=nx) for nx in (6, 9, 4)]
     rt = built[0][0].rt
     systems = [s for _, s in built]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, 2)
+        rb, xb = _solve(rt, systems, md, 1e-10, stage)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, 2)
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
