@@ -53,6 +53,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 SPMV_STAGE = None   # --spmv-stage: None keeps the library default
+SELL_SORT = None    # --sell-sort: None keeps the library default
 
 
 def _set_scheduler(rt, name):
@@ -65,6 +66,8 @@ def _set_scheduler(rt, name):
     N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, code))
     if SPMV_STAGE is not None:
         rt.set_param(N.PARAM_SPMV_STAGE, SPMV_STAGE)
+    if SELL_SORT is not None:
+        rt.set_param(N.PARAM_SELL_SORT, SELL_SORT)
 
 
 def _scalar_spmv_kernel(rt):
@@ -327,7 +330,6 @@ def run_ours(args, rank, world, local_rank):
     h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
     d2h = 3 * mesh.n_nodes * 8
     value = world * free * args.steps / (ms * 1e-3)
-    plain_rate = world * free / plain_s
     out = {
         "metric": METRIC,
         "value": value,
@@ -1215,9 +1217,13 @@ def main():
                          "blocks in registers; 2 both staged; 0 both in registers; 3 "
                          "scalar rows in the sliced-ELL layout (one row per lane), 3x3 "
                          "blocks in registers (default: the library's)")
+    ap.add_argument("--sell-sort", type=int, default=None, choices=[0, 1],
+                    help="sliced-ELL SpMV: 1 sort each 256-row window by row length, "
+                         "0 keep rows in order (default: the library's)")
     args = ap.parse_args()
-    global SPMV_STAGE
+    global SPMV_STAGE, SELL_SORT
     SPMV_STAGE = args.spmv_stage
+    SELL_SORT = args.sell_sort
     if args.precision is None:
         args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -76,6 +76,7 @@ struct cfem_ctx {
     int graph_iters = 2;               // iterations per solve-loop body
     int pdl = 1;                       // dependent launches in solve graphs
     int spmv_stage = 1;                // SpMV: 0 registers, 1 staged scalar rows, 2 also 3x3
+    int sell_sort = 1;                 // sliced ELL: sort rows by length per window
     int barrier_timeout_us = 4000000;  // persistent grid-barrier wait limit
     int barrier_hold = 0;              // phantom barrier arrivals (fault injection)
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler

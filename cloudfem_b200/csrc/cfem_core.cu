@@ -236,6 +236,11 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
                        "SpMV staging must be 0, 1, 2 or 3 (got %d)", value);
             ctx->spmv_stage = value;
             return CFEM_OK;
+        case CFEM_PARAM_SELL_SORT:
+            CFEM_CHECK(value == 0 || value == 1, CFEM_ERR_INVALID,
+                       "sliced-ELL row sorting must be 0 or 1 (got %d)", value);
+            ctx->sell_sort = value;
+            return CFEM_OK;
         case CFEM_PARAM_BARRIER_TIMEOUT_US:
             CFEM_CHECK(value >= 1 && value <= 60000000, CFEM_ERR_INVALID,
                        "grid-barrier wait limit must be 1 us .. 60 s (got %d us)", value);
@@ -259,6 +264,7 @@ int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
         case CFEM_PARAM_GRAPH_ITERS: return ctx->graph_iters;
         case CFEM_PARAM_PDL: return ctx->pdl;
         case CFEM_PARAM_SPMV_STAGE: return ctx->spmv_stage;
+        case CFEM_PARAM_SELL_SORT: return ctx->sell_sort;
         case CFEM_PARAM_BARRIER_TIMEOUT_US: return ctx->barrier_timeout_us;
         case CFEM_PARAM_BARRIER_HOLD: return ctx->barrier_hold;
         default: return -1;

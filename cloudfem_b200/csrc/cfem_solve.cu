@@ -439,12 +439,43 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
 
 // ------------------------------------------------------- phase R / INIT
 // True residual in FP64; INIT also forms ||b_lift|| and the Jacobi inverse.
+// Compensated (double-double) sums for the FP64 true residual: hi + lo
+// carries sum_j a_j x_j with the rounding error of every product (exact by
+// FMA) and of every addition (TwoSum), so r = b - A x is accurate to about
+// eps |r| rather than eps |A||x| and the solver can certify (and reach) a
+// residual at the level a direct solver's answer has. The _rn intrinsics
+// keep the compiler from contracting the error terms away.
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double h2, double l2) {
+    const double s = __dadd_rn(hi, h2);
+    const double bp = __dsub_rn(s, hi);
+    const double e = __dadd_rn(__dsub_rn(hi, __dsub_rn(s, bp)), __dsub_rn(h2, bp));
+    hi = s;
+    lo = __dadd_rn(lo, __dadd_rn(e, l2));
+}
+__device__ __forceinline__ void dd_fma(double &hi, double &lo, double a, double x) {
+    const double p = __dmul_rn(a, x);
+    dd_add(hi, lo, p, fma(a, x, -p));
+}
+template <int L>
+__device__ __forceinline__ void group_sum_dd(double &hi, double &lo) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) {
+        const double h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        const double l2 = __shfl_xor_sync(0xffffffffu, lo, o);
+        dd_add(hi, lo, h2, l2);
+    }
+}
+// b - (hi + lo), rounded once at the end
+__device__ __forceinline__ double dd_residual(double b, double hi, double lo) {
+    return __dsub_rn(__dsub_rn(b, hi), lo);
+}
+
 template <bool INIT, int BS>
 __device__ __forceinline__ void acc_R(const double *__restrict__ v,
                                       const int32_t *__restrict__ ci, int32_t k,
                                       int64_t row, const double *x,
                                       const uint8_t *fixed, double acc[BS],
-                                      double aab[BS], double accf[BS],
+                                      double alo[BS], double aab[BS], double accf[BS],
                                       double dg[BS * BS]) {
     const int64_t j = __ldg(ci + k);
     const double *vk = v + (int64_t)k * BS * BS;
@@ -461,7 +492,7 @@ __device__ __forceinline__ void acc_R(const double *__restrict__ v,
         for (int d = 0; d < BS; ++d) {
             const double a = __ldg(vk + c * BS + d);
             const double ax = a * xj[d];
-            acc[c] += ax;
+            dd_fma(acc[c], alo[c], a, xj[d]);
             aab[c] += fabs(ax);
             if (INIT && fj[d]) accf[c] += ax;
             if (INIT && j == row) dg[c * BS + d] = a;
@@ -481,19 +512,19 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
     for (int64_t base = r0; base < r1; base += RPP) {
         const int64_t row = base + grp;
         const bool valid = row < r1;
-        double acc[BS], accf[BS], aab[BS], dg[BS * BS];
+        double acc[BS], alo[BS], accf[BS], aab[BS], dg[BS * BS];
 #pragma unroll
-        for (int c = 0; c < BS; ++c) acc[c] = accf[c] = aab[c] = 0.0;
+        for (int c = 0; c < BS; ++c) acc[c] = alo[c] = accf[c] = aab[c] = 0.0;
 #pragma unroll
         for (int c = 0; c < BS * BS; ++c) dg[c] = 0.0;
         if (valid) {
             const int32_t k1 = __ldg(S.rp + row + 1);
             for (int32_t k = __ldg(S.rp + row) + sub; k < k1; k += LANES)
-                acc_R<INIT, BS>(S.v64, S.ci, k, row, S.x, S.fixed, acc, aab, accf, dg);
+                acc_R<INIT, BS>(S.v64, S.ci, k, row, S.x, S.fixed, acc, alo, aab, accf, dg);
         }
 #pragma unroll
         for (int c = 0; c < BS; ++c) {
-            acc[c] = group_sum<LANES>(acc[c]);
+            group_sum_dd<LANES>(acc[c], alo[c]);
             aab[c] = group_sum<LANES>(aab[c]);
             if (INIT) accf[c] = group_sum<LANES>(accf[c]);
         }
@@ -509,7 +540,7 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
                 const int64_t i = row * BS + c;
                 fx[c] = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
                 const double bi = __ldg(S.b + i);
-                const double rt = fx[c] ? 0.0 : bi - acc[c];
+                const double rt = fx[c] ? 0.0 : dd_residual(bi, acc[c], alo[c]);
                 if (INIT && !fx[c]) {
                     const double bl = bi - accf[c];
                     bb += bl * bl;
@@ -586,7 +617,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
     for (int64_t base = r0; base < r1; base += 4 * H) {
         int64_t row[H], u[H], u0[H], uend[H], len[H];
         bool valid[H];
-        double acc[H], aab[H], accf[H], dg[H];
+        double acc[H], alo[H], aab[H], accf[H], dg[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             row[h] = base + grp + 4 * h;
@@ -598,7 +629,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
             u0[h] = (kb + 3 * rr_ + 3) >> 2;
             u[h] = u0[h] + sub;
             uend[h] = u0[h] + ((len[h] + 3) >> 2);
-            acc[h] = aab[h] = accf[h] = dg[h] = 0.0;
+            acc[h] = alo[h] = aab[h] = accf[h] = dg[h] = 0.0;
         }
         while (true) {
             bool more = false;
@@ -624,7 +655,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const double ax = a[e] * xj[e];
-                        acc[h] += ax;
+                        dd_fma(acc[h], alo[h], a[e], xj[e]);
                         aab[h] += fabs(ax);
                         if (INIT && fj[e]) accf[h] += ax;
                         if (INIT && c[e] == row[h] && pos + e < len[h]) dg[h] = a[e];
@@ -635,7 +666,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
         }
 #pragma unroll
         for (int h = 0; h < H; ++h) {
-            acc[h] = group_sum<8>(acc[h]);
+            group_sum_dd<8>(acc[h], alo[h]);
             aab[h] = group_sum<8>(aab[h]);
             if (INIT) {
                 accf[h] = group_sum<8>(accf[h]);
@@ -645,7 +676,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
                 const int64_t i = row[h];
                 const bool fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
                 const double bi = __ldg(S.b + i);
-                const double rt = fx ? 0.0 : bi - acc[h];
+                const double rt = fx ? 0.0 : dd_residual(bi, acc[h], alo[h]);
                 if (INIT && !fx) {
                     const double bl = bi - accf[h];
                     bb += bl * bl;
@@ -680,6 +711,16 @@ template <int BS>
 __device__ void phase_zero(const SysDev &S, int64_t r0, int64_t r1, int lane) {
     for (int64_t i = r0 * BS + lane; i < r1 * BS; i += 32)
         if (!(S.fixed && __ldg(S.fixed + i))) S.x[i] = 0.0;
+}
+
+// The true-residual phase of the graph scheduler's SpMV-phase kernels.
+template <typename T, int BS>
+__device__ __forceinline__ void run_R(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
+                                   int lane, double part[4], int *bad) {
+    if (BS == 1 && S.vec4)
+        phase_R_vec1<T, false>(S, st, r0, r1, lane, part, bad);
+    else
+        phase_R<T, BS, false>(S, st, r0, r1, lane, part, bad);
 }
 
 // State transition of a system once all its chunk sums are in.
@@ -1836,10 +1877,7 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
                 phase_A_lean<T, BS, sizeof(T) == 4>(S, &st[e.x], r0, r1, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
-            if (BS == 1 && S.vec4)
-                phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
-            else
-                phase_R<T, BS, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            run_R<T, BS>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<BS>(S, r0, r1, lane);
         }
@@ -1893,7 +1931,7 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
             if (fail && lane == 0) atomicExch(&bar->err, 2);
         } else if (ph == PH_R) {
             int bad = 0;
-            phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            run_R<T, 1>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<1>(S, r0, r1, lane);
         }
@@ -1940,7 +1978,7 @@ k_gxs3(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
             if (fail && lane == 0) atomicExch(&bar->err, 2);
         } else if (ph == PH_R) {
             int bad = 0;
-            phase_R<T, 3, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            run_R<T, 3>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<3>(S, r0, r1, lane);
         }
@@ -2096,7 +2134,7 @@ __device__ __forceinline__ double ld_stream(const double *p) {
 // (32 x longest row, 0 for slices of padding rows only).
 __global__ void __launch_bounds__(SELL_ROWS)
 k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
-            uint8_t *__restrict__ perm, int64_t *__restrict__ sizes) {
+            uint8_t *__restrict__ perm, int64_t *__restrict__ sizes, int sort) {
     __shared__ int len[SELL_ROWS];
     const int t = threadIdx.x;
     const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
@@ -2107,6 +2145,12 @@ k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         bool diag = false;
         for (int32_t k = kb; k < ke; ++k) diag |= __ldg(ci + k) == (int32_t)row;
         L = ke - kb + (diag ? 0 : 1);
+    }
+    if (!sort) {   // rows in their own order: a slice is 32 consecutive rows
+        perm[r0 + t] = (uint8_t)t;
+        const int m = __reduce_max_sync(0xffffffffu, L);
+        if ((t & 31) == 0) sizes[(int64_t)blockIdx.x * SELL_SLICES + (t >> 5)] = 32 * (int64_t)m;
+        return;
     }
     len[t] = L;
     __syncthreads();
@@ -2346,7 +2390,7 @@ k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
             phase_A_sell<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
-            phase_R_vec1<T, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            run_R<T, 1>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<1>(S, r0, r1, lane);
         }
@@ -2379,7 +2423,7 @@ k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
             phase_A_sell3<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
-            phase_R<T, 3, false>(S, &st[e.x], r0, r1, lane, part, &bad);
+            run_R<T, 3>(S, &st[e.x], r0, r1, lane, part, &bad);
         } else {
             phase_zero<3>(S, r0, r1, lane);
         }
@@ -2627,7 +2671,8 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
         int64_t *soff = (int64_t *)(P->ws_smeta + o);
         o += align256((nsl + 1) * 8);
         CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
-        CFEM_LAUNCH(k_sell_rank, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes);
+        CFEM_LAUNCH(k_sell_rank, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes,
+                    P->ctx->sell_sort);
         CFEM_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, sizes, soff, nsl + 1, s));
         CFEM_CUDA(cudaMemcpyAsync(&totals[i], soff + nsl, sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, s));

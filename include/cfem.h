@@ -177,18 +177,24 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * streams each scalar work entry's span through two shared-memory windows
  * of about 4 KB per warp with 1-D bulk copies (TMA) and loads 3x3 blocks
  * into registers, 2 streams 3x3 blocks through shared memory too (slower on
- * the elasticity beam: kept for tuning), 0 loads both into registers.
+ * the elasticity beam: kept for tuning), 0 loads both into registers, 3
+ * stores scalar rows and 3x3 block rows in the sliced-ELL layout (windows of
+ * 256 rows cut into slices of 32, one row per lane, coalesced slot-major
+ * loads, no cross-lane sums).
  * BARRIER_TIMEOUT_US: how long (microseconds, 1 .. 60e6; default 4e6) a
  * block of the persistent scheduler waits at its grid barrier before it
  * gives up; the solve then ends with CFEM_ERR_TIMEOUT and the context stays
  * usable. BARRIER_HOLD: fault injection for that path (0 default, or 1):
  * the barrier counts one phantom block that never arrives, so every wait
  * runs to the limit; no other waits of the library are affected. Both are
- * read when a solve plan is created. get returns -1 for an unknown
- * parameter. */
+ * read when a solve plan is created. SELL_SORT (SpMV staging 3): 1
+ * (default) sorts each window of 256 rows by length before cutting it into
+ * slices of 32 (less padding), 0 keeps the rows in order (neighbouring
+ * rows in a slice: gathers of p that share cache lines). get returns -1 for
+ * an unknown parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5, CFEM_PARAM_BARRIER_TIMEOUT_US = 6,
-       CFEM_PARAM_BARRIER_HOLD = 7 };
+       CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */

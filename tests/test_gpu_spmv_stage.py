@@ -83,18 +83,20 @@ def _system(torch, rt, A, b, offset):
     return s
 
 
-def _solve(rt, systems, mode, rtol, stage):
+def _solve(rt, systems, mode, rtol, stage, sort=1):
     from cloudfem_b200 import _native as N
     from cloudfem_b200.device import pcg
     N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_GRAPH))
     before = rt.get_param(N.PARAM_SPMV_STAGE)
     try:
         rt.set_param(N.PARAM_SPMV_STAGE, stage)
+        rt.set_param(N.PARAM_SELL_SORT, sort)
         for s in systems:
             s.x.zero_()
         res = pcg(systems, mode, rtol, 20000)
     finally:
         rt.set_param(N.PARAM_SPMV_STAGE, before)
+        rt.set_param(N.PARAM_SELL_SORT, 1)
         N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
     for r in res:
         assert r.status == N.CFEM_OK, r
@@ -121,10 +123,10 @@ def test_staged_spmv_matches_direct_solve(torch, mode):
         ref = spla.spsolve(A.tocsc(), b)
         sys_ = _system(torch, rt, A, b, offset)
         xs = {}
-        for stage in (0, 1, 3):
-            _, (x,) = _solve(rt, [sys_], md, rtol, stage)
+        for stage, sort in ((0, 1), (1, 1), (3, 1), (3, 0)):
+            _, (x,) = _solve(rt, [sys_], md, rtol, stage, sort)
             err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
-            assert err <= tol, (offset, stage, err)
+            assert err <= tol, (offset, stage, sort, err)
             xs[stage] = x
         for stage in (1, 3):
             d = np.linalg.norm(xs[stage] - xs[0]) / np.linalg.norm(xs[0])
