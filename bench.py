@@ -70,10 +70,12 @@ def _set_scheduler(rt, name):
         rt.set_param(N.PARAM_SELL_SORT, SELL_SORT)
 
 
-def _scalar_spmv_kernel(rt):
+def _scalar_spmv_kernel(rt, precision):
     """Name of the scalar SpMV-phase kernel the context's staging selects."""
     from cloudfem_b200 import _native as N
     stage = rt.get_param(N.PARAM_SPMV_STAGE)
+    if stage == 4:   # auto: sliced ELL in FP64, staged windows in FP32
+        stage = 3 if precision == "fp64" else 1
     return {0: "k_gx (register path)", 3: "k_gxl (sliced ELL, one row per lane)"}.get(
         stage, "k_gxs (matrix bulk-staged through shared memory)")
 
@@ -573,7 +575,7 @@ def run_batched_heat(args, rank, world, local_rank):
     if spmv_ms > 0:
         ach = spmv_b / (spmv_ms * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": _scalar_spmv_kernel(rt) + " (batched PCG SpMV phase over all systems: q = A p, p.q)",
+            "kernel": _scalar_spmv_kernel(rt, args.precision) + " (batched PCG SpMV phase over all systems: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": spmv_ms,
@@ -768,7 +770,7 @@ def run_transient_heat(args, rank, world, local_rank):
     if spmv:
         ach = spmv_b / (float(np.mean(spmv)) * 1e-3) / 1e9
         out["roofline"] = {
-            "kernel": _scalar_spmv_kernel(rt) + " (scalar PCG SpMV phase: q = A p, p.q)",
+            "kernel": _scalar_spmv_kernel(rt, args.precision) + " (scalar PCG SpMV phase: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": float(np.mean(spmv)), "traffic": None,
@@ -1212,11 +1214,11 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
                     help="batched-heat: number of meshes of the seeded draw (a smaller "
                          "batch of the same kind, e.g. for profiling)")
-    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2, 3],
+    ap.add_argument("--spmv-stage", type=int, default=None, choices=[0, 1, 2, 3, 4],
                     help="SpMV: 1 scalar rows bulk-staged through shared memory, 3x3 "
                          "blocks in registers; 2 both staged; 0 both in registers; 3 "
-                         "scalar rows in the sliced-ELL layout (one row per lane), 3x3 "
-                         "blocks in registers (default: the library's)")
+                         "scalar and 3x3 rows in the sliced-ELL layout (one row per "
+                         "lane); 4 per precision and block size (library default)")
     ap.add_argument("--sell-sort", type=int, default=None, choices=[0, 1],
                     help="sliced-ELL SpMV: 1 sort each 256-row window by row length, "
                          "0 keep rows in order (default: the library's)")

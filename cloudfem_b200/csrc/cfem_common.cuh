@@ -75,7 +75,8 @@ struct cfem_ctx {
     int p1_threads = 128;              // P1 element kernels, threads per block
     int graph_iters = 2;               // iterations per solve-loop body
     int pdl = 1;                       // dependent launches in solve graphs
-    int spmv_stage = 1;                // SpMV: 0 registers, 1 staged scalar rows, 2 also 3x3
+    int spmv_stage = 4;                // SpMV: 0 registers, 1 staged scalar rows, 2 also
+                                       // 3x3, 3 sliced ELL, 4 auto (per precision and bs)
     int sell_sort = 1;                 // sliced ELL: sort rows by length per window
     int barrier_timeout_us = 4000000;  // persistent grid-barrier wait limit
     int barrier_hold = 0;              // phantom barrier arrivals (fault injection)

@@ -232,8 +232,8 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
             ctx->pdl = value;
             return CFEM_OK;
         case CFEM_PARAM_SPMV_STAGE:
-            CFEM_CHECK(value >= 0 && value <= 3, CFEM_ERR_INVALID,
-                       "SpMV staging must be 0, 1, 2 or 3 (got %d)", value);
+            CFEM_CHECK(value >= 0 && value <= 4, CFEM_ERR_INVALID,
+                       "SpMV staging must be 0, 1, 2, 3 or 4 (got %d)", value);
             ctx->spmv_stage = value;
             return CFEM_OK;
         case CFEM_PARAM_SELL_SORT:

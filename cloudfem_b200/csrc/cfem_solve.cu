@@ -55,6 +55,11 @@ constexpr double FLOOR_C = 16.0 * 2.220446049250313e-16;
 // answer carries a residual of about eps * |A||x|, so stopping at the tight
 // bound matches its accuracy even on ill-conditioned systems.
 constexpr double FLOOR_TIGHT = 2.0 * 2.220446049250313e-16;
+// At the floor, the FP64 solver keeps cycling (one cycle = the iterations
+// between two true residuals) until a whole cycle moved x by less than
+// DX_TOL |x|: on ill-conditioned systems the residual is all rounding noise
+// there while the error in smooth modes still falls about tenfold per cycle.
+constexpr double DX_TOL = 1e-13;
 constexpr int BAR_GROUP = 16;              // blocks per first-level counter
 constexpr int BAR_MAX_GROUPS = 64;
 
@@ -110,6 +115,7 @@ struct SysDev {
 
 struct SysState {
     double rz, alpha, beta, bb, rmax2, best, relres, zeta;
+    double dx2, xx;       // FP64: sum |alpha p|^2 since the last true residual, |x|^2
     int32_t phase, iter, status, nres, stall, pbuf;
     unsigned int cnt;
     int32_t pad;
@@ -411,8 +417,13 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     } else {
         d0 = ldcg(dinv + ii);
     }
+    double dxx = 0.0, xx = 0.0;
     if (valid && !fx) {
-        S.x[i] = xi + alpha64 * (double)pi;
+        const double dx = alpha64 * (double)pi;
+        const double xn = xi + dx;
+        S.x[i] = xn;
+        dxx = dx * dx;
+        xx = xn * xn;
         rv -= alpha * qi;
     }
     T zv;
@@ -435,6 +446,8 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     }
     part[0] += (double)rz;
     part[1] += (double)rr;
+    part[2] += dxx;
+    part[3] += xx;
 }
 
 // ------------------------------------------------------- phase R / INIT
@@ -765,6 +778,8 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
         const double rz = tot[0], rr = tot[1];
         const double bb = st->bb;
         st->iter += 1;
+        st->dx2 += tot[2];
+        st->xx = tot[3];
         if (!isfinite(rz) || !isfinite(rr)) {
             st->status = CFEM_ERR_BREAKDOWN;
         } else if (rr <= rtol2 * bb || rr < S.delta2 * st->rmax2) {
@@ -803,11 +818,15 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
             } else {
                 st->stall += 1;
             }
-            if (rr <= loose2 && st->stall >= 1) {
+            const bool at_floor = rr <= loose2;
+            const bool settled = S.mode != CFEM_SOLVE_FP64 ||
+                                 st->dx2 <= DX_TOL * DX_TOL * st->xx;
+            if (at_floor && (st->stall >= S.max_stall || (st->stall >= 1 && settled))) {
                 // converged at the round-off floor
             } else if (st->stall >= S.max_stall) {
                 st->status = CFEM_ERR_NOT_CONVERGED;
             } else {
+                st->dx2 = 0.0;
                 // The replaced residual is no longer orthogonal to the last
                 // search direction; restore r.p' = 0 with p' = p - g z,
                 // g = r.p / r.z, folded into the next p = z + beta p'.
@@ -1792,10 +1811,15 @@ __device__ void phase_B_multi(const SysDev &S, const SysState *st, int64_t r0,
         }
     }
     T rz = 0, rr = 0;
+    double dxx = 0.0, xx = 0.0;
 #pragma unroll
     for (int k = 0; k < BPASS; ++k) {
         if (valid[k] && !fx[k]) {
-            S.x[iv[k]] = xi[k] + alpha64 * (double)pi[k];
+            const double dx = alpha64 * (double)pi[k];
+            const double xn = xi[k] + dx;
+            S.x[iv[k]] = xn;
+            dxx += dx * dx;
+            xx += xn * xn;
             rv[k] -= alpha * qi[k];
         }
         T zv;
@@ -1818,6 +1842,8 @@ __device__ void phase_B_multi(const SysDev &S, const SysState *st, int64_t r0,
     }
     part[0] += (double)rz;
     part[1] += (double)rr;
+    part[2] += dxx;
+    part[3] += xx;
 }
 
 // Work lists hold each system's chunks padded to whole groups of GROUP
@@ -2004,7 +2030,7 @@ k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
         const int64_t r1 = min(S.n, r0 + brows(BS));
         phase_B_multi<T, BS>(S, &st[e.x], r0, r1, lane, part);
     }
-    group_store(part, 2, S.partialB + (int64_t)(lead.y / GROUP) * 4, lane, w);
+    group_store(part, 4, S.partialB + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
 // Direction update of the A phase, p = zeta z + beta p_old, over the rows of
@@ -2060,7 +2086,8 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     const int ph = *(volatile int32_t *)&st[s].phase;
     const bool mine = which ? (ph == PH_B) : (ph == PH_A || ph == PH_R || ph == PH_ZERO);
     if (!mine) return;
-    const int n = which ? (S.nchunksB + GROUP - 1) / GROUP : (S.nxe + GROUP - 1) / GROUP;
+    const int n = which ? (S.nchunksB + GROUP - 1) / GROUP
+                        : (S.sell && S.bs == 1 ? S.nxe : (S.nxe + GROUP - 1) / GROUP);
     const double *P = which ? S.partialB : S.partial;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     // four independent slots per round keep the loads in flight
@@ -2364,38 +2391,88 @@ __device__ __forceinline__ void phase_A_sell(const SysDev &S, const SysState *st
     part[0] += (double)pq;
 }
 
-// k_gx for scalar systems with the sliced-ELL A phase: one slice of 32
-// rows per warp (work entries of 32 rows, so the GROUP warps of a block
-// cover one window of SELL_ROWS rows); R and ZERO phases on the entry's rows
-// from the unit-padded copy, as in k_gxs.
+// FP64 true residual (R phase, not INIT) over the 32 rows of slice sl from
+// the sliced-ELL copy itself, whose values are FP64 when the system is
+// solved in FP64: one row per lane, compensated sums as in phase_R.
+template <typename T>
+__device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st, int64_t sl,
+                                             int lane, double part[4]) {
+    const int64_t r0 = (sl / SELL_SLICES) * SELL_ROWS;
+    const int s = (int)(sl % SELL_SLICES);
+    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    if (s * 32 >= nr) return;
+    const int64_t base = __ldg(S.soff + sl);
+    const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+    const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
+    const int32_t *cp = S.scol + base + lane;
+    const double *vp = (const double *)S.sval + base + lane;
+    double hi = 0.0, lo = 0.0, aab = 0.0;
+    for (int k = 0; k < w; ++k) {
+        const double a = ld_stream(vp + 32 * k);
+        const double xj = ldcg(S.x + ld_stream(cp + 32 * k));
+        dd_fma(hi, lo, a, xj);
+        aab += fabs(a * xj);
+    }
+    if (rl >= nr) return;
+    const int64_t i = r0 + rl;
+    const bool fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
+    const double rt = fx ? 0.0 : dd_residual(__ldg(S.b + i), hi, lo);
+    const T rv = (T)rt;
+    ((T *)S.r)[i] = rv;
+    T zv = fx ? (T)0 : ldcg((const T *)S.dinv + i) * rv;
+    ((T *)S.z)[i] = zv;
+    const T *pc = (const T *)(vcgi(&st->pbuf) == 0 ? S.p0 : S.p1);
+    part[0] += rt * rt;
+    part[1] += (double)(rv * ldcg(pc + i));
+    part[2] += (double)(rv * zv);
+    if (!fx) part[3] += aab * aab;
+}
+
+// k_gx for scalar systems with the sliced-ELL A phase. The grid is a fixed
+// resident set of warps, each taking a contiguous run of the list's entries
+// (one slice of 32 rows each; the slices of a window differ in length, so a
+// run holds every kind and no block waits on its longest warp); every entry
+// writes its own partial sums, summed per system by k_greduce in entry
+// order, so the result does not depend on which warp took which entry. R and
+// ZERO phases on the entry's rows from the unit-padded copy, as in k_gxs.
 template <typename T>
 __global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
 k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
       const int2 *__restrict__ list, int n) {
     pdl_wait();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wid = blockIdx.x * GROUP + w;
-    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
-    const int2 lead = __ldg(list + blockIdx.x * GROUP);
     if (*(volatile const int *)&bar->active <= 0) return;   // all finished
-    const SysDev &S = sys[lead.x];
-    const int ph = *(volatile int32_t *)&st[lead.x].phase;
-    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
-    if (!x_phase) return;                 // uniform over the block
-    double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (int64_t)blockIdx.x * GROUP + (threadIdx.x >> 5);
+    const int64_t nw = (int64_t)gridDim.x * GROUP;
+    const int64_t per = (n + nw - 1) / nw;
+    const int64_t i0 = wid * per, i1 = min((int64_t)n, i0 + per);
+    for (int64_t idx = i0; idx < i1; ++idx) {
+        const int2 e = __ldg(list + idx);
+        if (e.x < 0) continue;
+        const SysDev &S = sys[e.x];
+        const int ph = *(volatile int32_t *)&st[e.x].phase;
+        if (!(ph == PH_A || ph == PH_R || ph == PH_ZERO)) continue;   // warp-uniform
+        double part[4] = {0.0, 0.0, 0.0, 0.0};
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
             phase_A_sell<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
         } else if (ph == PH_R) {
-            int bad = 0;
-            run_R<T, 1>(S, &st[e.x], r0, r1, lane, part, &bad);
+            if (sizeof(T) == 8) {
+                phase_R_sell<T>(S, &st[e.x], e.y, lane, part);
+            } else {
+                int bad = 0;
+                run_R<T, 1>(S, &st[e.x], r0, r1, lane, part, &bad);
+            }
         } else {
             phase_zero<1>(S, r0, r1, lane);
         }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
+        if (lane == 0)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) S.partial[(int64_t)e.y * 4 + v] = part[v];
     }
-    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
 // k_gx for 3x3 systems with the sliced-ELL A phase (one block row per
@@ -2830,19 +2907,28 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     P->bar_hold = (unsigned)ctx->barrier_hold;
     // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
     // systems a padded block copy (staged SpMV) or an entry-major copy.
-    const bool stage3 = ctx->spmv_stage == 2;
-    const bool sell = ctx->spmv_stage == 3;   // sliced-ELL scalar SpMV
+    // SpMV staging per list type t = 2 (mixed) + (3x3): explicit, or AUTO
+    // (4): sliced ELL for FP64 scalar rows, the bulk-staged windows for FP32
+    // scalar rows, the register path for 3x3 blocks (the fastest measured
+    // for each on the benchmark workloads)
+    int tstage[4];
+    for (int t = 0; t < 4; ++t)
+        tstage[t] = ctx->spmv_stage != 4 ? ctx->spmv_stage : (t == 0 ? 3 : t == 2 ? 1 : 0);
+    auto stage_of = [&](const SysDev &S) {
+        return tstage[(S.mode == CFEM_SOLVE_MIXED ? 2 : 0) + (S.bs == 3 ? 1 : 0)];
+    };
     if (!persistent)
         for (int i = 0; i < n_systems; ++i) {
             const size_t ts = (hs[i].mode == CFEM_SOLVE_MIXED) ? 4 : 8;
             if (hs[i].bs == 1) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 8) +
-                              (hs[i].mode == CFEM_SOLVE_MIXED && !sell ? align256(ne * 4) : 0);
-            } else if (stage3) {
+                              (hs[i].mode == CFEM_SOLVE_MIXED && stage_of(hs[i]) != 3
+                                   ? align256(ne * 4) : 0);
+            } else if (stage_of(hs[i]) == 2) {
                 const size_t ne = (size_t)hs[i].nnzb + 3 * (size_t)hs[i].n + 8;
                 copy_bytes += align256(ne * 4) + align256(ne * 9 * ts);
-            } else if (sell) {
+            } else if (stage_of(hs[i]) == 3) {
                 // sliced-ELL copy allocated by sell_layout
             } else {
                 copy_bytes += align256((size_t)hs[i].nnzb * 9 * ts);
@@ -2875,11 +2961,11 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         S.tcnt = (unsigned *)take_s(S.ntiles * sizeof(unsigned));
         S.partialB = (double *)take_s(S.nchunksB * 4 * sizeof(double));
         if (S.bs == 3) {
-            if (!persistent && stage3) {
+            if (!persistent && stage_of(S) == 2) {
                 const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
                 S.c3 = (const int32_t *)take_c(ne * 4);
                 S.v3 = take_c(ne * 9 * ts);
-            } else if (!persistent && sell) {
+            } else if (!persistent && stage_of(S) == 3) {
                 S.sell = 1;
             } else if (!persistent) {
                 S.vsoa = take_c((size_t)S.nnzb * 9 * ts);
@@ -2890,6 +2976,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                 const size_t ne = (size_t)S.nnzb + 3 * (size_t)S.n + 8;
                 S.ci4 = (const int32_t *)take_c(ne * 4);
                 S.va4d = (const double *)take_c(ne * 8);
+                const bool sell = stage_of(S) == 3;
                 S.va4 = (S.mode == CFEM_SOLVE_MIXED) ? (sell ? nullptr : take_c(ne * 4))
                                                      : (const void *)S.va4d;
                 S.vec4 = 1;
@@ -2911,7 +2998,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     P->d_chunks = (int32_t *)take_c(n_chunks * sizeof(int32_t));
     int2 *d_lista = (int2 *)take_c(list_a * sizeof(int2));
     int2 *d_listb = (int2 *)take_c(list_b * sizeof(int2));
-    if (sell) CFEM_TRY(sell_layout(P, s));
+    CFEM_TRY(sell_layout(P, s));
     CFEM_TRY(plan_copies(P, s));
     CFEM_CUDA(cudaMemcpyAsync(P->d_sys, hs.data(), n_systems * sizeof(SysDev),
                               cudaMemcpyHostToDevice, s));
@@ -2959,7 +3046,6 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // SpMV: bulk-staged (2) or the register path (0, 1); lanes
     // per row from the mean row length of the list's systems (4 up to 16
     // entries, whole units of a P1 row; 8 above, Tet10 rows of ~27)
-    const int stage = ctx->spmv_stage;
     int lpr[4] = {8, 8, 8, 8};
     for (int t = 0; t < 4; t += 2) {
         double nz = 0.0, rows = 0.0;
@@ -2970,12 +3056,12 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             }
         if (rows > 0 && nz <= 16.0 * rows) lpr[t] = 4;
     }
-    if ((stage == 1 || stage == 2) && !la[0].empty())
+    if ((tstage[0] == 1 || tstage[0] == 2) && !la[0].empty())
         CFEM_TRY((lpr[0] == 4 ? gxs_prepare<double, 4>() : gxs_prepare<double, 8>()));
-    if ((stage == 1 || stage == 2) && !la[2].empty())
+    if ((tstage[2] == 1 || tstage[2] == 2) && !la[2].empty())
         CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
-    if (stage == 2 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
-    if (stage == 2 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
+    if (tstage[1] == 2 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
+    if (tstage[3] == 2 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
         const bool pdl = use_pdl && !t0;
@@ -2996,8 +3082,11 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (!n) continue;
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
-            if (t == 0 && stage == 3) glaunch(p, k_gxl<double>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 2 && stage == 3) glaunch(p, k_gxl<float>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            const int stage = tstage[t];
+            // sliced ELL (scalar): one resident wave of warps over the list
+            const unsigned gl = std::min(g, (unsigned)(ctx->num_sms * SELL_BLOCKS));
+            if (t == 0 && stage == 3) glaunch(p, k_gxl<double>, gl, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 3) glaunch(p, k_gxl<float>, gl, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 0 && (stage == 1 || stage == 2))
                 glaunch_smem(p, lpr[0] == 4 ? k_gxs<double, 4> : k_gxs<double, 8>, g, 32 * GROUP, gxs_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 2 && (stage == 1 || stage == 2))

@@ -173,14 +173,16 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * convergence). PDL: 1 (default) captures the solve graphs' kernels as
  * programmatic dependent launches (launch processing overlaps the previous
  * kernel's drain), 0 as plain launches. SPMV_STAGE: how the graph
- * scheduler's SpMV reads its padded working copy of the matrix: 1 (default)
- * streams each scalar work entry's span through two shared-memory windows
- * of about 4 KB per warp with 1-D bulk copies (TMA) and loads 3x3 blocks
- * into registers, 2 streams 3x3 blocks through shared memory too (slower on
- * the elasticity beam: kept for tuning), 0 loads both into registers, 3
- * stores scalar rows and 3x3 block rows in the sliced-ELL layout (windows of
- * 256 rows cut into slices of 32, one row per lane, coalesced slot-major
- * loads, no cross-lane sums).
+ * scheduler's SpMV reads its working copy of the matrix: 1 streams each
+ * scalar work entry's span through two shared-memory windows of about 4 KB
+ * per warp with 1-D bulk copies (TMA) and loads 3x3 blocks into registers,
+ * 2 streams 3x3 blocks through shared memory too, 0 loads both into
+ * registers, 3 stores scalar rows and 3x3 block rows in the sliced-ELL
+ * layout (windows of 256 rows cut into slices of 32, one row per lane,
+ * coalesced slot-major loads, no cross-lane sums), 4 (default) picks per
+ * precision and block size what measured fastest: sliced ELL for FP64
+ * scalar rows, the staged windows for FP32 scalar rows, registers for 3x3
+ * blocks.
  * BARRIER_TIMEOUT_US: how long (microseconds, 1 .. 60e6; default 4e6) a
  * block of the persistent scheduler waits at its grid barrier before it
  * gives up; the solve then ends with CFEM_ERR_TIMEOUT and the context stays
