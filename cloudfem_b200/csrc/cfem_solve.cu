@@ -55,11 +55,6 @@ constexpr double FLOOR_C = 16.0 * 2.220446049250313e-16;
 // answer carries a residual of about eps * |A||x|, so stopping at the tight
 // bound matches its accuracy even on ill-conditioned systems.
 constexpr double FLOOR_TIGHT = 2.0 * 2.220446049250313e-16;
-// At the floor, the FP64 solver keeps cycling (one cycle = the iterations
-// between two true residuals) until a whole cycle moved x by less than
-// DX_TOL |x|: on ill-conditioned systems the residual is all rounding noise
-// there while the error in smooth modes still falls about tenfold per cycle.
-constexpr double DX_TOL = 1e-13;
 constexpr int BAR_GROUP = 16;              // blocks per first-level counter
 constexpr int BAR_MAX_GROUPS = 64;
 
@@ -115,7 +110,6 @@ struct SysDev {
 
 struct SysState {
     double rz, alpha, beta, bb, rmax2, best, relres, zeta;
-    double dx2, xx;       // FP64: sum |alpha p|^2 since the last true residual, |x|^2
     int32_t phase, iter, status, nres, stall, pbuf;
     unsigned int cnt;
     int32_t pad;
@@ -417,13 +411,8 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     } else {
         d0 = ldcg(dinv + ii);
     }
-    double dxx = 0.0, xx = 0.0;
     if (valid && !fx) {
-        const double dx = alpha64 * (double)pi;
-        const double xn = xi + dx;
-        S.x[i] = xn;
-        dxx = dx * dx;
-        xx = xn * xn;
+        S.x[i] = xi + alpha64 * (double)pi;
         rv -= alpha * qi;
     }
     T zv;
@@ -446,8 +435,6 @@ __device__ void phase_B(const SysDev &S, const SysState *st, int64_t r0,
     }
     part[0] += (double)rz;
     part[1] += (double)rr;
-    part[2] += dxx;
-    part[3] += xx;
 }
 
 // ------------------------------------------------------- phase R / INIT
@@ -778,8 +765,6 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
         const double rz = tot[0], rr = tot[1];
         const double bb = st->bb;
         st->iter += 1;
-        st->dx2 += tot[2];
-        st->xx = tot[3];
         if (!isfinite(rz) || !isfinite(rr)) {
             st->status = CFEM_ERR_BREAKDOWN;
         } else if (rr <= rtol2 * bb || rr < S.delta2 * st->rmax2) {
@@ -818,15 +803,11 @@ __device__ void advance(const SysDev &S, SysState *st, GridBar *bar, int ph,
             } else {
                 st->stall += 1;
             }
-            const bool at_floor = rr <= loose2;
-            const bool settled = S.mode != CFEM_SOLVE_FP64 ||
-                                 st->dx2 <= DX_TOL * DX_TOL * st->xx;
-            if (at_floor && (st->stall >= S.max_stall || (st->stall >= 1 && settled))) {
+            if (rr <= loose2 && st->stall >= 1) {
                 // converged at the round-off floor
             } else if (st->stall >= S.max_stall) {
                 st->status = CFEM_ERR_NOT_CONVERGED;
             } else {
-                st->dx2 = 0.0;
                 // The replaced residual is no longer orthogonal to the last
                 // search direction; restore r.p' = 0 with p' = p - g z,
                 // g = r.p / r.z, folded into the next p = z + beta p'.
@@ -1811,15 +1792,10 @@ __device__ void phase_B_multi(const SysDev &S, const SysState *st, int64_t r0,
         }
     }
     T rz = 0, rr = 0;
-    double dxx = 0.0, xx = 0.0;
 #pragma unroll
     for (int k = 0; k < BPASS; ++k) {
         if (valid[k] && !fx[k]) {
-            const double dx = alpha64 * (double)pi[k];
-            const double xn = xi[k] + dx;
-            S.x[iv[k]] = xn;
-            dxx += dx * dx;
-            xx += xn * xn;
+            S.x[iv[k]] = xi[k] + alpha64 * (double)pi[k];
             rv[k] -= alpha * qi[k];
         }
         T zv;
@@ -1842,8 +1818,6 @@ __device__ void phase_B_multi(const SysDev &S, const SysState *st, int64_t r0,
     }
     part[0] += (double)rz;
     part[1] += (double)rr;
-    part[2] += dxx;
-    part[3] += xx;
 }
 
 // Work lists hold each system's chunks padded to whole groups of GROUP
@@ -2086,8 +2060,7 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
     const int ph = *(volatile int32_t *)&st[s].phase;
     const bool mine = which ? (ph == PH_B) : (ph == PH_A || ph == PH_R || ph == PH_ZERO);
     if (!mine) return;
-    const int n = which ? (S.nchunksB + GROUP - 1) / GROUP
-                        : (S.sell && S.bs == 1 ? S.nxe : (S.nxe + GROUP - 1) / GROUP);
+    const int n = which ? (S.nchunksB + GROUP - 1) / GROUP : (S.nxe + GROUP - 1) / GROUP;
     const double *P = which ? S.partialB : S.partial;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     // four independent slots per round keep the loads in flight
@@ -2428,31 +2401,27 @@ __device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st
     if (!fx) part[3] += aab * aab;
 }
 
-// k_gx for scalar systems with the sliced-ELL A phase. The grid is a fixed
-// resident set of warps, each taking a contiguous run of the list's entries
-// (one slice of 32 rows each; the slices of a window differ in length, so a
-// run holds every kind and no block waits on its longest warp); every entry
-// writes its own partial sums, summed per system by k_greduce in entry
-// order, so the result does not depend on which warp took which entry. R and
-// ZERO phases on the entry's rows from the unit-padded copy, as in k_gxs.
+// k_gx for scalar systems with the sliced-ELL A phase: one slice of 32
+// rows per warp (work entries of 32 rows, so the GROUP warps of a block
+// cover one window of SELL_ROWS rows). R phase: from the sliced-ELL copy in
+// FP64 (its values are FP64 then), else from the unit-padded copy as in
+// k_gxs; ZERO phase on the entry's rows.
 template <typename T>
 __global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
 k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
       const int2 *__restrict__ list, int n) {
     pdl_wait();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);
     if (*(volatile const int *)&bar->active <= 0) return;   // all finished
-    const int lane = threadIdx.x & 31;
-    const int64_t wid = (int64_t)blockIdx.x * GROUP + (threadIdx.x >> 5);
-    const int64_t nw = (int64_t)gridDim.x * GROUP;
-    const int64_t per = (n + nw - 1) / nw;
-    const int64_t i0 = wid * per, i1 = min((int64_t)n, i0 + per);
-    for (int64_t idx = i0; idx < i1; ++idx) {
-        const int2 e = __ldg(list + idx);
-        if (e.x < 0) continue;
-        const SysDev &S = sys[e.x];
-        const int ph = *(volatile int32_t *)&st[e.x].phase;
-        if (!(ph == PH_A || ph == PH_R || ph == PH_ZERO)) continue;   // warp-uniform
-        double part[4] = {0.0, 0.0, 0.0, 0.0};
+    const SysDev &S = sys[lead.x];
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
+    if (!x_phase) return;                 // uniform over the block
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e.x >= 0) {
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -2467,12 +2436,8 @@ k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
         } else {
             phase_zero<1>(S, r0, r1, lane);
         }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) part[v] = warp_sum(part[v]);
-        if (lane == 0)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) S.partial[(int64_t)e.y * 4 + v] = part[v];
     }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
 // k_gx for 3x3 systems with the sliced-ELL A phase (one block row per
@@ -3083,10 +3048,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             const unsigned g = (unsigned)(n / GROUP);
             const bool p = L(pdl);
             const int stage = tstage[t];
-            // sliced ELL (scalar): one resident wave of warps over the list
-            const unsigned gl = std::min(g, (unsigned)(ctx->num_sms * SELL_BLOCKS));
-            if (t == 0 && stage == 3) glaunch(p, k_gxl<double>, gl, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
-            if (t == 2 && stage == 3) glaunch(p, k_gxl<float>, gl, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 0 && stage == 3) glaunch(p, k_gxl<double>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 2 && stage == 3) glaunch(p, k_gxl<float>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 0 && (stage == 1 || stage == 2))
                 glaunch_smem(p, lpr[0] == 4 ? k_gxs<double, 4> : k_gxs<double, 8>, g, 32 * GROUP, gxs_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
             if (t == 2 && (stage == 1 || stage == 2))

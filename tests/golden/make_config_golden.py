@@ -51,6 +51,7 @@ def refine_ext(A, b, x, solve, steps=4):
 
 def main(ref_path):
     sys.path.insert(0, ref_path)
+    import scipy.sparse as sp
     import scipy.sparse.linalg as spla
 
     from cloudfem.fem import tet10 as t10
@@ -133,6 +134,14 @@ def main(ref_path):
     put("c2q_sol_refined", np.stack([u[0::3], u[1::3], u[2::3]]))
     put("c2q_refine_relres", np.array(hist))
     put("c2q_refine_change", np.array(np.linalg.norm(xr - x0) / np.linalg.norm(xr)))
+    # condition number of the Jacobi-scaled reduced system (the solver's
+    # preconditioned operator): the tests state errors beside kappa * eps
+    dh = 1.0 / np.sqrt(Af.diagonal())
+    As = (sp.diags(dh) @ Af @ sp.diags(dh)).tocsc()
+    lmax = spla.eigsh(As, k=1, which="LA", return_eigenvectors=False)[0]
+    lmin = spla.eigsh(As, k=1, sigma=0.0, which="LM", return_eigenvectors=False)[0]
+    put("c2q_kappa", np.array(lmax / lmin))
+    log(f"C2 quarter: Jacobi-scaled condition number {lmax / lmin:.3e}")
     log(f"C2 quarter refinement: residuals {hist}, "
         f"change {np.linalg.norm(xr - x0) / np.linalg.norm(xr):.2e}")
     del e3
