@@ -23,6 +23,7 @@ CFEM_ERR_NOT_CONVERGED = 4
 CFEM_ERR_BREAKDOWN = 5
 CFEM_ERR_TIMEOUT = 6
 CFEM_ERR_UNSUPPORTED = 7
+CFEM_SLOT_RUNNING = -1
 
 OP_P1_STIFF, OP_P1_MASS, OP_T10_STIFF, OP_T10_MASS = 1, 2, 3, 4
 OP_P1_ELAST, OP_T10_ELAST = 5, 6
@@ -132,6 +133,12 @@ SIGNATURES = [
     ("cfem_cocg_solve", ctypes.c_int,
      [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _f64, _i32, ctypes.POINTER(SolveStats), _vp]),
     ("cfem_pcg_noalloc_capacity", ctypes.c_size_t, []),
+    ("cfem_pcg_slots_create", ctypes.c_int,
+     [_vp, _i32, _i32, _i32, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
+    ("cfem_pcg_slots_assign", ctypes.c_int, [_vp, _i32, ctypes.POINTER(LinSys), _vp]),
+    ("cfem_pcg_slots_run", ctypes.c_int, [_vp, _i32, _vp]),
+    ("cfem_pcg_slots_poll", ctypes.c_int, [_vp, ctypes.POINTER(SolveStats)]),
+    ("cfem_pcg_slots_release", ctypes.c_int, [_vp, _i32, _vp]),
     ("cfem_pcg_solve_noalloc", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), ctypes.POINTER(SolveStats), _vp]),
 ]

@@ -927,6 +927,7 @@ __device__ __forceinline__ void dispatch(const SysDev *__restrict__ sys,
     if (RUN == RUN_X && ph == PH_B) return;
     if (RUN == RUN_B && ph != PH_B) return;
     const int lc = c - S.chunk0;
+    if (lc >= S.nchunks) return;   // a solve slot holding a smaller system
     if (S.mode == CFEM_SOLVE_MIXED) {
         if (S.bs == 3) run_chunk<float, 3, RUN>(S, &st[s], bar, ph, lc, lane);
         else run_chunk<float, 1, RUN>(S, &st[s], bar, ph, lc, lane);
@@ -1867,7 +1868,7 @@ k_gx(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -1919,7 +1920,7 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -1967,7 +1968,7 @@ k_gxs3(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -1999,7 +2000,7 @@ k_gb(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     const SysDev &S = sys[lead.x];
     if (*(volatile int32_t *)&st[lead.x].phase != PH_B) return;
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && e.y < S.nchunksB) {
         const int64_t r0 = (int64_t)e.y * brows(BS);
         const int64_t r1 = min(S.n, r0 + brows(BS));
         phase_B_multi<T, BS>(S, &st[e.x], r0, r1, lane, part);
@@ -2421,7 +2422,7 @@ k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -2458,7 +2459,7 @@ k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0) {
+    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
@@ -2627,6 +2628,12 @@ struct cfem_pcg_plan {
     // POLL_ITERS iterations replayed in turn
     bool polled = false;
     int giters = 2;               // iterations per body of the solve loop
+    // solve slots (cfem_pcg_slots_*): each system of the plan is a slot of
+    // fixed capacity whose system is replaced between rounds of iterations
+    bool slots = false;
+    std::vector<int64_t> cap_rows, cap_nnzb;
+    std::vector<cfem::SysDev> tmpl;   // slot templates: workspace pointers
+    char *tmpl_mem = nullptr;         // the templates' placeholder CSR
     cudaGraph_t pgraph[2] = {nullptr, nullptr};
     cudaGraphExec_t pexec[2] = {nullptr, nullptr};
 };
@@ -2636,8 +2643,9 @@ namespace cfem {
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // (Re)build the working copies of the matrix values on stream s.
-static int plan_copies(cfem_pcg_plan *P, cudaStream_t s) {
-    for (int i = 0; i < P->n_systems; ++i) {
+static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last = -1) {
+    if (last < 0) last = P->n_systems;
+    for (int i = first; i < last; ++i) {
         SysDev &S = P->hs[i];
         if (S.bs == 3 && S.sell) {
             if (S.mode == CFEM_SOLVE_MIXED)
@@ -2758,6 +2766,7 @@ static void plan_free(cfem_pcg_plan *P) {
         if (P->ws_copy) cudaFreeAsync(P->ws_copy, P->w);
         if (P->ws_state) cudaFreeAsync(P->ws_state, P->w);
         if (P->ws_smeta) cudaFreeAsync(P->ws_smeta, P->w);
+        if (P->tmpl_mem) cudaFreeAsync(P->tmpl_mem, P->w);
         if (P->ws_sdata) cudaFreeAsync(P->ws_sdata, P->w);
         cudaStreamSynchronize(P->w);
     }
@@ -2862,8 +2871,9 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // One resident wave holds every chunk: the persistent kernel pays a grid
     // barrier per phase and no launches. Otherwise the graph scheduler keeps
     // the SMs fed with one warp per chunk per launch.
-    const bool persistent = ctx->scheduler == CFEM_SCHED_PERSISTENT ||
-                            (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid);
+    const bool persistent = !P->slots &&
+                            (ctx->scheduler == CFEM_SCHED_PERSISTENT ||
+                             (ctx->scheduler == CFEM_SCHED_AUTO && useful <= grid));
     if (grid > useful) grid = useful < 1 ? 1 : useful;
     if (grid > BAR_GROUP * BAR_MAX_GROUPS) grid = BAR_GROUP * BAR_MAX_GROUPS;
     P->persistent = persistent;
@@ -2879,6 +2889,10 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     int tstage[4];
     for (int t = 0; t < 4; ++t)
         tstage[t] = ctx->spmv_stage != 4 ? ctx->spmv_stage : (t == 0 ? 3 : t == 2 ? 1 : 0);
+    // solve slots: copies whose size follows the capacity alone (no sliced
+    // ELL, whose padding depends on the system)
+    if (P->slots)
+        for (int t = 0; t < 4; ++t) tstage[t] = (t & 1) ? 0 : 1;
     auto stage_of = [&](const SysDev &S) {
         return tstage[(S.mode == CFEM_SOLVE_MIXED ? 2 : 0) + (S.bs == 3 ? 1 : 0)];
     };
@@ -3089,7 +3103,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // GRAPH_ITERS iterations that ends when no system is active. No host
     // polling; at most GRAPH_ITERS - 1 iterations run past convergence
     // (their kernels return at once for finished systems).
-    if (ctx->scheduler == CFEM_SCHED_GRAPH_POLLED) {
+    if (ctx->scheduler == CFEM_SCHED_GRAPH_POLLED || P->slots) {
         // Plain graphs of POLL_ITERS iterations replayed by the host, which
         // polls the active count one replay behind (every kernel launch is
         // visible to per-launch profilers).
@@ -3314,6 +3328,248 @@ extern "C" int cfem_pcg_solve(cfem_ctx *ctx, const cfem_linsys *systems,
     if (st == CFEM_OK) st = plan_run(P, stats, (cudaStream_t)stream);
     plan_free(P);
     return st;
+    CFEM_API_END
+}
+
+// ---------------------------------------------------------------------------
+// Solve slots: continuous batching at iteration level. A slot plan is a
+// plan of n_slots systems of fixed capacity (rows, nonzero blocks), built
+// from placeholder systems of that size on the host-polled graph scheduler,
+// so its work lists, workspace and captured iteration graphs never change.
+// A system is put into a free slot between rounds (its SysDev entry
+// replaced, its working copy built, its state reset and INIT run for its
+// own chunks), every round replays the captured iterations over all slots
+// (kernels skip idle slots and the list entries past a smaller system), and
+// a finished system's slot is free for the next one at once: new systems
+// join a running batch without waiting for the others to converge. Each
+// system keeps its own scalars and fixed-order sums, so its answer does not
+// depend on which other systems share the rounds.
+namespace cfem {
+
+__global__ void k_slots_idle(SysState *st, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) st[i].phase = PH_DONE;
+}
+
+__global__ void k_slot_open(GridBar *bar) {
+    if (threadIdx.x == 0) atomicAdd(&bar->active, 1);
+}
+
+__global__ void k_slot_cancel(SysState *st, GridBar *bar) {
+    if (threadIdx.x == 0 && st->phase != PH_DONE) {
+        st->phase = PH_DONE;
+        atomicSub(&bar->active, 1);
+    }
+}
+
+// INIT (FP64 true residual, Jacobi inverse) over chunks [c0, c0 + n).
+__global__ void __launch_bounds__(256)
+k_pcg_init_range(const SysDev *__restrict__ sys, SysState *st,
+                 const int32_t *__restrict__ chunk_sys, int c0, int n, GridBar *bar) {
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= n) return;
+    dispatch<RUN_INIT>(sys, st, bar, chunk_sys, c0 + c, threadIdx.x & 31);
+}
+
+// Placeholder CSR of a slot template: rows of nnzb / rows entries, column 0.
+__global__ void k_tmpl_rows(int64_t n, int64_t nnzb, int32_t *rp) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i <= n) rp[i] = (int32_t)((i * nnzb) / n);
+}
+
+}  // namespace cfem
+
+extern "C" int cfem_pcg_slots_create(cfem_ctx *ctx, int32_t n_slots, int32_t bs,
+                                     int32_t mode, int64_t max_rows, int64_t max_nnzb,
+                                     void *stream, cfem_pcg_plan **out) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && out && n_slots > 0 && (bs == 1 || bs == 3) &&
+                   (mode == CFEM_SOLVE_FP64 || mode == CFEM_SOLVE_MIXED) && max_rows > 0 &&
+                   max_nnzb > 0 && max_rows < ((int64_t)1 << 31) / 9 &&
+                   max_nnzb < ((int64_t)1 << 31) / 9,
+               CFEM_ERR_INVALID, "cfem_pcg_slots_create: bad arguments");
+    *out = nullptr;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bb = (size_t)bs * bs;
+    const size_t o_rp = 0, o_ci = align256((max_rows + 1) * 4);
+    const size_t o_v64 = o_ci + align256(max_nnzb * 4);
+    const size_t o_v32 = o_v64 + align256(max_nnzb * bb * 8);
+    const size_t o_b = o_v32 + align256(max_nnzb * bb * 4);
+    const size_t o_x = o_b + align256(max_rows * bs * 8);
+    const size_t total = o_x + align256(max_rows * bs * 8);
+    cfem_pcg_plan *P = new cfem_pcg_plan();
+    P->slots = true;
+    if (tmp_alloc(&P->tmpl_mem, total, s) != CFEM_OK ||
+        cudaMemsetAsync(P->tmpl_mem, 0, total, s) != cudaSuccess) {
+        const int st = fail(CFEM_ERR_NOMEM, "slot templates: %zu bytes", total);
+        if (P->tmpl_mem) cudaFreeAsync(P->tmpl_mem, s);
+        P->tmpl_mem = nullptr;
+        delete P;
+        return st;
+    }
+    int32_t *rp = (int32_t *)(P->tmpl_mem + o_rp);
+    k_tmpl_rows<<<grid_for(max_rows + 1, 256), 256, 0, s>>>(max_rows, max_nnzb, rp);
+    std::vector<cfem_linsys> L(n_slots);
+    for (int i = 0; i < n_slots; ++i) {
+        cfem_linsys &t = L[i];
+        memset(&t, 0, sizeof(t));
+        t.n_rows = max_rows;
+        t.bs = bs;
+        t.precond = CFEM_PRECOND_JACOBI;
+        t.d_row_ptr = rp;
+        t.d_col = (const int32_t *)(P->tmpl_mem + o_ci);
+        t.d_vals64 = (const double *)(P->tmpl_mem + o_v64);
+        t.d_vals32 = mode == CFEM_SOLVE_MIXED ? (const float *)(P->tmpl_mem + o_v32) : nullptr;
+        t.d_b = (const double *)(P->tmpl_mem + o_b);
+        t.d_x = (double *)(P->tmpl_mem + o_x);
+        t.rtol = 1.0;
+        t.max_iter = 1;
+        t.mode = mode;
+    }
+    int st = plan_build(ctx, L.data(), n_slots, s, P);
+    if (st == CFEM_OK) {
+        P->tmpl = P->hs;
+        P->cap_rows.assign(n_slots, max_rows);
+        P->cap_nnzb.assign(n_slots, max_nnzb);
+        // every slot idle, no system active
+        if (cudaMemsetAsync(P->ws_state, 0, P->state_bytes, P->w) != cudaSuccess)
+            st = fail(CFEM_ERR_CUDA, "slot state reset failed");
+        else
+            k_slots_idle<<<grid_for(n_slots, 128), 128, 0, P->w>>>(P->d_st, n_slots);
+        if (st == CFEM_OK && cudaStreamSynchronize(P->w) != cudaSuccess)
+            st = fail(CFEM_ERR_CUDA, "slot set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (st != CFEM_OK) {
+        plan_free(P);
+        return st;
+    }
+    *out = P;
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_slots_assign(cfem_pcg_plan *P, int32_t slot, const cfem_linsys *L,
+                                     void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(P && P->slots && L, CFEM_ERR_INVALID, "cfem_pcg_slots_assign: not a slot plan");
+    CFEM_CHECK(slot >= 0 && slot < P->n_systems, CFEM_ERR_INVALID, "slot %d out of range", slot);
+    CFEM_TRY(set_device(P->device));
+    const SysDev &T = P->tmpl[slot];
+    CFEM_CHECK(L->bs == T.bs && L->mode == T.mode, CFEM_ERR_INVALID,
+               "slot %d holds bs %d mode %d systems", slot, T.bs, T.mode);
+    CFEM_CHECK(L->bs == 1 || L->precond == CFEM_PRECOND_JACOBI, CFEM_ERR_INVALID,
+               "solve slots use point Jacobi");
+    CFEM_CHECK(L->n_rows > 0 && L->n_rows <= P->cap_rows[slot] && L->d_row_ptr && L->d_col &&
+                   L->d_vals64 && L->d_b && L->d_x &&
+                   (L->mode == CFEM_SOLVE_FP64 || L->d_vals32),
+               CFEM_ERR_INVALID, "system does not fit slot %d (%lld rows, capacity %lld)",
+               slot, (long long)L->n_rows, (long long)P->cap_rows[slot]);
+    CFEM_CHECK(L->rtol > 0.0 && L->max_iter > 0, CFEM_ERR_INVALID,
+               "rtol and max_iter must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t nnzb = 0;
+    CFEM_CUDA(cudaMemcpyAsync(&nnzb, L->d_row_ptr + L->n_rows, sizeof(int32_t),
+                              cudaMemcpyDeviceToHost, s));
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    CFEM_CHECK(nnzb >= 0 && nnzb <= P->cap_nnzb[slot], CFEM_ERR_INVALID,
+               "system has %d blocks, slot %d holds %lld", nnzb, slot,
+               (long long)P->cap_nnzb[slot]);
+    SysDev S = T;   // the slot's workspace, lists and copies
+    S.n = L->n_rows;
+    S.nnzb = nnzb;
+    S.nchunks = (int32_t)((S.n + S.crows - 1) / S.crows);
+    S.ntiles = (S.nchunks + TILE - 1) / TILE;
+    S.nchunksB = (int32_t)((S.n + brows(S.bs) - 1) / brows(S.bs));
+    S.nxe = (int32_t)((S.n + S.xrows - 1) / S.xrows);
+    S.max_iter = L->max_iter;
+    S.rp = L->d_row_ptr;
+    S.ci = L->d_col;
+    S.v64 = L->d_vals64;
+    S.v32 = L->d_vals32;
+    S.b = L->d_b;
+    S.x = L->d_x;
+    S.fixed = L->d_fixed;
+    S.rtol2 = L->rtol * L->rtol;
+    const double dl = L->reliable_delta > 0.0 ? L->reliable_delta : RELIABLE_DELTA;
+    S.delta2 = dl * dl;
+    S.max_stall = L->max_stall > 0 ? L->max_stall : MAX_STALL;
+    S.hist_cap = L->d_history ? L->history_cap : 0;
+    S.hist = L->d_history;
+    if (S.bs == 1) S.vsoa = (S.mode == CFEM_SOLVE_MIXED) ? (const void *)S.v32 : (const void *)S.v64;
+    P->hs[slot] = S;
+    cudaStream_t w = P->w;
+    CFEM_CUDA(cudaEventRecord(P->ev[0], s));
+    CFEM_CUDA(cudaStreamWaitEvent(w, P->ev[0], 0));
+    CFEM_CUDA(cudaMemcpyAsync(P->d_sys + slot, &P->hs[slot], sizeof(SysDev),
+                              cudaMemcpyHostToDevice, w));
+    CFEM_TRY(plan_copies(P, w, slot, slot + 1));
+    CFEM_CUDA(cudaMemsetAsync(P->d_st + slot, 0, sizeof(SysState), w));
+    CFEM_CUDA(cudaMemsetAsync(S.tcnt, 0, (size_t)T.ntiles * sizeof(unsigned), w));
+    CFEM_LAUNCH(k_slot_open, 1, 32, 0, w, P->d_bar);
+    CFEM_LAUNCH(k_pcg_init_range, grid_for((int64_t)S.nchunks * 32, 256), 256, 0, w,
+                (const SysDev *)P->d_sys, P->d_st, (const int32_t *)P->d_chunks, S.chunk0,
+                S.nchunks, P->d_bar);
+    // the pageable copy of hs[slot] is staged before cudaMemcpyAsync returns
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_slots_run(cfem_pcg_plan *P, int32_t rounds, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(P && P->slots && rounds > 0, CFEM_ERR_INVALID, "cfem_pcg_slots_run: bad args");
+    CFEM_TRY(set_device(P->device));
+    cudaStream_t s = (cudaStream_t)stream, w = P->w;
+    CFEM_CUDA(cudaEventRecord(P->ev[0], s));
+    CFEM_CUDA(cudaStreamWaitEvent(w, P->ev[0], 0));
+    for (int r = 0; r < rounds; ++r) {
+        CFEM_CUDA(cudaGraphLaunch(P->pexec[r & 1], w));
+        g_launches.fetch_add((int64_t)P->per_iter * POLL_ITERS, std::memory_order_relaxed);
+    }
+    CFEM_CUDA(cudaEventRecord(P->ev[1], w));
+    CFEM_CUDA(cudaStreamWaitEvent(s, P->ev[1], 0));
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_slots_poll(cfem_pcg_plan *P, cfem_solve_stats *stats) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(P && P->slots && stats, CFEM_ERR_INVALID, "cfem_pcg_slots_poll: bad args");
+    CFEM_TRY(set_device(P->device));
+    const int n = P->n_systems;
+    std::vector<SysState> hst(n);
+    int h_err = 0;
+    CFEM_CUDA(cudaMemcpyAsync(hst.data(), P->d_st, n * sizeof(SysState),
+                              cudaMemcpyDeviceToHost, P->w));
+    CFEM_CUDA(cudaMemcpyAsync(&h_err, &P->d_bar->err, sizeof(int), cudaMemcpyDeviceToHost, P->w));
+    CFEM_CUDA(cudaStreamSynchronize(P->w));
+    for (int i = 0; i < n; ++i) {
+        cfem_solve_stats &o = stats[i];
+        memset(&o, 0, sizeof(o));
+        o.status = hst[i].phase == PH_DONE ? hst[i].status : CFEM_SLOT_RUNNING;
+        o.iterations = hst[i].iter;
+        o.residual_updates = hst[i].nres;
+        o.relres = hst[i].relres;
+        o.bnorm = sqrt(hst[i].bb);
+    }
+    CFEM_CHECK(h_err != 2, CFEM_ERR_TIMEOUT,
+               "solver SpMV bulk-copy wait timed out (device wait bound reached)");
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_pcg_slots_release(cfem_pcg_plan *P, int32_t slot, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(P && P->slots && slot >= 0 && slot < P->n_systems, CFEM_ERR_INVALID,
+               "cfem_pcg_slots_release: bad args");
+    CFEM_TRY(set_device(P->device));
+    cudaStream_t s = (cudaStream_t)stream, w = P->w;
+    CFEM_CUDA(cudaEventRecord(P->ev[0], s));
+    CFEM_CUDA(cudaStreamWaitEvent(w, P->ev[0], 0));
+    CFEM_LAUNCH(k_slot_cancel, 1, 32, 0, w, P->d_st + slot, P->d_bar);
+    CFEM_CUDA(cudaEventRecord(P->ev[1], w));
+    CFEM_CUDA(cudaStreamWaitEvent(s, P->ev[1], 0));
+    return CFEM_OK;
     CFEM_API_END
 }
 

@@ -565,3 +565,81 @@ def csr_to_device(rt, A):
     return (torch.from_numpy(A.indptr.astype(np.int32)).to(dev),
             torch.from_numpy(A.indices.astype(np.int32)).to(dev),
             torch.from_numpy(A.data.astype(np.float64)).to(dev), A)
+
+
+class SlotEngine:
+    """Solve slots (``cfem_pcg_slots_*``): iteration-level continuous
+    batching. ``n_slots`` systems of one block size and precision, each of
+    at most ``max_rows`` block rows and ``max_nnzb`` stored blocks, iterate
+    together in rounds of 16 CG iterations on the engine's own stream; a
+    system assigned between rounds joins the running ones, and a finished
+    system frees its slot at once. Systems are BlockSystem objects whose
+    arrays stay alive while they are in a slot."""
+
+    def __init__(self, rt, n_slots, bs, mode, max_rows, max_nnzb):
+        self.rt = rt
+        self.n_slots = int(n_slots)
+        self.bs, self.mode = int(bs), int(mode)
+        self.max_rows, self.max_nnzb = int(max_rows), int(max_nnzb)
+        h = N._vp()
+        N.check(rt.lib.cfem_pcg_slots_create(rt.ctx, self.n_slots, self.bs, self.mode,
+                                             self.max_rows, self.max_nnzb, rt.stream(),
+                                             ctypes.byref(h)))
+        self.handle = h
+        self.free = list(range(self.n_slots))
+        self.busy = {}                       # slot -> (system, tag)
+        self._stats = (N.SolveStats * self.n_slots)()
+
+    def fits(self, system):
+        return (system.bs == self.bs and system.n_rows <= self.max_rows)
+
+    def assign(self, system, rtol, max_iter=None, tag=None):
+        """Put a system into a free slot (raises if none is free); returns it."""
+        if not self.free:
+            raise RuntimeError("no free solve slot")
+        mi = max_iter if max_iter is not None else max(
+            1000, 20 * int(np.sqrt(system.n_rows * system.bs)) + 2000)
+        ls = system.linsys(self.mode, rtol, mi)
+        slot = self.free[0]
+        N.check(self.rt.lib.cfem_pcg_slots_assign(self.handle, slot, ctypes.byref(ls),
+                                                  self.rt.stream()))
+        self.free.pop(0)
+        self.busy[slot] = (system, tag)
+        return slot
+
+    def run(self, rounds=1):
+        """Queue `rounds` rounds of 16 iterations over every slot."""
+        N.check(self.rt.lib.cfem_pcg_slots_run(self.handle, int(rounds), self.rt.stream()))
+
+    def poll(self):
+        """Wait for the queued rounds; returns [(system, tag, SolveResult)] of
+        the systems that finished (their slots are free again)."""
+        N.check(self.rt.lib.cfem_pcg_slots_poll(self.handle, self._stats))
+        done = []
+        for slot in sorted(self.busy):
+            st = self._stats[slot]
+            if st.status == N.CFEM_SLOT_RUNNING:
+                continue
+            system, tag = self.busy.pop(slot)
+            self.free.append(slot)
+            done.append((system, tag, SolveResult(st)))
+        self.free.sort()
+        return done
+
+    def release(self, slot):
+        N.check(self.rt.lib.cfem_pcg_slots_release(self.handle, int(slot), self.rt.stream()))
+        if slot in self.busy:
+            del self.busy[slot]
+            self.free.append(slot)
+            self.free.sort()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.rt.lib.cfem_pcg_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -1,40 +1,43 @@
-"""Request serving: continuous batching of heat and elasticity solves.
+"""Request serving: iteration-level continuous batching of heat and
+elasticity solves.
 
 The reference answers one call at a time on the host (``solve_tet_poisson``,
 ``solve_tet10_poisson``, ``solve_elasticity_tet10``). Here a server takes a
 stream of requests - each a mesh (host arrays, as a client would send them),
 its coefficients and boundary data - and keeps the GPU busy with them:
 
-* requests wait in a queue from their arrival time; a free worker takes the
-  oldest one together with other queued requests of the same kind and size
-  class (powers of two of the DOF count), up to a DOF cap per batch;
-* a batch is admitted only while the device memory it is expected to need
-  fits in the HBM budget next to the batches in flight (estimates from the
-  DOF and nonzero counts); otherwise it waits for memory to free up;
-* each worker thread has its own CUDA stream, so batches overlap on the
-  device; a batch is one batched assembly and one batched PCG launch
-  sequence (``cfem_assemble_batch`` / ``cfem_pcg_solve``);
+* requests wait in a queue from their arrival time; each (kind, size class)
+  - size classes are powers of two of the DOF count - has a slot engine
+  (``device.SlotEngine`` over ``cfem_pcg_slots_*``): a fixed set of solve
+  slots of that class's capacity whose systems iterate together in rounds
+  of 16 CG iterations on the engine's own stream;
+* between rounds the server admits the oldest waiting requests into free
+  slots (their matrices assembled and their solver state initialised while
+  the other slots keep their iterates), as long as the device memory they
+  are expected to need fits in the HBM budget next to everything in flight
+  (estimates from the DOF and nonzero counts); a request that finishes
+  frees its slot at once, whatever the others are doing;
+* the engines' rounds are queued on their own streams before any of them
+  is polled, so different classes overlap on the device;
 * meshes stay resident on the device between requests (connectivity,
   pattern, boundary masks), keyed by the mesh object.
 
-Every result is the solve of its own system: batching changes only which
-launch it shares, never the arithmetic of another system (per-system
-scalars, fixed-order reductions), so a request's answer in the mix equals
-its answer alone on the same scheduler, and stays within the solve tolerance
-of it otherwise.
+Every result is the solve of its own system: a slot's iterates depend only
+on its own system (per-system scalars, fixed-order reductions), so a
+request's answer in the mix is bitwise its answer alone on the same engine
+class, and within the solve tolerance of any other solve of it.
 """
 
 import threading
 import time
 from collections import deque
-from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
 from . import _native as N
 from ._driver import accept, solver_mode
 from .batch import BatchSolver, HeatProblem
-from .device import BlockSystem, DeviceMesh, fixed_mask, fixed_vector, pcg
+from .device import BlockSystem, DeviceMesh, SlotEngine, fixed_mask, fixed_vector, pcg
 
 KINDS = ("p1_heat", "t10_heat", "t10_elast")
 
@@ -98,9 +101,18 @@ class Request:
 
 
 class Server:
+    """A serving loop on one GPU.
+
+    hbm_budget: device bytes the server may have in flight (engines and
+    requests); precision / rtol: the solves' mode and relative residual;
+    rounds: rounds of 16 iterations between admission points. workers,
+    max_batch_dofs and max_batch only shape ``run_batch`` (one batched
+    assembly and solve of a list of requests, the non-streaming path).
+    """
+
     def __init__(self, device=None, hbm_budget=150e9, workers=3,
                  precision="mixed", rtol=1e-10, max_batch_dofs=8e6,
-                 max_batch=64):
+                 max_batch=64, rounds=1):
         import torch
         self.rt = N.runtime(device)
         self.torch = torch
@@ -113,6 +125,10 @@ class Server:
         self.solver = BatchSolver(self.rt.device)
         self._mesh_lock = threading.Lock()
         self._dms = {}
+        self.rounds = int(rounds)
+        self._mode = solver_mode(precision, rtol)[0]
+        self._engines = {}
+        self._engine_bytes = 0.0
 
     # -------------------------------------------------------------- batches
     def _device_mesh(self, mesh):
@@ -176,81 +192,157 @@ class Server:
             r.solve_s = res[0].kernel_ms * 1e-3 if res else 0.0
         return sols, res
 
-    # ---------------------------------------------------------------- loop
-    def _take_batch(self, queue, free_bytes):
-        """Oldest request plus same-kind, same-size-class followers."""
-        head = queue[0]
-        if head.bytes_estimate() > free_bytes:
-            return None
-        batch, dofs, used = [head], head.dofs, head.bytes_estimate()
-        cls = (head.kind, head.size_class())
-        for r in list(queue)[1:]:
-            if len(batch) >= self.max_batch:
-                break
-            if (r.kind, r.size_class()) != cls:
-                continue
-            b = r.bytes_estimate()
-            if dofs + r.dofs > self.max_batch_dofs or used + b > free_bytes:
-                continue
-            batch.append(r)
-            dofs += r.dofs
-            used += b
-        for r in batch:
-            queue.remove(r)
-        return batch, used
+    # ---------------------------------------------------------- slot engines
+    def _engine(self, kind, cls):
+        """The slot engine of a (kind, size class), created on first use."""
+        key = (kind, cls)
+        eng = self._engines.get(key)
+        if eng is None:
+            bs = 3 if kind == "t10_elast" else 1
+            max_rows = -(-(2 ** (cls + 1)) // bs)
+            per_row = SLOT_ROW_BLOCKS[kind]
+            eng = SlotEngine(self.rt, slots_for_class(cls), bs, self._mode,
+                             max_rows, max_rows * per_row)
+            self._engines[key] = eng
+            self._engine_bytes += engine_bytes(eng, self._mode)
+        return eng
+
+    def _system(self, r):
+        """Assemble request r on the device; returns its BlockSystem (the
+        arrays it needs are kept alive by the system's `keep`)."""
+        if r.kind == "t10_elast":
+            from .physics.elastic3d import _assemble
+            dm = self._device_mesh(r.mesh)
+            vals, rhs = _assemble(dm, r.mesh, N.OP_T10_ELAST, r.E, r.nu, None,
+                                  r.traction, None, 0.0, 0.0, tet10=True)
+            idx, v = fixed_vector(r.mesh, {c: (0.0, 0.0, 0.0) for c in r.clamp})
+            mask, x = fixed_mask(dm.rt, 3 * r.mesh.n_nodes, idx, v)
+            pat = dm.pattern
+            return BlockSystem(dm.rt, dm.n_nodes, 3, pat.row_ptr, pat.col, vals,
+                               rhs, x, mask, keep=(dm,))
+        with self._mesh_lock:
+            self.solver.device_mesh(r.mesh)
+            batch = self.solver.prepare([HeatProblem(r.mesh, k=r.k, f=r.f, bc=r.bc)])
+        batch.assemble()
+        it = batch.items[0]
+        dm, pat = it["dm"], it["dm"].pattern
+        return BlockSystem(self.rt, dm.n_nodes, 1, pat.row_ptr, pat.col, it["vals"],
+                           it["rhs"], it["x"], it["mask"], keep=(dm, batch))
 
     def serve(self, requests, realtime=True):
         """Run a request stream; returns a summary dict. Requests arrive at
         their arrival times (realtime) or all at once."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queue = []
-        inflight = {}
         in_use = 0.0
         t0 = time.perf_counter()
-        pool = ThreadPoolExecutor(max_workers=self.workers)
         errors = []
-        try:
-            while pending or queue or inflight:
-                now = time.perf_counter() - t0
-                while pending and (not realtime or pending[0].arrival <= now):
-                    queue.append(pending.popleft())
-                # collect finished batches
-                for fut in [f for f in inflight if f.done()]:
-                    reqs, used = inflight.pop(fut)
-                    in_use -= used
-                    t_done = time.perf_counter() - t0
+        while pending or queue or any(e.busy for e in self._engines.values()):
+            now = time.perf_counter() - t0
+            while pending and (not realtime or pending[0].arrival <= now):
+                queue.append(pending.popleft())
+            # admit the oldest waiting requests into free slots
+            budget = self.budget - self._engine_bytes - in_use
+            for r in admit(queue, self._free_slots, budget, self._slot_class):
+                eng = self._engine(r.kind, self._slot_class(r))
+                r.t_start = time.perf_counter() - t0
+                eng.assign(self._system(r), self.rtol, tag=r)
+                in_use += r.bytes_estimate()
+                queue.remove(r)
+            active = [e for e in self._engines.values() if e.busy]
+            for e in active:          # queue every engine's round first
+                e.run(self.rounds)
+            for e in active:
+                for system, r, res in e.poll():
+                    r.t_done = time.perf_counter() - t0
+                    in_use -= r.bytes_estimate()
+                    r.info = res
                     try:
-                        sols, res = fut.result()
-                    except Exception as exc:  # noqa: BLE001 - reported below
-                        errors.append((reqs, exc))
+                        accept(res, self.rtol, f"request {r.id}")
+                    except RuntimeError as exc:
+                        errors.append((r, exc))
                         continue
-                    for r, x, info in zip(reqs, sols, res):
-                        r.result, r.info, r.t_done = x, info, t_done
-                # admit new batches while workers and memory are free
-                while queue and len(inflight) < self.workers:
-                    got = self._take_batch(queue, self.budget - in_use)
-                    if got is None and not inflight:
-                        # larger than the whole budget: run it alone
-                        got = ([queue.pop(0)], 0.0)
-                    if got is None:
-                        break
-                    reqs, used = got
-                    start = time.perf_counter() - t0
-                    for r in reqs:
-                        r.t_start = start
-                    in_use += used
-                    inflight[pool.submit(self.run_batch, reqs)] = (reqs, used)
-                if not queue or len(inflight) >= self.workers:
-                    time.sleep(0.0005)
-                elif realtime and pending and not queue:
-                    time.sleep(min(0.0005, max(0.0, pending[0].arrival - now)))
-        finally:
-            pool.shutdown(wait=True)
+                    r.result = system.x.cpu().numpy()
+            if not active and not queue and pending and realtime:
+                time.sleep(min(0.0005, max(0.0, pending[0].arrival - now)))
         if errors:
-            reqs, exc = errors[0]
-            raise RuntimeError(f"batch of requests {[r.id for r in reqs]} "
-                               f"failed: {exc}") from exc
+            r, exc = errors[0]
+            raise RuntimeError(f"request {r.id} failed: {exc}") from exc
         return summarize(requests, time.perf_counter() - t0)
+
+    def _slot_class(self, r):
+        """The engine class of a request: its size class, or the next one up
+        when it would not fit (rows or stored blocks) the class's slots."""
+        cls = r.size_class()
+        bs = r.bs
+        rows = r.mesh.n_nodes
+        if rows > -(-(2 ** (cls + 1)) // bs) or r.nnz_estimate() // (bs * bs) > \
+                -(-(2 ** (cls + 1)) // bs) * SLOT_ROW_BLOCKS[r.kind]:
+            cls += 1
+        return cls
+
+    def _free_slots(self, kind, cls):
+        eng = self._engines.get((kind, cls))
+        return slots_for_class(cls) if eng is None else len(eng.free)
+
+    def solve_alone(self, r):
+        """The answer a request gets with nothing else in flight (a new
+        server of the same settings, the same slot engine class)."""
+        import copy
+        q = copy.copy(r)
+        q.result = q.info = q.t_start = q.t_done = None
+        q.arrival = 0.0
+        srv = Server(self.rt.device, self.budget, self.workers, self.precision,
+                     self.rtol, rounds=self.rounds)
+        srv.serve([q], realtime=False)
+        return q.result, q.info
+
+
+# Stored blocks per row a slot is sized for: P1 rows hold at most 15 entries
+# on box meshes, Tet10 rows 27-28 on average (vertex rows up to 65).
+SLOT_ROW_BLOCKS = {"p1_heat": 16, "t10_heat": 30, "t10_elast": 30}
+
+
+def slots_for_class(cls):
+    """Slots of an engine whose systems hold up to 2^(cls+1) DOFs: about 4 M
+    DOFs of capacity per engine, between 2 and 64 slots."""
+    return int(min(64, max(2, (1 << 22) >> (cls + 1))))
+
+
+def engine_bytes(eng, mode):
+    """Device bytes a slot engine holds: solver vectors, Jacobi inverse,
+    partial sums and the padded working copies of every slot."""
+    ts = 4 if mode == N.SOLVE_MIXED else 8
+    bs2 = eng.bs * eng.bs
+    nd = eng.max_rows * eng.bs
+    vec = 6 * nd * ts + nd * 8
+    if eng.bs == 1:
+        ne = eng.max_nnzb + 3 * eng.max_rows + 8
+        copies = ne * (4 + 8 + (4 if mode == N.SOLVE_MIXED else 0))
+    else:
+        copies = eng.max_nnzb * bs2 * ts
+    return eng.n_slots * (vec + copies)
+
+
+def admit(queue, free_slots, budget, slot_class):
+    """Requests of `queue` (oldest first) to put into solve slots now: each
+    needs a free slot of its (kind, slot class) - free_slots(kind, cls)
+    counts them - and its memory estimate within what is left of `budget`.
+    A request that does not fit waits; younger requests of other classes
+    may still go ahead of it."""
+    taken = {}
+    out = []
+    left = float(budget)
+    for r in queue:
+        key = (r.kind, slot_class(r))
+        free = free_slots(*key) - taken.get(key, 0)
+        b = r.bytes_estimate()
+        if free <= 0 or b > left:
+            continue
+        taken[key] = taken.get(key, 0) + 1
+        left -= b
+        out.append(r)
+    return out
 
 
 def free_dofs(req):
@@ -283,12 +375,8 @@ def summarize(requests, wall):
         "max_ms": float(lat.max() * 1e3) if lat.size else None,
         "by_kind": {k: {"requests": sum(1 for r in done if r.kind == k),
                         "solved_dofs": int(sum(free_dofs(r) for r in done if r.kind == k)),
-                        "batches": len({id(getattr(r, "t_start", None)) and (r.t_start, r.t_done)
-                                        for r in done if r.kind == k}),
-                        "worker_s": float(sum(getattr(r, "batch_s", 0.0) / max(getattr(r, "batch_size", 1), 1)
-                                              for r in done if r.kind == k)),
-                        "solve_device_s": float(sum(getattr(r, "solve_s", 0.0) / max(getattr(r, "batch_size", 1), 1)
-                                                    for r in done if r.kind == k)),
+                        "in_flight_s": float(sum(r.t_done - r.t_start for r in done
+                                                 if r.kind == k and r.t_start is not None)),
                         "iterations_max": int(max([r.info.iterations for r in done
                                                    if r.kind == k and r.info is not None] or [0]))}
                     for k in KINDS},

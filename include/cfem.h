@@ -44,7 +44,8 @@ enum {
     CFEM_ERR_NOT_CONVERGED = 4, /* iteration cap or stagnation               */
     CFEM_ERR_BREAKDOWN = 5,     /* p'Ap <= 0, singular block, non-finite     */
     CFEM_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up        */
-    CFEM_ERR_UNSUPPORTED = 7    /* device is not sm_100 / feature missing    */
+    CFEM_ERR_UNSUPPORTED = 7,   /* device is not sm_100 / feature missing    */
+    CFEM_SLOT_RUNNING = -1      /* cfem_pcg_slots_poll: still iterating      */
 };
 
 /* Element operators of cfem_assemble (values are block bs x bs per node pair). */
@@ -383,6 +384,34 @@ CFEM_API int cfem_pcg_plan_refresh(cfem_pcg_plan *plan, void *stream);
 CFEM_API int cfem_pcg_plan_solve(cfem_pcg_plan *plan, cfem_solve_stats *stats,
                                  void *stream);
 CFEM_API int cfem_pcg_plan_destroy(cfem_pcg_plan *plan);
+
+/* Solve slots: continuous batching at iteration level, for serving loops
+ * where systems arrive while others are being solved (the reference solves
+ * one call at a time and has no counterpart). A slot plan holds n_slots
+ * systems of one block size (1 or 3) and precision mode, each of at most
+ * max_rows block rows and max_nnzb stored blocks, with point Jacobi; its
+ * work lists, workspace and iteration graphs are fixed at creation. Assign
+ * puts a system into a free slot (its working copy built, its state reset,
+ * INIT run: it joins whatever is running), run queues `rounds` replays of
+ * 16 iterations over every slot on the plan's stream (idle slots cost an
+ * early exit), poll waits for the plan's stream and reports every slot
+ * (status CFEM_SLOT_RUNNING while a system iterates; a finished system keeps
+ * its status until the slot is assigned again), release ends a running
+ * system or frees a finished one. The caller keeps a system's arrays alive
+ * while it is in a slot and reads x after poll reports it finished. Each
+ * system's scalars and sums are its own, so its iterates do not depend on
+ * the other slots. Calls on one slot plan must come from one thread at a
+ * time; assign and poll synchronise (poll the plan's stream, assign the
+ * given stream), create synchronises, run and release do not. Destroy with
+ * cfem_pcg_plan_destroy. */
+CFEM_API int cfem_pcg_slots_create(cfem_ctx *ctx, int32_t n_slots, int32_t bs, int32_t mode,
+                                   int64_t max_rows, int64_t max_nnzb, void *stream,
+                                   cfem_pcg_plan **out);
+CFEM_API int cfem_pcg_slots_assign(cfem_pcg_plan *plan, int32_t slot, const cfem_linsys *system,
+                                   void *stream);
+CFEM_API int cfem_pcg_slots_run(cfem_pcg_plan *plan, int32_t rounds, void *stream);
+CFEM_API int cfem_pcg_slots_poll(cfem_pcg_plan *plan, cfem_solve_stats *stats);
+CFEM_API int cfem_pcg_slots_release(cfem_pcg_plan *plan, int32_t slot, void *stream);
 
 /* Jacobi-preconditioned COCG (CG with the unconjugated form x^T y) for one
  * complex symmetric CSR system (A^T = A), values and vectors interleaved

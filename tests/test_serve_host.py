@@ -5,14 +5,6 @@ import numpy as np
 from cloudfem_b200 import serve
 
 
-def _server(budget, max_batch_dofs=1e9, max_batch=64):
-    s = object.__new__(serve.Server)
-    s.budget = budget
-    s.max_batch_dofs = max_batch_dofs
-    s.max_batch = max_batch
-    return s
-
-
 def test_stream_is_seeded_and_mixed():
     a = serve.make_stream(60, seed=3, dof_range=(1e3, 2e4))
     b = serve.make_stream(60, seed=3, dof_range=(1e3, 2e4))
@@ -25,34 +17,43 @@ def test_stream_is_seeded_and_mixed():
         assert 200 <= r.dofs <= 2e5
 
 
-def test_batches_take_oldest_and_same_class():
+def _slot_class(r):
+    return r.size_class()
+
+
+def test_admission_takes_oldest_into_free_slots():
+    """Oldest first; each request needs a free slot of its own class;
+    requests of full classes wait while others go ahead."""
     reqs = serve.make_stream(40, seed=1, dof_range=(1e3, 2e4))
-    queue = list(reqs)
-    srv = _server(1e12)
-    batch, used = srv._take_batch(queue, 1e12)
-    assert batch[0] is reqs[0]
-    cls = (reqs[0].kind, reqs[0].size_class())
-    assert all((r.kind, r.size_class()) == cls for r in batch)
-    assert used == sum(r.bytes_estimate() for r in batch)
-    assert all(r not in queue for r in batch)
+    head = reqs[0]
+    key = (head.kind, head.size_class())
+    free = {key: 1}
+    out = serve.admit(list(reqs), lambda k, c: free.get((k, c), 0), 1e15, _slot_class)
+    assert out == [head]
+    same = [r for r in reqs if (r.kind, r.size_class()) == key]
+    free = {key: 3}
+    out = serve.admit(list(reqs), lambda k, c: free.get((k, c), 0), 1e15, _slot_class)
+    assert out == same[:3]
+    # every class open: everything goes, in arrival order
+    out = serve.admit(list(reqs), lambda k, c: 64, 1e15, _slot_class)
+    assert out == list(reqs)
 
 
 def test_admission_respects_memory_budget():
     reqs = serve.make_stream(40, seed=2, dof_range=(1e3, 2e4))
     head = reqs[0]
-    srv = _server(1e12)
-    # no room for the oldest request: nothing is admitted
-    assert srv._take_batch(list(reqs), head.bytes_estimate() - 1) is None
-    # room for exactly the oldest: it goes alone
-    batch, used = srv._take_batch(list(reqs), head.bytes_estimate())
-    assert batch == [head] and used == head.bytes_estimate()
+    slots = lambda k, c: 64  # noqa: E731
+    assert head not in serve.admit(list(reqs), slots, head.bytes_estimate() - 1, _slot_class)
+    out = serve.admit([head], slots, head.bytes_estimate(), _slot_class)
+    assert out == [head]
+    budget = sum(r.bytes_estimate() for r in reqs[:5])
+    out = serve.admit(list(reqs), slots, budget, _slot_class)
+    assert sum(r.bytes_estimate() for r in out) <= budget
 
 
-def test_batch_dof_cap():
-    reqs = serve.make_stream(80, seed=4, dof_range=(1e3, 4e3))
-    srv = _server(1e12, max_batch_dofs=3 * reqs[0].dofs)
-    batch, _ = srv._take_batch(list(reqs), 1e12)
-    assert sum(r.dofs for r in batch) <= 3 * reqs[0].dofs
+def test_slot_engine_sizes():
+    assert serve.slots_for_class(9) == 64 and serve.slots_for_class(20) == 2
+    assert all(2 <= serve.slots_for_class(c) <= 64 for c in range(6, 24))
 
 
 def test_stream_cap_keeps_the_full_streams_requests():
