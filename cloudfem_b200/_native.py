@@ -137,6 +137,7 @@ SIGNATURES = [
      [_vp, _i32, _i32, _i32, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
     ("cfem_pcg_slots_assign", ctypes.c_int, [_vp, _i32, ctypes.POINTER(LinSys), _vp]),
     ("cfem_pcg_slots_run", ctypes.c_int, [_vp, _i32, _vp]),
+    ("cfem_pcg_slots_ready", ctypes.c_int, [_vp]),
     ("cfem_pcg_slots_poll", ctypes.c_int, [_vp, ctypes.POINTER(SolveStats)]),
     ("cfem_pcg_slots_release", ctypes.c_int, [_vp, _i32, _vp]),
     ("cfem_pcg_solve_noalloc", ctypes.c_int,

@@ -3526,10 +3526,20 @@ extern "C" int cfem_pcg_slots_run(cfem_pcg_plan *P, int32_t rounds, void *stream
         CFEM_CUDA(cudaGraphLaunch(P->pexec[r & 1], w));
         g_launches.fetch_add((int64_t)P->per_iter * POLL_ITERS, std::memory_order_relaxed);
     }
+    // no wait on the caller's stream: new systems are assembled there while
+    // the rounds run; poll orders the host after them
     CFEM_CUDA(cudaEventRecord(P->ev[1], w));
-    CFEM_CUDA(cudaStreamWaitEvent(s, P->ev[1], 0));
     return CFEM_OK;
     CFEM_API_END
+}
+
+extern "C" int cfem_pcg_slots_ready(cfem_pcg_plan *P) {
+    CFEM_CHECK(P && P->slots, CFEM_ERR_INVALID, "cfem_pcg_slots_ready: not a slot plan");
+    CFEM_TRY(set_device(P->device));
+    const cudaError_t e = cudaEventQuery(P->ev[1]);
+    if (e == cudaErrorNotReady) return CFEM_SLOT_RUNNING;
+    CFEM_CUDA(e);
+    return CFEM_OK;
 }
 
 extern "C" int cfem_pcg_slots_poll(cfem_pcg_plan *P, cfem_solve_stats *stats) {

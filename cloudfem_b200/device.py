@@ -611,6 +611,14 @@ class SlotEngine:
         """Queue `rounds` rounds of 16 iterations over every slot."""
         N.check(self.rt.lib.cfem_pcg_slots_run(self.handle, int(rounds), self.rt.stream()))
 
+    def ready(self):
+        """True once the queued rounds have run (no wait)."""
+        st = self.rt.lib.cfem_pcg_slots_ready(self.handle)
+        if st == N.CFEM_SLOT_RUNNING:
+            return False
+        N.check(st)
+        return True
+
     def poll(self):
         """Wait for the queued rounds; returns [(system, tag, SolveResult)] of
         the systems that finished (their slots are free again)."""

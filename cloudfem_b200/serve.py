@@ -237,33 +237,48 @@ class Server:
         in_use = 0.0
         t0 = time.perf_counter()
         errors = []
-        while pending or queue or any(e.busy for e in self._engines.values()):
+        inflight = set()
+        while pending or queue or inflight or any(e.busy for e in self._engines.values()):
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
             # admit the oldest waiting requests into free slots
             budget = self.budget - self._engine_bytes - in_use
-            for r in admit(queue, self._free_slots, budget, self._slot_class):
+            chosen = admit(queue, self._free_slots, budget, self._slot_class)
+            if not chosen and queue and not inflight and \
+                    not any(e.busy for e in self._engines.values()):
+                chosen = [queue[0]]   # larger than the whole budget: alone
+            for r in chosen:
                 eng = self._engine(r.kind, self._slot_class(r))
                 r.t_start = time.perf_counter() - t0
                 eng.assign(self._system(r), self.rtol, tag=r)
                 in_use += r.bytes_estimate()
                 queue.remove(r)
-            active = [e for e in self._engines.values() if e.busy]
-            for e in active:          # queue every engine's round first
-                e.run(self.rounds)
-            for e in active:
-                for system, r, res in e.poll():
-                    r.t_done = time.perf_counter() - t0
-                    in_use -= r.bytes_estimate()
-                    r.info = res
-                    try:
-                        accept(res, self.rtol, f"request {r.id}")
-                    except RuntimeError as exc:
-                        errors.append((r, exc))
+            # engines whose round has run: collect their finished requests
+            # and queue the next round at once; an engine still running is
+            # left alone (no engine waits for another)
+            idle = True
+            for e in list(self._engines.values()):
+                if e in inflight:
+                    if not e.ready():
+                        idle = False
                         continue
-                    r.result = system.x.cpu().numpy()
-            if not active and not queue and pending and realtime:
+                    inflight.discard(e)
+                    for system, r, res in e.poll():
+                        r.t_done = time.perf_counter() - t0
+                        in_use -= r.bytes_estimate()
+                        r.info = res
+                        try:
+                            accept(res, self.rtol, f"request {r.id}")
+                        except RuntimeError as exc:
+                            errors.append((r, exc))
+                            continue
+                        r.result = system.x.cpu().numpy()
+                if e.busy:
+                    e.run(self.rounds)
+                    inflight.add(e)
+                    idle = False
+            if idle and not queue and pending and realtime:
                 time.sleep(min(0.0005, max(0.0, pending[0].arrival - now)))
         if errors:
             r, exc = errors[0]

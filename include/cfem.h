@@ -396,13 +396,16 @@ CFEM_API int cfem_pcg_plan_destroy(cfem_pcg_plan *plan);
  * 16 iterations over every slot on the plan's stream (idle slots cost an
  * early exit), poll waits for the plan's stream and reports every slot
  * (status CFEM_SLOT_RUNNING while a system iterates; a finished system keeps
- * its status until the slot is assigned again), release ends a running
- * system or frees a finished one. The caller keeps a system's arrays alive
+ * its status until the slot is assigned again), ready returns CFEM_OK once
+ * the queued rounds have run and CFEM_SLOT_RUNNING before (no wait), release
+ * ends a running system or frees a finished one. The caller keeps a system's arrays alive
  * while it is in a slot and reads x after poll reports it finished. Each
  * system's scalars and sums are its own, so its iterates do not depend on
  * the other slots. Calls on one slot plan must come from one thread at a
  * time; assign and poll synchronise (poll the plan's stream, assign the
- * given stream), create synchronises, run and release do not. Destroy with
+ * given stream), create synchronises, run, ready and release do not; run
+ * does not order the given stream after the rounds (poll does, for the
+ * host). Destroy with
  * cfem_pcg_plan_destroy. */
 CFEM_API int cfem_pcg_slots_create(cfem_ctx *ctx, int32_t n_slots, int32_t bs, int32_t mode,
                                    int64_t max_rows, int64_t max_nnzb, void *stream,
@@ -410,6 +413,7 @@ CFEM_API int cfem_pcg_slots_create(cfem_ctx *ctx, int32_t n_slots, int32_t bs, i
 CFEM_API int cfem_pcg_slots_assign(cfem_pcg_plan *plan, int32_t slot, const cfem_linsys *system,
                                    void *stream);
 CFEM_API int cfem_pcg_slots_run(cfem_pcg_plan *plan, int32_t rounds, void *stream);
+CFEM_API int cfem_pcg_slots_ready(cfem_pcg_plan *plan);
 CFEM_API int cfem_pcg_slots_poll(cfem_pcg_plan *plan, cfem_solve_stats *stats);
 CFEM_API int cfem_pcg_slots_release(cfem_pcg_plan *plan, int32_t slot, void *stream);
 

@@ -52,7 +52,7 @@ def test_request_joins_a_running_solve(torch):
     srv = serve.Server(precision="mixed", rtol=1e-10)
     assert srv._slot_class(slow) == srv._slot_class(fast)
     srv.serve([slow, fast], realtime=True)
-    assert slow.info.iterations > 10 * fast.info.iterations
+    assert slow.info.iterations > 3 * fast.info.iterations
     assert fast.t_start < slow.t_done           # admitted mid-solve
     assert fast.t_done < slow.t_done            # and done first
     assert len(srv._engines) == 1               # in the same slot engine
