@@ -104,14 +104,17 @@ class Server:
     """A serving loop on one GPU.
 
     hbm_budget: device bytes the server may have in flight (engines and
-    requests); precision / rtol: the solves' mode and relative residual;
+    requests); precision: "mixed", "fp64" or "auto" (default: mixed for
+    the heat kinds, FP64 for elasticity, where FP32 CG needs about 1.5x the
+    FP64 iterations on Tet10 cantilevers while its SpMV is only 1.3x faster);
+    rtol: the solves' relative residual;
     rounds: rounds of 16 iterations between admission points. workers,
     max_batch_dofs and max_batch only shape ``run_batch`` (one batched
     assembly and solve of a list of requests, the non-streaming path).
     """
 
     def __init__(self, device=None, hbm_budget=150e9, workers=3,
-                 precision="mixed", rtol=1e-10, max_batch_dofs=8e6,
+                 precision="auto", rtol=1e-10, max_batch_dofs=8e6,
                  max_batch=64, rounds=1):
         import torch
         self.rt = N.runtime(device)
@@ -126,7 +129,10 @@ class Server:
         self._mesh_lock = threading.Lock()
         self._dms = {}
         self.rounds = int(rounds)
-        self._mode = solver_mode(precision, rtol)[0]
+        self._prec = {k: (precision if precision != "auto" else
+                          ("fp64" if k == "t10_elast" else "mixed")) for k in KINDS}
+        for v in self._prec.values():
+            solver_mode(v, rtol)   # validates
         self._engines = {}
         self._engine_bytes = 0.0
 
@@ -152,12 +158,12 @@ class Server:
             self.torch.cuda.current_stream(self.rt.device).synchronize()
             batch = self.solver.prepare(probs)
         batch.assemble()
-        res = batch.solve(self.precision, rtol=self.rtol)
+        res = batch.solve(self._prec[reqs[0].kind], rtol=self.rtol)
         return batch.solutions(), res
 
     def _run_elast(self, reqs):
         from .physics.elastic3d import _assemble
-        mode, rtol = solver_mode(self.precision, self.rtol)
+        mode, rtol = solver_mode(self._prec["t10_elast"], self.rtol)
         systems, keep = [], []
         for r in reqs:
             dm = self._device_mesh(r.mesh)
@@ -201,10 +207,11 @@ class Server:
             bs = 3 if kind == "t10_elast" else 1
             max_rows = -(-(2 ** (cls + 1)) // bs)
             per_row = SLOT_ROW_BLOCKS[kind]
-            eng = SlotEngine(self.rt, slots_for_class(cls), bs, self._mode,
+            mode = solver_mode(self._prec[kind], self.rtol)[0]
+            eng = SlotEngine(self.rt, slots_for_class(cls), bs, mode,
                              max_rows, max_rows * per_row)
             self._engines[key] = eng
-            self._engine_bytes += engine_bytes(eng, self._mode)
+            self._engine_bytes += engine_bytes(eng, mode)
         return eng
 
     def _system(self, r):
@@ -319,9 +326,10 @@ SLOT_ROW_BLOCKS = {"p1_heat": 16, "t10_heat": 30, "t10_elast": 30}
 
 
 def slots_for_class(cls):
-    """Slots of an engine whose systems hold up to 2^(cls+1) DOFs: about 4 M
-    DOFs of capacity per engine, between 2 and 64 slots."""
-    return int(min(64, max(2, (1 << 22) >> (cls + 1))))
+    """Slots of an engine whose systems hold up to 2^(cls+1) DOFs: about 2 M
+    DOFs of capacity per engine (every round launches over all of it, idle
+    slots included), between 2 and 32 slots."""
+    return int(min(32, max(2, (1 << 21) >> (cls + 1))))
 
 
 def engine_bytes(eng, mode):
