@@ -1100,8 +1100,7 @@ def run_serving(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": float(np.mean([d["span_s"] for d in runs])) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"mixed": "f32 PCG + f64 residual/update", "fp64": "f64",
-                  "auto": "heat: f32 PCG + f64 residual/update; elasticity: f64"}[args.precision],
+        "dtype": "f32 PCG + f64 residual/update" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded Poisson request stream of box meshes)",
         "config": {
             "workload": f"serving_stream_{len(stream)}_requests_lambda200",
@@ -1185,10 +1184,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default=None, choices=["mixed", "fp64", "auto"],
+    ap.add_argument("--precision", default=None, choices=["mixed", "fp64"],
                     help="default: fp64 for the elasticity beam and the A-V transient, "
-                         "auto for serving (mixed heat, FP64 elasticity), mixed "
-                         "otherwise")
+                         "mixed otherwise")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="batched-heat",
                     choices=["elasticity", "batched-heat", "transient-heat", "serving",
@@ -1229,8 +1227,7 @@ def main():
     SPMV_STAGE = args.spmv_stage
     SELL_SORT = args.sell_sort
     if args.precision is None:
-        args.precision = ("fp64" if args.workload in ("elasticity", "av-transient") else
-                          "auto" if args.workload == "serving" else "mixed")
+        args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -104,17 +104,15 @@ class Server:
     """A serving loop on one GPU.
 
     hbm_budget: device bytes the server may have in flight (engines and
-    requests); precision: "mixed", "fp64" or "auto" (default: mixed for
-    the heat kinds, FP64 for elasticity, where FP32 CG needs about 1.5x the
-    FP64 iterations on Tet10 cantilevers while its SpMV is only 1.3x faster);
-    rtol: the solves' relative residual;
+    requests); precision / rtol: the solves' mode ("mixed" or "fp64") and
+    relative residual;
     rounds: rounds of 16 iterations between admission points. workers,
     max_batch_dofs and max_batch only shape ``run_batch`` (one batched
     assembly and solve of a list of requests, the non-streaming path).
     """
 
     def __init__(self, device=None, hbm_budget=150e9, workers=3,
-                 precision="auto", rtol=1e-10, max_batch_dofs=8e6,
+                 precision="mixed", rtol=1e-10, max_batch_dofs=8e6,
                  max_batch=64, rounds=1):
         import torch
         self.rt = N.runtime(device)
@@ -129,10 +127,8 @@ class Server:
         self._mesh_lock = threading.Lock()
         self._dms = {}
         self.rounds = int(rounds)
-        self._prec = {k: (precision if precision != "auto" else
-                          ("fp64" if k == "t10_elast" else "mixed")) for k in KINDS}
-        for v in self._prec.values():
-            solver_mode(v, rtol)   # validates
+        solver_mode(precision, rtol)   # validates
+        self._prec = {k: precision for k in KINDS}
         self._engines = {}
         self._engine_bytes = 0.0
 
@@ -326,10 +322,10 @@ SLOT_ROW_BLOCKS = {"p1_heat": 16, "t10_heat": 30, "t10_elast": 30}
 
 
 def slots_for_class(cls):
-    """Slots of an engine whose systems hold up to 2^(cls+1) DOFs: about 2 M
-    DOFs of capacity per engine (every round launches over all of it, idle
-    slots included), between 2 and 32 slots."""
-    return int(min(32, max(2, (1 << 21) >> (cls + 1))))
+    """Slots of an engine whose systems hold up to 2^(cls+1) DOFs: about 4 M
+    DOFs of capacity per engine (measured faster on the mixed stream than
+    2 M: fewer requests wait for a slot), between 2 and 64 slots."""
+    return int(min(64, max(2, (1 << 22) >> (cls + 1))))
 
 
 def engine_bytes(eng, mode):

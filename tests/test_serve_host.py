@@ -52,8 +52,8 @@ def test_admission_respects_memory_budget():
 
 
 def test_slot_engine_sizes():
-    assert serve.slots_for_class(9) == 32 and serve.slots_for_class(20) == 2
-    assert all(2 <= serve.slots_for_class(c) <= 32 for c in range(6, 24))
+    assert serve.slots_for_class(9) == 64 and serve.slots_for_class(20) == 2
+    assert all(2 <= serve.slots_for_class(c) <= 64 for c in range(6, 24))
 
 
 def test_stream_cap_keeps_the_full_streams_requests():
