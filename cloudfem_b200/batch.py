@@ -79,32 +79,91 @@ class BatchSolver:
             self.rt.device, non_blocking=True)
         return N.Coef(ptr(t), 0.0, mode, 0), t
 
+    def _dirichlet(self, dm, mesh, bc):
+        """Device mask and initial guess holding the Dirichlet values, cached
+        per mesh for constant-valued bc dicts; (mask, x0, free count)."""
+        import torch
+        key = None
+        if all(not callable(v) for v in (bc or {}).values()):
+            key = (id(mesh), tuple(sorted((k, float(v)) for k, v in (bc or {}).items())))
+            hit = self._fixed.get(key)
+            if hit is not None and hit[0] is mesh:
+                return hit[1:]
+        idx, v = fixed_scalar(mesh, bc)
+        mask = np.zeros(dm.n_nodes, dtype=np.uint8)
+        mask[idx] = 1
+        x0 = np.zeros(dm.n_nodes)
+        x0[idx] = v
+        out = (torch.from_numpy(mask).to(self.rt.device, non_blocking=True),
+               torch.from_numpy(x0).to(self.rt.device, non_blocking=True),
+               int(dm.n_nodes - len(idx)))
+        if key is not None:
+            self._fixed[key] = (mesh,) + out
+        return out
+
     def prepare(self, problems):
-        """Device inputs of every problem; returns a Batch."""
+        """Device inputs of every problem; returns a Batch. Per-element
+        coefficient arrays cross in one pinned copy; matrix values, loads and
+        solutions live in one allocation each."""
         import torch
         dev = self.rt.device
-        items, keep = [], []
-        for pb in problems:
-            dm = self.device_mesh(pb.mesh)
-            kc, t1 = self._coef(dm, pb.k)
-            fc, t2 = self._coef(dm, pb.f)
-            keep += [t1, t2]
-            idx, v = fixed_scalar(pb.mesh, pb.bc)
-            mask = np.zeros(dm.n_nodes, dtype=np.uint8)
-            mask[idx] = 1
-            x0 = np.zeros(dm.n_nodes)
-            x0[idx] = v
-            item = {
-                "dm": dm, "coef": kc, "load": fc,
-                "vals": torch.empty(dm.pattern.nnz, dtype=torch.float64, device=dev),
-                "rhs": torch.empty(dm.n_nodes, dtype=torch.float64, device=dev),
-                "mask": torch.from_numpy(mask).to(dev, non_blocking=True),
-                "x0": torch.from_numpy(x0).to(dev, non_blocking=True),
-                "free": int(dm.n_nodes - len(idx)),
-            }
-            item["x"] = item["x0"].clone()
-            items.append(item)
-        return Batch(self, items, keep)
+        dms = [self.device_mesh(pb.mesh) for pb in problems]
+        packed = []
+        for i, (pb, dm) in enumerate(zip(problems, dms)):
+            for which in ("k", "f"):
+                spec = getattr(pb, which)
+                if isinstance(spec, np.ndarray):
+                    a = np.ascontiguousarray(spec, dtype=float)
+                    if a.shape != (dm.n_elems,):
+                        raise ValueError(f"per-element array needs {dm.n_elems} "
+                                         f"values, got {a.shape}")
+                    packed.append((i, which, a))
+        keep = []
+        dev_arrays = {}
+        total = sum(a.size for _, _, a in packed)
+        if total:
+            host = torch.empty(total, dtype=torch.float64, pin_memory=True)
+            hv = host.numpy()
+            off, offs = 0, []
+            for _, _, a in packed:
+                hv[off:off + a.size] = a
+                offs.append(off)
+                off += a.size
+            dbuf = host.to(dev, non_blocking=True)
+            keep += [host, dbuf]
+            for (i, which, a), o in zip(packed, offs):
+                dev_arrays[(i, which)] = dbuf[o:o + a.size]
+        nnz = [dm.pattern.nnz for dm in dms]
+        nn = [dm.n_nodes for dm in dms]
+        vals_all = torch.empty(max(sum(nnz), 1), dtype=torch.float64, device=dev)
+        rhs_all = torch.empty(max(sum(nn), 1), dtype=torch.float64, device=dev)
+        fixed = [self._dirichlet(dm, pb.mesh, pb.bc) for pb, dm in zip(problems, dms)]
+        x0_all = torch.cat([f[1] for f in fixed]) if fixed else rhs_all[:0]
+        x_all = x0_all.clone()
+        items = []
+        ov = on = 0
+        for i, (pb, dm) in enumerate(zip(problems, dms)):
+            coefs = []
+            for which in ("k", "f"):
+                t = dev_arrays.get((i, which))
+                if t is not None:
+                    coefs.append(N.Coef(ptr(t), 0.0, N.COEF_ELEM, 0))
+                else:
+                    c, t2 = self._coef(dm, getattr(pb, which))
+                    keep.append(t2)
+                    coefs.append(c)
+            mask, x0, free = fixed[i]
+            items.append({
+                "dm": dm, "coef": coefs[0], "load": coefs[1],
+                "vals": vals_all[ov:ov + nnz[i]], "rhs": rhs_all[on:on + nn[i]],
+                "mask": mask, "x0": x0_all[on:on + nn[i]], "x": x_all[on:on + nn[i]],
+                "free": free,
+            })
+            ov += nnz[i]
+            on += nn[i]
+        batch = Batch(self, items, keep)
+        batch.x_all, batch.x0_all = x_all, x0_all
+        return batch
 
 
 class Batch:
@@ -138,8 +197,11 @@ class Batch:
         """One batched PCG over every problem; returns SolveResult list."""
         mode, rtol = solver_mode(precision, rtol)
         systems = []
+        x_all = getattr(self, "x_all", None)
+        if fresh and x_all is not None:
+            x_all.copy_(self.x0_all)
         for it in self.items:
-            if fresh:
+            if fresh and x_all is None:
                 it["x"].copy_(it["x0"])
             dm = it["dm"]
             pat = dm.pattern
@@ -153,7 +215,17 @@ class Batch:
         return self.results
 
     def solutions(self):
-        return [it["x"].cpu().numpy() for it in self.items]
+        """Host copies of every problem's solution (one device-to-host copy)."""
+        x_all = getattr(self, "x_all", None)
+        if x_all is None:
+            return [it["x"].cpu().numpy() for it in self.items]
+        h = x_all.cpu().numpy()
+        out, o = [], 0
+        for it in self.items:
+            n = it["dm"].n_nodes
+            out.append(h[o:o + n].copy())
+            o += n
+        return out
 
 
 def solve_batch(problems, precision="mixed", rtol=None, max_iter=None,
