@@ -202,10 +202,18 @@ class DeviceMesh:
 
     # ------------------------------------------------------ coefficients
     def coef(self, spec, where):
-        """cfem_coef for a float/callable sampled at 'centroid' or 'qp'.
+        """cfem_coef for a float/callable sampled at 'centroid' or 'qp', or
+        a per-element array (constant over each element).
 
         Returns (struct, keepalive) - the tensor must outlive the launch.
         """
+        if isinstance(spec, np.ndarray):
+            a = np.ascontiguousarray(spec, dtype=float)
+            if a.shape != (self.n_elems,):
+                raise ValueError(f"per-element array needs {self.n_elems} values, "
+                                 f"got {a.shape}")
+            t = _torch().from_numpy(a).to(self.rt.device)
+            return N.Coef(ptr(t), 0.0, N.COEF_ELEM, 0), t
         if not callable(spec):
             return N.Coef(None, float(spec), N.COEF_CONST, 0), None
         if where == "qp":

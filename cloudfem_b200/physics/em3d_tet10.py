@@ -59,8 +59,11 @@ __all__ = ["assemble_tet10_av", "solve_eddy_current_tet10",
 
 
 def _element_values(mesh, q):
-    """Float or callable(x, y, z) at element centroids, (M,) float."""
+    """Float or callable(x, y, z) at element centroids, or a per-element
+    array as it is, (M,) float."""
     els = np.asarray(mesh.elements)
+    if isinstance(q, np.ndarray) and q.shape == (len(els),):
+        return np.asarray(q, dtype=float).copy()
     v = evaluate(q, centroids(np.asarray(mesh.nodes, dtype=float), els))
     return np.full(len(els), float(v)) if np.isscalar(v) else np.asarray(v, dtype=float)
 
@@ -481,6 +484,50 @@ def _as_fn(q):
     return q if callable(q) else (lambda x, y, z, _q=q: _q)
 
 
+def _picard(mesh, M, Gs, S, v_nodes, sigma, omega, B_applied, J_s, boundary,
+            a_bc, permc_spec, iron_mask, nu_e, mu_target, tol, max_iter, relax,
+            rtol, cocg_max_iter):
+    """The secant Picard loop shared by the nonlinear phasor solvers
+    (em3d_tet10.py:914-967, induction3d_tet10.py:336-371): K rebuilt on the
+    device from nu_e (updated in place), a device COCG phasor solve warm-
+    started from the previous iterate, centroid |B|, the exact Joule power,
+    and nu of the iron elements relaxed towards 1 / (mu0 mu_target(|H|)).
+    Returns (a, v, B, Q, iterations, converged, rel_dB, P, cocg iterations)."""
+    dm = DeviceMesh(mesh)
+    js_rhs = _js_load(mesh, dm, J_s) if J_s is not None else None
+    sel = iron_mask if iron_mask.any() else slice(None)
+    hist_rel, hist_P, cocg_iters = [], [], []
+    B_prev = None
+    converged = False
+    a = v = B = Q = None
+    it = 0
+    for it in range(1, max_iter + 1):
+        K = _curl_curl(dm, nu_e)
+        a, v = _solve_phasor_with_K_tet10(
+            mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s, boundary, a_bc,
+            permc_spec, rtol=rtol, max_iter=cocg_max_iter, dm=dm, js_rhs=js_rhs,
+            x0=None if a is None else (a, v))
+        cocg_iters.append(_last_info["iterations"])
+        B = element_flux_density_tet10(mesh, a)
+        B_amp = np.sqrt(np.sum(np.abs(B) ** 2, axis=1))
+        P, Q = total_joule_power_tet10(mesh, a, v, sigma, omega)
+        hist_P.append(P)
+        if B_prev is not None:
+            denom = max(float(np.linalg.norm(B_amp[sel])), 1e-300)
+            rel = float(np.linalg.norm(B_amp[sel] - B_prev[sel]) / denom)
+            hist_rel.append(rel)
+            if rel < tol:
+                converged = True
+                break
+        if it == max_iter:
+            break
+        B_prev = B_amp
+        if iron_mask.any():
+            nu_t = 1.0 / (MU0 * mu_target(B_amp[iron_mask] * nu_e[iron_mask]))
+            nu_e[iron_mask] = (1.0 - relax) * nu_e[iron_mask] + relax * nu_t
+    return a, v, B, Q, it, converged, hist_rel, hist_P, cocg_iters
+
+
 def solve_eddy_current_nonlinear_tet10(mesh, nu=1.0 / MU0, sigma=0.0, omega=0.0,
                                        B_applied=None, J_s=None, boundary=None,
                                        a_bc=None, gauge_eps=1e-6, permc_spec=None,
@@ -526,39 +573,13 @@ def solve_eddy_current_nonlinear_tet10(mesh, nu=1.0 / MU0, sigma=0.0, omega=0.0,
     mu_r0 = (1.0 + float(mu_mag0)) if mu_init is None else float(mu_init)
     nu_e[iron_mask] = 1.0 / (MU0 * mu_r0)
 
-    dm = DeviceMesh(mesh)
-    js_rhs = _js_load(mesh, dm, J_s) if J_s is not None else None
-    sel = iron_mask if iron_mask.any() else slice(None)
-    hist_rel, hist_P, cocg_iters = [], [], []
-    B_prev = None
-    converged = False
-    a = v = B = None
-    it = 0
-    for it in range(1, max_iter + 1):
-        K = _curl_curl(dm, nu_e)
-        a, v = _solve_phasor_with_K_tet10(
-            mesh, K, M, Gs, S, v_nodes, omega, B_applied, J_s, boundary, a_bc,
-            permc_spec, rtol=rtol, max_iter=cocg_max_iter, dm=dm, js_rhs=js_rhs,
-            x0=None if a is None else (a, v))
-        cocg_iters.append(_last_info["iterations"])
-        B = element_flux_density_tet10(mesh, a)
-        B_amp = np.sqrt(np.sum(np.abs(B) ** 2, axis=1))
-        hist_P.append(total_joule_power_tet10(mesh, a, v, sigma, omega)[0])
-        if B_prev is not None:
-            denom = max(float(np.linalg.norm(B_amp[sel])), 1e-300)
-            rel = float(np.linalg.norm(B_amp[sel] - B_prev[sel]) / denom)
-            hist_rel.append(rel)
-            if rel < tol:
-                converged = True
-                break
-        if it == max_iter:
-            break
-        B_prev = B_amp
-        if iron_mask.any():
-            mu_t = bh_secant_mu_r(B_amp[iron_mask] * nu_e[iron_mask], bsat=bsat,
-                                  mu_mag0=mu_mag0)
-            nu_e[iron_mask] = ((1.0 - relax) * nu_e[iron_mask]
-                               + relax / (MU0 * mu_t))
+    def mu_target(H_amp):
+        return bh_secant_mu_r(H_amp, bsat=bsat, mu_mag0=mu_mag0)
+
+    a, v, B, Q, it, converged, hist_rel, hist_P, cocg_iters = _picard(
+        mesh, M, Gs, S, v_nodes, sigma, omega, B_applied, J_s, boundary, a_bc,
+        permc_spec, iron_mask, nu_e, mu_target, tol, max_iter, relax, rtol,
+        cocg_max_iter)
     info = {"iterations": it, "converged": converged,
             "rel_dB": np.array(hist_rel), "P": np.array(hist_P),
             "mu_r_elem": 1.0 / (MU0 * nu_e), "nu_elem": nu_e.copy(),

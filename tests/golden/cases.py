@@ -181,3 +181,19 @@ def avn_iron(x, y, z):
 
 # B-H curve sample points [A/m], including the small-h series branch
 BH_H = np.array([0.0, 1e-9, 1.0, 30.0, 500.0, 3e3, 2e4, 1e5, 1e6])
+
+
+# staggered EM -> heat induction heating of a steel block (x < 0.5) in a
+# background field: two EM intervals of two heat steps each; the second
+# case adds the temperature-dependent capacity and a second stagger pass
+IND_N = 3
+IND_KW = dict(omega=2.0 * np.pi * 50.0, B_applied=(0.0, 0.0, 1.5),
+              boundary=list(FACES), T0=20.0, t_end=0.04, dt=0.01, em_every=2,
+              k_th=30.0, rho_cp=3.768e6, method="be", em_tol=1e-3,
+              em_max_iter=40, em_relax=0.8)
+IND_KW2 = dict(IND_KW, method="cn", stagger_iter=2, cp_slope=1e-3,
+               cp_peak_h=2e6, cp_peak_w=25.0)
+
+
+def ind_iron(x, y, z):
+    return x < 0.5

@@ -234,6 +234,26 @@ def main(ref_path):
     put("avn_mu_r", info["mu_r_elem"])
     put("avn_B", info["B_elem"])
 
+    # ---------------- induction heating (EM -> heat, staggered) ----------------
+    from cloudfem.physics import induction3d_tet10 as ind
+    mi = box_mesh_tet10(C.IND_N, C.IND_N, C.IND_N)
+    for tag, kw in (("ind", C.IND_KW), ("ind2", C.IND_KW2)):
+        res = ind.induction_heating_3d_tet10(mi, iron=C.ind_iron, **kw)
+        put(tag + "_times", res["times"])
+        put(tag + "_T_hist", res["T_hist"])
+        put(tag + "_P", np.array([h["P"] for h in res["history"]]))
+        put(tag + "_em_iterations", np.array([h["em_iterations"] for h in res["history"]]))
+        put(tag + "_E_in", np.array(res["E_in"]))
+        put(tag + "_balance_rel", np.array(res["balance_rel"]))
+        put(tag + "_enthalpy_gain", np.array(res["enthalpy_gain"]))
+        put(tag + "_mu_r_iron", res["history"][-1]["mu_r_iron"])
+    Tt = 20.0 + 900.0 * np.linspace(0.0, 1.0, 9)
+    put("law_sigma", ind.steel_sigma_T(Tt))
+    put("law_step", ind.curie_step_T(Tt))
+    put("law_mu_HT", ind.bh_secant_mu_r_HT(C.BH_H, Tt))
+    put("law_cp", ind.steel_cp_T(Tt, cp_slope=1e-3, cp_peak_h=2e6))
+    put("law_H", ind.steel_enthalpy_T(Tt, cp_slope=1e-3, cp_peak_h=2e6))
+
     # ---------------- Tet10 A-V transient (theta method, LU) ----------------
     mt = box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)
     res = em.transient_eddy_current_tet10(

@@ -38,3 +38,14 @@ def test_bh_curve_matches_reference(golden):
     assert_close(em.bh_secant_mu_r(C.BH_H, bsat=1.2, mu_mag0=50.0),
                  golden["bh_mu_r_soft"], 1e-15, "mu_r soft")
     assert np.array_equal(em.bh_secant_mu_r(C.BH_H, mu_mag0=0.0), np.ones(len(C.BH_H)))
+
+
+def test_induction_material_laws_match_reference(golden):
+    from cloudfem_b200.physics import induction3d_tet10 as ind
+    Tt = 20.0 + 900.0 * np.linspace(0.0, 1.0, 9)
+    assert_close(ind.steel_sigma_T(Tt), golden["law_sigma"], 1e-15, "sigma(T)")
+    assert_close(ind.curie_step_T(Tt), golden["law_step"], 1e-15, "Curie step")
+    assert_close(ind.bh_secant_mu_r_HT(C.BH_H, Tt), golden["law_mu_HT"], 1e-15, "mu_r(H, T)")
+    assert_close(ind.steel_cp_T(Tt, cp_slope=1e-3, cp_peak_h=2e6), golden["law_cp"], 1e-15, "cp(T)")
+    assert_close(ind.steel_enthalpy_T(Tt, cp_slope=1e-3, cp_peak_h=2e6), golden["law_H"],
+                 1e-14, "H(T)")

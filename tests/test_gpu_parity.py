@@ -306,3 +306,24 @@ def test_av_nonlinear_picard_golden(cf, golden):
     assert_close(info["mu_r_elem"], g["avn_mu_r"], tol, "mu_r")
     assert_close(np.abs(info["B_elem"]), np.abs(g["avn_B"]), tol, "|B|")
     assert np.abs(info["rel_dB"] - g["avn_rel_dB"]).max() <= 1e-6 * g["avn_rel_dB"].max()
+
+
+@pytest.mark.parametrize("tag", ["ind", "ind2"])
+def test_induction_heating_golden(cf, golden, tag):
+    """Staggered EM -> heat induction heating (device Picard A-V solves and
+    device heat march) against the reference's SuperLU/LU chain: constant
+    capacity with backward Euler, and T-dependent capacity with Crank-
+    Nicolson and two stagger passes per interval."""
+    from cloudfem_b200.physics import induction3d_tet10 as ind
+    g = golden
+    kw = dict(C.IND_KW if tag == "ind" else C.IND_KW2)
+    m = cf.mesh.box_mesh_tet10(C.IND_N, C.IND_N, C.IND_N)
+    res = ind.induction_heating_3d_tet10(m, iron=C.ind_iron, **kw)
+    np.testing.assert_array_equal(res["times"], g[tag + "_times"])
+    assert [h["em_iterations"] for h in res["history"]] == list(g[tag + "_em_iterations"])
+    tol = 1e-8
+    assert_close(res["T_hist"], g[tag + "_T_hist"], tol, "temperatures")
+    assert_close([h["P"] for h in res["history"]], g[tag + "_P"], tol, "power")
+    assert abs(res["E_in"] - float(g[tag + "_E_in"])) <= tol * float(g[tag + "_E_in"])
+    assert abs(res["balance_rel"]) <= 1e-9
+    assert_close(res["history"][-1]["mu_r_iron"], g[tag + "_mu_r_iron"], tol, "mu_r")
