@@ -579,8 +579,9 @@ def run_batched_heat(args, rank, world, local_rank):
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
             "launch_ms": spmv_ms,
-            "traffic": _profiled_traffic("k_gxs_batched_tet10_heat",
-                                         "fp32" if args.precision == "mixed" else "fp64"),
+            "traffic": (_profiled_traffic("k_gxs_batched_tet10_heat", "fp32")
+                        if args.precision == "mixed" else
+                        _profiled_traffic("k_gxl_batched_tet10_heat_fp64", "fp64")),
         }
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_batched_heat(ns, ks)
