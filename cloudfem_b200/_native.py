@@ -112,6 +112,8 @@ SIGNATURES = [
       ctypes.POINTER(Coef), _f64, _f64, _vp, _vp, _i32, _vp]),
     ("cfem_face_candidates", ctypes.c_int,
      [_vp, _vp, _i64, _i32, _i32, _vp, _i64, _vp, ctypes.POINTER(_i64), _vp]),
+    ("cfem_face_exterior", ctypes.c_int,
+     [_vp, _vp, _i32, _i32, _vp, _i64, _i64, _vp, _vp, ctypes.POINTER(_i64), _vp]),
     ("cfem_axpby", ctypes.c_int, [_vp, _i64, _f64, _vp, _f64, _vp, _vp, _vp]),
     ("cfem_csr_add_subset", ctypes.c_int,
      [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),

@@ -181,6 +181,75 @@ __global__ void k_face_flags(const int32_t *__restrict__ elems,
     }
 }
 
+// Local face tables: corners (tet_heat.py:112, tet10.py:287-292) and, for
+// Tet10, the midside nodes of the three face edges in corner order.
+__device__ __forceinline__ int face_corner(int faces10, int f, int v) {
+    const int f4[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    const int f10[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    return faces10 ? f10[f][v] : f4[f][v];
+}
+__device__ __forceinline__ int face_mid(int f, int v) {
+    const int m10[4][3] = {{4, 5, 6}, {7, 8, 4}, {6, 9, 7}, {8, 9, 5}};
+    return m10[f][v];
+}
+
+// Sort keys of candidate faces: (min, mid) of the corner triple packed as
+// min * n_nodes + mid, and max; value = the candidate's position.
+__global__ void k_face_keys(const int32_t *__restrict__ elems, int npe, int faces10,
+                            const int64_t *__restrict__ cand, int64_t n, int64_t n_nodes,
+                            uint64_t *__restrict__ lo, uint32_t *__restrict__ hi,
+                            int32_t *__restrict__ pos) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = cand[i] >> 2;
+        const int f = (int)(cand[i] & 3);
+        int64_t c[3];
+        for (int v = 0; v < 3; ++v) c[v] = elems[e * npe + face_corner(faces10, f, v)];
+        int64_t a = min(c[0], min(c[1], c[2])), z = max(c[0], max(c[1], c[2]));
+        int64_t m = c[0] + c[1] + c[2] - a - z;
+        lo[i] = (uint64_t)a * (uint64_t)n_nodes + (uint64_t)m;
+        hi[i] = (uint32_t)z;
+        pos[i] = (int32_t)i;
+    }
+}
+
+template <typename K>
+__global__ void k_gather_key(const K *__restrict__ in, const int32_t *__restrict__ pos,
+                             int64_t n, K *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[pos[i]];
+}
+
+// In sorted order, a key that differs from both neighbours occurs once:
+// flag its candidate position.
+__global__ void k_face_once(const uint64_t *__restrict__ lo, const uint32_t *__restrict__ hi,
+                            const int32_t *__restrict__ pos, int64_t n,
+                            uint8_t *__restrict__ keep) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const bool prev = i > 0 && lo[i - 1] == lo[i] && hi[i - 1] == hi[i];
+        const bool next = i + 1 < n && lo[i + 1] == lo[i] && hi[i + 1] == hi[i];
+        keep[pos[i]] = (!prev && !next) ? 1 : 0;
+    }
+}
+
+// Node lists of the kept faces: 3 corners (P1) or 3 corners + 3 midsides.
+__global__ void k_face_nodes(const int32_t *__restrict__ elems, int npe, int faces10,
+                             const int64_t *__restrict__ ids, int64_t n,
+                             int64_t *__restrict__ out) {
+    const int width = faces10 ? 6 : 3;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = ids[i] >> 2;
+        const int f = (int)(ids[i] & 3);
+        for (int v = 0; v < 3; ++v)
+            out[i * width + v] = elems[e * npe + face_corner(faces10, f, v)];
+        if (faces10)
+            for (int v = 0; v < 3; ++v) out[i * width + 3 + v] = elems[e * npe + face_mid(f, v)];
+    }
+}
+
 static int bits_for(uint64_t maxval) {
     int b = 1;
     while (b < 64 && (maxval >> b) != 0) ++b;
@@ -422,6 +491,71 @@ int cfem_face_candidates(cfem_ctx *ctx, const int32_t *d_elems,
     tmp_free(flags, s);
     tmp_free(cnt, s);
     CFEM_CUDA(cudaStreamSynchronize(s));
+    *n_out = h_cnt;
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+int cfem_face_exterior(cfem_ctx *ctx, const int32_t *d_elems, int32_t npe, int32_t faces10,
+                       const int64_t *d_cand, int64_t n_cand, int64_t n_nodes,
+                       int64_t *d_ids, int64_t *d_nodes, int64_t *n_out, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && d_elems && d_ids && d_nodes && n_out && (npe == 4 || npe == 10) &&
+                   (faces10 == 0 || npe == 10) && n_cand >= 0 && n_cand < ((int64_t)1 << 31) &&
+                   n_nodes > 0 && n_nodes < ((int64_t)1 << 32),
+               CFEM_ERR_INVALID, "cfem_face_exterior: bad args");
+    *n_out = 0;
+    if (n_cand == 0) return CFEM_OK;
+    CFEM_CHECK(d_cand, CFEM_ERR_INVALID, "cfem_face_exterior: no candidates");
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = n_cand;
+    uint64_t *lo = nullptr, *lo2 = nullptr;
+    uint32_t *hi = nullptr, *hi2 = nullptr;
+    int32_t *pos = nullptr, *pos2 = nullptr;
+    uint8_t *keep = nullptr;
+    int64_t *cnt = nullptr;
+    CFEM_TRY(tmp_alloc(&lo, n, s));
+    CFEM_TRY(tmp_alloc(&lo2, n, s));
+    CFEM_TRY(tmp_alloc(&hi, n, s));
+    CFEM_TRY(tmp_alloc(&hi2, n, s));
+    CFEM_TRY(tmp_alloc(&pos, n, s));
+    CFEM_TRY(tmp_alloc(&pos2, n, s));
+    CFEM_TRY(tmp_alloc(&keep, n, s));
+    CFEM_TRY(tmp_alloc(&cnt, 1, s));
+    unsigned g = grid_for(n, 256);
+    if (g > (unsigned)ctx->num_sms * 32) g = ctx->num_sms * 32;
+    CFEM_LAUNCH(k_face_keys, g, 256, 0, s, d_elems, npe, faces10, d_cand, n, n_nodes, lo, hi,
+                pos);
+    // lexicographic (min, mid, max) with ties in candidate order: a stable
+    // sort by max, then a stable sort by (min, mid)
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    CFEM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, hi, hi2, pos, pos2, (int)n, 0,
+                                              bits_for(n_nodes), s));
+    CFEM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, lo2, lo, pos2, pos, (int)n, 0,
+                                              bits_for((uint64_t)n_nodes * n_nodes), s));
+    CFEM_CUDA(cub::DeviceSelect::Flagged(nullptr, b3, d_cand, keep, d_ids, cnt, n, s));
+    char *tmp = nullptr;
+    CFEM_TRY(tmp_alloc(&tmp, std::max(b1, std::max(b2, b3)), s));
+    CFEM_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b1, hi, hi2, pos, pos2, (int)n, 0,
+                                              bits_for(n_nodes), s));
+    CFEM_LAUNCH(k_gather_key<uint64_t>, g, 256, 0, s, lo, pos2, n, lo2);
+    CFEM_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b2, lo2, lo, pos2, pos, (int)n, 0,
+                                              bits_for((uint64_t)n_nodes * n_nodes), s));
+    // hi in the final order: hi2 is sorted by max with pos2; gather by pos
+    CFEM_LAUNCH(k_gather_key<uint32_t>, g, 256, 0, s, hi, pos, n, hi2);
+    CFEM_LAUNCH(k_face_once, g, 256, 0, s, lo, hi2, pos, n, keep);
+    CFEM_CUDA(cub::DeviceSelect::Flagged(tmp, b3, d_cand, keep, d_ids, cnt, n, s));
+    g_launches.fetch_add(4, std::memory_order_relaxed);
+    int64_t h_cnt = 0;
+    CFEM_CUDA(cudaMemcpyAsync(&h_cnt, cnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CFEM_CUDA(cudaStreamSynchronize(s));
+    if (h_cnt > 0)
+        CFEM_LAUNCH(k_face_nodes, grid_for(h_cnt, 256), 256, 0, s, d_elems, npe, faces10, d_ids,
+                    h_cnt, d_nodes);
+    for (void *q : {(void *)lo, (void *)lo2, (void *)hi, (void *)hi2, (void *)pos, (void *)pos2,
+                    (void *)keep, (void *)cnt, (void *)tmp})
+        tmp_free(q, s);
     *n_out = h_cnt;
     return CFEM_OK;
     CFEM_API_END

@@ -323,9 +323,12 @@ class DeviceMesh:
 
         Faces whose key (sorted corner triple) occurs once among all element
         faces and whose corners are all in the set, listed at their first
-        occurrence in element order (tet_heat.py:97-120, tet10.py:329-352).
-        Only faces with all corners in the set can share a key with such a
-        face, so counting among the device-selected candidates is exact.
+        occurrence in element order (tet_heat.py:97-120, tet10.py:329-352):
+        candidates flagged and compacted on the device
+        (cfem_face_candidates), the once-only count and the node lists on
+        the device too (cfem_face_exterior). Only faces with all corners in
+        the set can share a key with such a face, so counting among the
+        candidates is exact.
         """
         torch = _torch()
         host = self.host
@@ -343,34 +346,16 @@ class DeviceMesh:
             self.rt.ctx, ptr(self.elems), self.n_elems, self.npe,
             1 if tet10 else 0, ptr(inset), self.n_nodes, ptr(out),
             ctypes.byref(cnt), self.rt.stream()))
-        cand = out[: cnt.value].cpu().numpy()
-        if cand.size == 0:
+        nc = cnt.value
+        if nc == 0:
             return np.zeros((0, width), dtype=np.int64)
-        return exterior_faces(np.asarray(host.elements, dtype=np.int64), cand, tet10)
-
-
-def exterior_faces(els, cand, tet10=False):
-    """Faces (node lists) of candidate face ids e*4+f that occur once among
-    the candidates (by sorted corner triple), in first-occurrence order.
-
-    The corner triple is packed into one int64 over the compact ids of the
-    candidates' corner nodes (exact while there are < 2^21 of them), so one
-    1-D stable unique replaces a row-wise unique."""
-    e, f = cand // 4, cand % 4
-    table = np.array([c + m for c, m in FACES_T10]) if tet10 else np.array(FACES_P1)
-    full = els[e[:, None], table[f]]
-    keys = np.sort(full[:, :3], axis=1)
-    ids, inv = np.unique(keys.ravel(), return_inverse=True)
-    B = len(ids)
-    if B < (1 << 21):
-        k = inv.reshape(-1, 3).astype(np.int64)
-        packed = (k[:, 0] * B + k[:, 1]) * B + k[:, 2]
-        _, first, counts = np.unique(packed, return_index=True, return_counts=True)
-    else:
-        _, first, counts = np.unique(keys, axis=0, return_index=True,
-                                     return_counts=True)
-    keep = np.sort(first[counts == 1])
-    return full[keep]
+        ids = torch.empty(nc, dtype=torch.int64, device=self.rt.device)
+        nodes = torch.empty(nc * width, dtype=torch.int64, device=self.rt.device)
+        nout = N._i64()
+        N.check(self.rt.lib.cfem_face_exterior(
+            self.rt.ctx, ptr(self.elems), self.npe, 1 if tet10 else 0, ptr(out), nc,
+            self.n_nodes, ptr(ids), ptr(nodes), ctypes.byref(nout), self.rt.stream()))
+        return nodes[: nout.value * width].cpu().numpy().reshape(-1, width)
 
 
 # ------------------------------------------------------------ solver

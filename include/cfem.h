@@ -305,6 +305,21 @@ CFEM_API int cfem_face_candidates(cfem_ctx *ctx, const int32_t *d_elems,
                          const uint8_t *d_in_set, int64_t n_nodes,
                          int64_t *d_out, int64_t *n_out, void *stream);
 
+/* Exterior faces among the candidates of cfem_face_candidates
+ * (tet_heat.py:97-120, tet10.py:329-352, elastic3d.py:37-59): the faces
+ * whose sorted corner triple occurs once among the candidates - every face
+ * sharing a key with one whose corners are all in the set is itself a
+ * candidate, so this count equals the reference's count over all element
+ * faces - in candidate order (the reference's first-occurrence order).
+ * Writes their ids (element*4 + face) to d_ids and their nodes (3 corners,
+ * or with faces10 3 corners + 3 midside nodes) to d_nodes (n_cand * 3 or 6
+ * entries at most), and the count to *n_out. Sorting by the triple on the
+ * device (two stable radix sorts). Synchronises. */
+CFEM_API int cfem_face_exterior(cfem_ctx *ctx, const int32_t *d_elems, int32_t npe,
+                                int32_t faces10, const int64_t *d_cand, int64_t n_cand,
+                                int64_t n_nodes, int64_t *d_ids, int64_t *d_nodes,
+                                int64_t *n_out, void *stream);
+
 /* ---- sparse helpers -----------------------------------------------------
  * d_vals_out = a*d_x + b*d_y over n values (sums such as C + theta h K,
  * tet_heat.py:239-240). */

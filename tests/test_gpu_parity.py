@@ -327,3 +327,28 @@ def test_induction_heating_golden(cf, golden, tag):
     assert abs(res["E_in"] - float(g[tag + "_E_in"])) <= tol * float(g[tag + "_E_in"])
     assert abs(res["balance_rel"]) <= 1e-9
     assert_close(res["history"][-1]["mu_r_iron"], g[tag + "_mu_r_iron"], tol, "mu_r")
+
+
+def test_boundary_faces_on_device_against_oracle(cf):
+    """Device face dedup (two stable radix sorts of corner triples) against
+    the oracle's dict-order restatement: every face of a 24^3 P1 box and a
+    Tet10 box, named sets and 'interior' sets whose faces occur twice."""
+    from cloudfem_b200.device import DeviceMesh
+    from oracle import cfem_oracle as O
+    m = cf.mesh.box_mesh(24, 20, 16)
+    mo = O.Mesh(m.nodes, m.elements, m.boundaries)
+    dm = DeviceMesh(m)
+    for name in C.FACES:
+        np.testing.assert_array_equal(dm.boundary_faces(name), O.boundary_faces_p1(mo, name))
+    # a node set containing interior faces: the x < 0.5 half of the box
+    half = np.nonzero(m.nodes[:, 0] <= 0.5)[0]
+    m.boundaries["half"] = half
+    mo.boundaries["half"] = half
+    np.testing.assert_array_equal(DeviceMesh(m).boundary_faces("half"),
+                                  O.boundary_faces_p1(mo, "half"))
+    m10 = cf.mesh.box_mesh_tet10(6, 5, 4)
+    mo10 = O.Mesh(m10.nodes, m10.elements, m10.boundaries)
+    dm10 = DeviceMesh(m10)
+    for name in ("xmin", "ymax", "zmin"):
+        np.testing.assert_array_equal(dm10.boundary_faces(name, tet10=True),
+                                      O.boundary_faces10(mo10, name))

@@ -39,23 +39,6 @@ def test_mesh_sizes_of_benchmark_configs():
     assert mb.n_elements == 48
 
 
-def test_exterior_faces_packed_keys_match_rowwise_unique():
-    """The packed-key dedup of boundary face candidates gives the same faces
-    in the same order as a row-wise unique of the sorted corner triples."""
-    from cloudfem_b200.device import FACES_P1, FACES_T10, exterior_faces
-    rng = np.random.default_rng(5)
-    for tet10 in (False, True):
-        els = rng.integers(0, 500, (4000, 10 if tet10 else 4))
-        cand = np.sort(rng.choice(16000, 9000, replace=False))
-        e, f = cand // 4, cand % 4
-        table = np.array([c + m for c, m in FACES_T10]) if tet10 else np.array(FACES_P1)
-        full = els[e[:, None], table[f]]
-        _, first, counts = np.unique(np.sort(full[:, :3], axis=1), axis=0,
-                                     return_index=True, return_counts=True)
-        ref = full[np.sort(first[counts == 1])]
-        np.testing.assert_array_equal(exterior_faces(els, cand, tet10), ref)
-
-
 def test_add_at_matches_numpy():
     from cloudfem_b200._faces import add_at
     rng = np.random.default_rng(6)
