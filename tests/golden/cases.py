@@ -197,3 +197,23 @@ IND_KW2 = dict(IND_KW, method="cn", stagger_iter=2, cp_slope=1e-3,
 
 def ind_iron(x, y, z):
     return x < 0.5
+
+
+# P1 structural dynamics: a steel beam clamped at x = 0 (modal3d /
+# dynamics3d), a vertical tip load ramped in over the first steps
+DYN_BOX = (8, 2, 2, (0.0, 1.0), (0.0, 0.125), (0.0, 0.125))
+DYN_E, DYN_NU, DYN_RHO = 210e9, 0.3, 7800.0
+DYN_BC = {"xmin": (0.0, 0.0, 0.0)}
+DYN_T_END, DYN_DT = 4e-3, 2e-4
+
+
+def dyn_load(mesh):
+    """F(t) on the full 3N DOFs: -z force on the x = 1 face, ramped."""
+    n3 = 3 * mesh.n_nodes
+    tip = np.asarray(mesh.boundaries["xmax"])
+    base = np.zeros(n3)
+    base[3 * tip + 2] = -1e4 / len(tip)
+
+    def F(t):
+        return base * min(1.0, t / 1e-3)
+    return F

@@ -254,6 +254,38 @@ def main(ref_path):
     put("law_cp", ind.steel_cp_T(Tt, cp_slope=1e-3, cp_peak_h=2e6))
     put("law_H", ind.steel_enthalpy_T(Tt, cp_slope=1e-3, cp_peak_h=2e6))
 
+    # ---------------- P1 modal analysis and Newmark dynamics ----------------
+    from cloudfem.physics import dynamics3d as dyn
+    from cloudfem.physics import modal3d as mod
+    nx, ny, nz, xl, yl, zl = C.DYN_BOX
+    md = box_mesh(nx, ny, nz, xlim=xl, ylim=yl, zlim=zl)
+    put_csr("dyn_M", mod.assemble_mass_3d(md, C.DYN_RHO))
+    put_csr("dyn_Ml", mod.assemble_mass_3d(md, C.DYN_RHO, lumped=True))
+    for lumped in (False, True):
+        fr, modes = mod.solve_modes_3d(md, C.DYN_E, C.DYN_NU, C.DYN_RHO, bc=C.DYN_BC,
+                                       n_modes=6, lumped=lumped)
+        put("dyn_freqs" + ("_l" if lumped else ""), fr)
+        put("dyn_modes" + ("_l" if lumped else ""), modes)
+    for tag, kw in (("avg", dict(method="average")),
+                    ("lin", dict(method="linear", rayleigh=(5.0, 1e-6)))):
+        times, U, V, A = dyn.transient_3d(md, C.DYN_E, C.DYN_NU, C.DYN_RHO, bc=C.DYN_BC,
+                                          t_end=C.DYN_T_END, dt=C.DYN_DT,
+                                          load=C.dyn_load(md), **kw)
+        put("dyn_" + tag + "_times", times)
+        put("dyn_" + tag + "_U", U[:, ::7])
+        put("dyn_" + tag + "_V", V[-1])
+        put("dyn_" + tag + "_A", A[-1])
+    times, U, V, A = dyn.modal_superposition_3d(
+        md, C.DYN_E, C.DYN_NU, C.DYN_RHO, bc=C.DYN_BC, t_end=C.DYN_T_END,
+        dt=C.DYN_DT, load=C.dyn_load(md), n_modes=6, rayleigh=(5.0, 1e-6))
+    put("dyn_ms_U", U[:, ::7])
+    # single-DOF oscillator through the low-level core
+    times, U, V, A = dyn.newmark_integrate(np.array([[2.0]]), np.array([[0.3]]),
+                                           np.array([[50.0]]), lambda t: np.array([np.sin(3 * t)]),
+                                           2.0, 0.05, u0=1.0, v0=0.0)
+    put("dyn_sdof_U", U.ravel())
+    put("dyn_sdof_A", A.ravel())
+
     # ---------------- Tet10 A-V transient (theta method, LU) ----------------
     mt = box_mesh_tet10(C.AVT_N, C.AVT_N, C.AVT_N)
     res = em.transient_eddy_current_tet10(

@@ -13,7 +13,7 @@ pytest.importorskip("torch")
 
 NAMES = ("mesh.tet_mesh", "mesh.tet10_mesh", "fem.tet_poisson", "fem.tet_heat",
          "fem.tet10", "physics.elastic3d", "physics.elastic_tet10",
-         "physics.em3d_tet10")
+         "physics.em3d_tet10", "physics.modal3d", "physics.dynamics3d")
 
 
 def test_aliases_resolve_to_the_package(tmp_path, monkeypatch):
@@ -79,6 +79,12 @@ assert L.source_complex_power_tet10 is em.source_complex_power_tet10
 from cloudfem.physics.em3d_tet10 import solve_eddy_current_nonlinear_tet10
 assert solve_eddy_current_nonlinear_tet10 is em.solve_eddy_current_nonlinear_tet10
 assert tm.solve_elasticity_3d is e3.solve_elasticity_3d
+from cloudfem.physics.dynamics3d import modal_superposition_3d, transient_3d
+from cloudfem.physics.modal3d import solve_modes_3d
+import cloudfem_b200.physics.dynamics3d as dyn
+import cloudfem_b200.physics.modal3d as mod
+assert transient_3d is dyn.transient_3d and solve_modes_3d is mod.solve_modes_3d
+assert modal_superposition_3d is dyn.modal_superposition_3d
 print("ALIAS_OK")
 """
 
