@@ -54,6 +54,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 SPMV_STAGE = None   # --spmv-stage: None keeps the library default
 SELL_SORT = None    # --sell-sort: None keeps the library default
+SELL3_LANES = None  # --sell3-lanes: None keeps the library default
 
 
 def _set_scheduler(rt, name):
@@ -68,6 +69,23 @@ def _set_scheduler(rt, name):
         rt.set_param(N.PARAM_SPMV_STAGE, SPMV_STAGE)
     if SELL_SORT is not None:
         rt.set_param(N.PARAM_SELL_SORT, SELL_SORT)
+    if SELL3_LANES is not None:
+        rt.set_param(N.PARAM_SELL3_LANES, SELL3_LANES)
+
+
+def _block_spmv_kernel(rt):
+    """(name, profile summary) of the 3x3 SpMV-phase kernel the context's
+    staging selects."""
+    from cloudfem_b200 import _native as N
+    stage = rt.get_param(N.PARAM_SPMV_STAGE)
+    if stage in (3, 4):
+        lanes = rt.get_param(N.PARAM_SELL3_LANES)
+        return (f"k_gxl3 (PCG SpMV phase, sliced ELL, {lanes} lanes per block row: "
+                "q = A p, p update, p.q)", "k_gxl3_tet10_elasticity_80x10x10")
+    if stage == 2:
+        return ("k_gxs3 (PCG SpMV phase, blocks bulk-staged through shared memory)", None)
+    return ("k_gx (PCG SpMV phase, register path: q = A p, p update, p.q)",
+            "k_gx_tet10_elasticity_80x10x10")
 
 
 def _scalar_spmv_kernel(rt, precision):
@@ -327,8 +345,9 @@ def run_ours(args, rank, world, local_rank):
         achieved = bytes_spmv / (spmv_ms * 1e-3) / 1e9
     else:
         achieved = bytes_solve / (last.kernel_ms * 1e-3) / 1e9
-    traffic = _profiled_traffic("k_gx_tet10_elasticity_80x10x10",
-                                "fp32" if args.precision == "mixed" else "fp64")
+    kname, kprof = _block_spmv_kernel(rt)
+    traffic = (_profiled_traffic(kprof, "fp32" if args.precision == "mixed" else "fp64")
+               if kprof else None)
     h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
     d2h = 3 * mesh.n_nodes * 8
     value = world * free * args.steps / (ms * 1e-3)
@@ -369,7 +388,7 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {
-            "kernel": "k_gx (PCG SpMV phase: q = A p, p update, p.q)",
+            "kernel": kname,
             "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "bytes_per_launch": bytes_spmv,
@@ -1223,10 +1242,14 @@ def main():
     ap.add_argument("--sell-sort", type=int, default=None, choices=[0, 1],
                     help="sliced-ELL SpMV: 1 sort each 256-row window by row length, "
                          "0 keep rows in order (default: the library's)")
+    ap.add_argument("--sell3-lanes", type=int, default=None, choices=[1, 2, 4],
+                    help="sliced-ELL SpMV of 3x3 blocks: lanes per block row (default: "
+                         "the library's)")
     args = ap.parse_args()
-    global SPMV_STAGE, SELL_SORT
+    global SPMV_STAGE, SELL_SORT, SELL3_LANES
     SPMV_STAGE = args.spmv_stage
     SELL_SORT = args.sell_sort
+    SELL3_LANES = args.sell3_lanes
     if args.precision is None:
         args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -78,6 +78,7 @@ struct cfem_ctx {
     int spmv_stage = 4;                // SpMV: 0 registers, 1 staged scalar rows, 2 also
                                        // 3x3, 3 sliced ELL, 4 auto (per precision and bs)
     int sell_sort = 1;                 // sliced ELL: sort rows by length per window
+    int sell3_lanes = 4;               // sliced ELL of 3x3 blocks: lanes per block row
     int barrier_timeout_us = 4000000;  // persistent grid-barrier wait limit
     int barrier_hold = 0;              // phantom barrier arrivals (fault injection)
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler

@@ -135,6 +135,13 @@ struct GridBar {
 __device__ __forceinline__ void pdl_wait() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
+// Lets the next kernel of the graph launch before this one ends (it runs
+// what precedes its own pdl_wait, which still waits for this kernel's
+// completion and memory). Issued after this kernel's own wait, so every
+// earlier kernel has completed by then.
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     unsigned v;
@@ -2055,6 +2062,7 @@ constexpr int RED_THREADS = 1024;
 __global__ void __launch_bounds__(RED_THREADS)
 k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which) {
     pdl_wait();
+    pdl_trigger();   // the next kernel's fixed-data prologue may start now
     __shared__ double red[4][RED_THREADS / 32];
     const int s = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
     const SysDev &S = sys[s];
@@ -2130,12 +2138,16 @@ __device__ __forceinline__ double ld_stream(const double *p) {
     return v;
 }
 
-// Sort each work entry's rows by stored length (the diagonal counted once
-// even when absent: it gets its own slot) and write the slice sizes
-// (32 x longest row, 0 for slices of padding rows only).
+// Sort each window's rows by stored length (the diagonal counted once
+// even when absent: it gets its own slot) and write the slice sizes. A
+// slice holds RS rows, each over 32 / RS lanes, so its size is 32 x its
+// longest row's slot count rounded up to whole steps of 32 / RS slots (0
+// for slices of padding rows only). RS = 32: one row per lane.
+template <int RS>
 __global__ void __launch_bounds__(SELL_ROWS)
 k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
             uint8_t *__restrict__ perm, int64_t *__restrict__ sizes, int sort) {
+    constexpr int LPR = 32 / RS, NS = SELL_ROWS / RS;
     __shared__ int len[SELL_ROWS];
     const int t = threadIdx.x;
     const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
@@ -2147,10 +2159,13 @@ k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         for (int32_t k = kb; k < ke; ++k) diag |= __ldg(ci + k) == (int32_t)row;
         L = ke - kb + (diag ? 0 : 1);
     }
-    if (!sort) {   // rows in their own order: a slice is 32 consecutive rows
+    if (!sort) {   // rows in their own order: a slice is RS consecutive rows
         perm[r0 + t] = (uint8_t)t;
-        const int m = __reduce_max_sync(0xffffffffu, L);
-        if ((t & 31) == 0) sizes[(int64_t)blockIdx.x * SELL_SLICES + (t >> 5)] = 32 * (int64_t)m;
+        int m = L;
+#pragma unroll
+        for (int o = RS / 2; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t % RS) == 0)
+            sizes[(int64_t)blockIdx.x * NS + t / RS] = 32 * (int64_t)((m + LPR - 1) / LPR);
         return;
     }
     len[t] = L;
@@ -2161,7 +2176,8 @@ k_sell_rank(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         rank += (Lu > L || (Lu == L && u < t)) ? 1 : 0;
     }
     perm[r0 + rank] = (uint8_t)t;
-    if ((rank & 31) == 0) sizes[(int64_t)blockIdx.x * SELL_SLICES + (rank >> 5)] = 32 * (int64_t)L;
+    if ((rank % RS) == 0)
+        sizes[(int64_t)blockIdx.x * NS + rank / RS] = 32 * (int64_t)((L + LPR - 1) / LPR);
 }
 
 // Fill the slices from the CSR: position t of entry blockIdx.x (slice t/32,
@@ -2204,19 +2220,22 @@ k_sell_fill(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
     }
 }
 
-// 3x3 blocks: as k_sell_fill, with the slot's 9 values (row-major block)
-// in 9 planes of 32 lanes: value e of slot k of a slice at
-// 9 soff[slice] + (9 k + e) 32 + lane.
-template <typename T>
+// 3x3 blocks: as k_sell_fill, with RS block rows per slice, each over
+// L = 32 / RS lanes: slot k of the slice's row r sits at step k / L, lane
+// r L + k % L, and the step's 9 values (row-major block) in 9 planes of 32
+// lanes: column at soff[slice] + 32 step + lane, value e at
+// 9 soff[slice] + (9 step + e) 32 + lane. Slot 0 is the diagonal block.
+template <typename T, int RS>
 __global__ void __launch_bounds__(SELL_ROWS)
 k_sell_fill3(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
              const T *__restrict__ v, const uint8_t *__restrict__ perm,
              const int64_t *__restrict__ soff, int32_t *__restrict__ scol, T *__restrict__ sval) {
+    constexpr int L = 32 / RS, NS = SELL_ROWS / RS;
     const int t = threadIdx.x;
     const int64_t r0 = (int64_t)blockIdx.x * SELL_ROWS;
-    const int64_t sl = (int64_t)blockIdx.x * SELL_SLICES + (t >> 5);
+    const int64_t sl = (int64_t)blockIdx.x * NS + t / RS;
     const int64_t base = soff[sl];
-    const int w = (int)((soff[sl + 1] - base) >> 5);
+    const int w = (int)((soff[sl + 1] - base) >> 5) * L;   // slots per row
     if (w == 0) return;
     const int64_t row = r0 + perm[r0 + t];
     const bool valid = row < n;
@@ -2225,12 +2244,14 @@ k_sell_fill3(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restric
     for (int k = 0; k < len; ++k)
         if (__ldg(ci + kb + k) == (int32_t)row) { dpos = k; break; }
     const int32_t own = valid ? (int32_t)row : (int32_t)r0;
-    const int lane = t & 31;
-    T *vb = sval + 9 * base + lane;
+    const int r = t % RS;
     auto put = [&](int k, int32_t c, int64_t src) {
-        scol[base + 32 * k + lane] = c;
+        const int64_t step = k / L;
+        const int lane = r * L + k % L;
+        scol[base + 32 * step + lane] = c;
+        T *vb = sval + 9 * base + 9 * 32 * step + lane;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) vb[(int64_t)(9 * k + e) * 32] = src >= 0 ? v[src * 9 + e] : (T)0;
+        for (int e = 0; e < 9; ++e) vb[32 * e] = src >= 0 ? v[src * 9 + e] : (T)0;
     };
     put(0, own, dpos >= 0 ? (int64_t)kb + dpos : -1);
     int k = 1;
@@ -2241,72 +2262,134 @@ k_sell_fill3(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restric
     for (; k < w; ++k) put(k, own, -1);
 }
 
-// q = A p and p.q over the 32 block rows of slice sl of a 3x3 system (A
-// phase), one block row per lane. As the register path does, the new
+// q = A p and p.q over the RS = 32 / L block rows of slice sl of a 3x3
+// system (A phase), L lanes per block row, each over every L-th slot; the
+// lanes' partial sums meet by shuffles. As the register path does, the new
 // direction p = zeta z + beta p_old is formed at every gathered block and
-// written for the lane's own row (3x3 systems have no separate direction
-// launch). DIFF: slot 0 holds the FP32 block row sum S_i, applied to p_i,
-// the other slots A_ij (p_j - p_i).
-template <typename T, bool DIFF>
-__device__ __forceinline__ void phase_A_sell3(const SysDev &S, const SysState *st, int64_t sl,
-                                              int lane, double part[4]) {
+// written for the row (3x3 systems have no separate direction launch).
+// DIFF: slot 0 holds the FP32 block row sum S_i, applied to p_i, the other
+// slots A_ij (p_j - p_i).
+//
+// Split in two: sell3_open reads only what is fixed for the whole solve
+// (the slice's place, its row, its first columns and block values), so
+// k_gxl3 runs it before waiting for its predecessor kernel; sell3_run
+// then streams the slice: columns two steps ahead of their gathers, block
+// values D steps ahead (D = 2 for FP32, 1 for FP64, whose registers allow
+// one), the gathers of z and p_old one step ahead of their use.
+template <typename T> struct Sell3Depth { static constexpr int D = sizeof(T) == 4 ? 2 : 1; };
+
+template <typename T> struct Sell3Slice {
+    const int32_t *cp;
+    const T *vp;
+    int w;            // steps
+    int64_t row;      // the lane's block row (its window's first row if padding)
+    bool valid, live;
+    int64_t j0, j1;   // columns of steps 0 and 1
+    T a0[9], a1[9];   // block values of steps 0 and 1 (a1: FP32 only)
+};
+
+template <typename T, int L>
+__device__ __forceinline__ void sell3_open(const SysDev &S, int64_t sl, int lane,
+                                           Sell3Slice<T> &q) {
+    constexpr int RS = 32 / L, NS = SELL_ROWS / RS;
+    const int64_t r0 = (sl / NS) * SELL_ROWS;
+    const int s = (int)(sl % NS);
+    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    q.live = s * RS < nr;
+    if (!q.live) return;
+    const int64_t base = __ldg(S.soff + sl);
+    q.w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+    const int rl = __ldg(S.sperm + r0 + s * RS + lane / L);
+    q.valid = rl < nr;
+    q.row = q.valid ? r0 + rl : r0;
+    q.cp = S.scol + base + lane;
+    q.vp = (const T *)S.sval + 9 * base + lane;
+    q.j0 = ld_stream(q.cp);
+    q.j1 = ld_stream(q.cp + 32 * (q.w > 1 ? 1 : 0));
+#pragma unroll
+    for (int e = 0; e < 9; ++e) q.a0[e] = ld_stream(q.vp + 32 * e);
+    if (Sell3Depth<T>::D == 2) {
+        const int t1 = q.w > 1 ? 1 : 0;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) q.a1[e] = ld_stream(q.vp + 32 * (9 * t1 + e));
+    }
+}
+
+template <typename T, bool DIFF, int L>
+__device__ __forceinline__ void sell3_run(const SysDev &S, const SysState *st, Sell3Slice<T> &q,
+                                          int lane, double part[4]) {
+    constexpr int D = Sell3Depth<T>::D;
+    if (!q.live) return;
     const T beta = (T)vcg(&st->beta);
     const T zeta = (T)vcg(&st->zeta);
     const int pbuf = vcgi(&st->pbuf);
     const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
     T *pout = (T *)(pbuf ? S.p0 : S.p1);
     const T *z = (const T *)S.z;
-    T *q = (T *)S.q;
-    const int64_t r0 = (sl / SELL_SLICES) * SELL_ROWS;
-    const int s = (int)(sl % SELL_SLICES);
-    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    T *qv = (T *)S.q;
+    const int u = lane % L;
+    const int w = q.w;
+    const int64_t row = q.row;
+    T pi[3], acc[3], gz[3], gp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        pi[c] = zeta * __ldg(z + row * 3 + c) + beta * __ldg(pin + row * 3 + c);
+        acc[c] = 0;
+        gz[c] = __ldg(z + q.j0 * 3 + c);
+        gp[c] = __ldg(pin + q.j0 * 3 + c);
+    }
+    int64_t jn = q.j1;
+    for (int t = 0; t < w; ++t) {
+        const int tn = t + 1 < w ? t + 1 : t;
+        const int tnn = t + 2 < w ? t + 2 : tn;
+        const int64_t jnn = ld_stream(q.cp + 32 * tnn);
+        T an[9], gz2[3], gp2[3];
+        const int tl = D == 2 ? tnn : tn;   // the step whose values load now
+#pragma unroll
+        for (int e = 0; e < 9; ++e) an[e] = ld_stream(q.vp + 32 * (9 * tl + e));
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            gz2[d] = __ldg(z + jn * 3 + d);
+            gp2[d] = __ldg(pin + jn * 3 + d);
+        }
+        T pj[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            pj[d] = zeta * gz[d] + beta * gp[d];
+            if (DIFF) pj[d] = (t == 0 && u == 0) ? pi[d] : pj[d] - pi[d];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[c] += q.a0[c * 3 + d] * pj[d];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            if (D == 2) {
+                q.a0[e] = q.a1[e];
+                q.a1[e] = an[e];
+            } else {
+                q.a0[e] = an[e];
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            gz[d] = gz2[d];
+            gp[d] = gp2[d];
+        }
+        jn = jnn;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int o = L / 2; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
     T pq = 0;
-    if (s * 32 < nr) {
-        const int64_t base = __ldg(S.soff + sl);
-        const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
-        const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
-        const bool valid = rl < nr;
-        const int64_t row = valid ? r0 + rl : r0;
-        T pi[3], acc[3];
+    if (q.valid && u == 0) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            pi[c] = zeta * __ldg(z + row * 3 + c) + beta * __ldg(pin + row * 3 + c);
-            acc[c] = 0;
-        }
-        const int32_t *cp = S.scol + base + lane;
-        const T *vp = (const T *)S.sval + 9 * base + lane;
-        {   // slot 0: the diagonal block (FP32: the block row sum)
-            T a[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a[e] = ld_stream(vp + 32 * e);
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) acc[c] += a[c * 3 + d] * pi[d];
-        }
-        for (int k = 1; k < w; ++k) {
-            const int64_t j = ld_stream(cp + 32 * k);
-            T a[9], pj[3];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a[e] = ld_stream(vp + 32 * (9 * k + e));
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                pj[d] = zeta * __ldg(z + j * 3 + d) + beta * __ldg(pin + j * 3 + d);
-                if (DIFF) pj[d] -= pi[d];
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) acc[c] += a[c * 3 + d] * pj[d];
-        }
-        if (valid) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int64_t i = row * 3 + c;
-                pout[i] = pi[c];
-                q[i] = acc[c];
-                pq += pi[c] * acc[c];
-            }
+            const int64_t i = row * 3 + c;
+            pout[i] = pi[c];
+            qv[i] = acc[c];
+            pq += pi[c] * acc[c];
         }
     }
     part[0] += (double)pq;
@@ -2441,29 +2524,37 @@ k_gxl(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
-// k_gx for 3x3 systems with the sliced-ELL A phase (one block row per
-// lane, one slice per warp); R and ZERO phases on the entry's block rows
-// as in k_gx.
-template <typename T>
-__global__ void __launch_bounds__(32 * GROUP, SELL_BLOCKS)
+// k_gx for 3x3 systems with the sliced-ELL A phase (one slice of 32 / L
+// block rows per warp, L lanes per block row); R and ZERO phases on the
+// entry's block rows as in k_gx. The slice's fixed data is read before the
+// wait for the predecessor kernel (dependent launches).
+template <typename T> struct Sell3Occ {   // the pipelined blocks need 80 registers
+    static constexpr int blocks = 3;
+};
+template <typename T, int L>
+__global__ void __launch_bounds__(32 * GROUP, Sell3Occ<T>::blocks)
 k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
        const int2 *__restrict__ list, int n) {
-    pdl_wait();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wid = blockIdx.x * GROUP + w;
     const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
-    const int2 lead = __ldg(list + blockIdx.x * GROUP);
-    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);   // a real entry (lists pad per system)
     const SysDev &S = sys[lead.x];
+    const bool mine = e.x >= 0 && (int64_t)e.y * S.xrows < S.n;
+    Sell3Slice<T> q;
+    q.live = false;
+    if (mine) sell3_open<T, L>(S, e.y, lane, q);
+    pdl_wait();
+    if (*(volatile const int *)&bar->active <= 0) return;   // all finished
     const int ph = *(volatile int32_t *)&st[lead.x].phase;
     const bool x_phase = ph == PH_A || ph == PH_R || ph == PH_ZERO;
     if (!x_phase) return;                 // uniform over the block
     double part[4] = {0.0, 0.0, 0.0, 0.0};
-    if (e.x >= 0 && (int64_t)e.y * S.xrows < S.n) {   // (slots: entries past a smaller system)
+    if (mine) {
         const int64_t r0 = (int64_t)e.y * S.xrows;
         const int64_t r1 = min(S.n, r0 + S.xrows);
         if (ph == PH_A) {
-            phase_A_sell3<T, sizeof(T) == 4>(S, &st[e.x], e.y, lane, part);
+            sell3_run<T, sizeof(T) == 4, L>(S, &st[e.x], q, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
             run_R<T, 3>(S, &st[e.x], r0, r1, lane, part, &bad);
@@ -2472,6 +2563,20 @@ k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
         }
     }
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
+// The k_gxl3 instance for L lanes per block row (1, 2 or 4: slices of at
+// least chunk_rows(3) block rows, so the work lists stay within their
+// per-chunk allocation).
+template <typename T>
+static void (*gxl3_kernel(int L))(const SysDev *, SysState *, const GridBar *, const int2 *, int) {
+    return L == 1 ? k_gxl3<T, 1> : L == 2 ? k_gxl3<T, 2> : k_gxl3<T, 4>;
+}
+
+// Rows per sliced-ELL slice: 32 scalar rows (one per lane), or 32 / L
+// block rows of a 3x3 system.
+__host__ __device__ inline int sell_slice_rows(int bs, int lanes3) {
+    return bs == 3 ? 32 / lanes3 : 32;
 }
 
 constexpr int POLL_ITERS = 16;    // iterations per replay, host-polled graphs
@@ -2628,6 +2733,7 @@ struct cfem_pcg_plan {
     // POLL_ITERS iterations replayed in turn
     bool polled = false;
     int giters = 2;               // iterations per body of the solve loop
+    int lanes3 = 4;               // sliced ELL of 3x3 systems: lanes per block row
     // solve slots (cfem_pcg_slots_*): each system of the plan is a slot of
     // fixed capacity whose system is replaced between rounds of iterations
     bool slots = false;
@@ -2648,12 +2754,24 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
     for (int i = first; i < last; ++i) {
         SysDev &S = P->hs[i];
         if (S.bs == 3 && S.sell) {
-            if (S.mode == CFEM_SOLVE_MIXED)
-                CFEM_LAUNCH(k_sell_fill3<float>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n,
-                            S.rp, S.ci, S.v32, S.sperm, S.soff, (int32_t *)S.scol, (float *)S.sval);
-            else
-                CFEM_LAUNCH(k_sell_fill3<double>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n,
-                            S.rp, S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
+            const unsigned nw = (unsigned)sell_windows(S.n);
+            const int rs = sell_slice_rows(3, P->lanes3);
+            auto fill = [&](auto kernel, const auto *v, auto *out) -> int {
+                CFEM_LAUNCH(kernel, nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, v, S.sperm, S.soff,
+                            (int32_t *)S.scol, out);
+                return CFEM_OK;
+            };
+            if (S.mode == CFEM_SOLVE_MIXED) {
+                float *o = (float *)S.sval;
+                CFEM_TRY(rs == 32 ? fill(k_sell_fill3<float, 32>, S.v32, o)
+                         : rs == 16 ? fill(k_sell_fill3<float, 16>, S.v32, o)
+                                    : fill(k_sell_fill3<float, 8>, S.v32, o));
+            } else {
+                double *o = (double *)S.sval;
+                CFEM_TRY(rs == 32 ? fill(k_sell_fill3<double, 32>, S.v64, o)
+                         : rs == 16 ? fill(k_sell_fill3<double, 16>, S.v64, o)
+                                    : fill(k_sell_fill3<double, 8>, S.v64, o));
+            }
         } else if (S.bs == 3 && S.c3) {
             const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
             if (S.mode == CFEM_SOLVE_MIXED)
@@ -2696,8 +2814,9 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     int64_t max_sl = 0;
     for (const SysDev &S : P->hs)
         if (S.sell) {
-            const int64_t nsl = sell_windows(S.n) * SELL_SLICES;
-            meta += align256((size_t)nsl * 32) + 2 * align256((nsl + 1) * 8);
+            const int64_t nw = sell_windows(S.n);
+            const int64_t nsl = nw * (SELL_ROWS / sell_slice_rows(S.bs, P->lanes3));
+            meta += align256((size_t)nw * SELL_ROWS) + 2 * align256((nsl + 1) * 8);
             max_sl = std::max(max_sl, nsl + 1);
         }
     if (!meta) return CFEM_OK;
@@ -2713,16 +2832,22 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     for (size_t i = 0; i < P->hs.size(); ++i) {
         SysDev &S = P->hs[i];
         if (!S.sell) continue;
-        const int64_t nw = sell_windows(S.n), nsl = nw * SELL_SLICES;
+        const int rs = sell_slice_rows(S.bs, P->lanes3);
+        const int64_t nw = sell_windows(S.n), nsl = nw * (SELL_ROWS / rs);
         uint8_t *perm = (uint8_t *)(P->ws_smeta + o);
-        o += align256((size_t)nsl * 32);
+        o += align256((size_t)nw * SELL_ROWS);
         int64_t *sizes = (int64_t *)(P->ws_smeta + o);
         o += align256((nsl + 1) * 8);
         int64_t *soff = (int64_t *)(P->ws_smeta + o);
         o += align256((nsl + 1) * 8);
         CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
-        CFEM_LAUNCH(k_sell_rank, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes,
-                    P->ctx->sell_sort);
+        const int srt = P->ctx->sell_sort;
+        if (rs == 32)
+            CFEM_LAUNCH(k_sell_rank<32>, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes, srt);
+        else if (rs == 16)
+            CFEM_LAUNCH(k_sell_rank<16>, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes, srt);
+        else
+            CFEM_LAUNCH(k_sell_rank<8>, (unsigned)nw, SELL_ROWS, 0, s, S.n, S.rp, S.ci, perm, sizes, srt);
         CFEM_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, sizes, soff, nsl + 1, s));
         CFEM_CUDA(cudaMemcpyAsync(&totals[i], soff + nsl, sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, s));
@@ -2786,6 +2911,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                       cudaStream_t s, cfem_pcg_plan *P) {
     P->ctx = ctx;
     P->device = ctx->device;
+    P->lanes3 = ctx->sell3_lanes;
     P->n_systems = n_systems;
     CFEM_CUDA(cudaStreamCreateWithFlags(&P->w, cudaStreamNonBlocking));
     CFEM_CUDA(cudaStreamCreateWithFlags(&P->w2, cudaStreamNonBlocking));
@@ -2883,12 +3009,13 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     // Scalar systems on the graph scheduler read a unit-padded copy; 3x3
     // systems a padded block copy (staged SpMV) or an entry-major copy.
     // SpMV staging per list type t = 2 (mixed) + (3x3): explicit, or AUTO
-    // (4): sliced ELL for FP64 scalar rows, the bulk-staged windows for FP32
-    // scalar rows, the register path for 3x3 blocks (the fastest measured
-    // for each on the benchmark workloads)
+    // (4): sliced ELL for FP64 scalar rows and for 3x3 blocks in both
+    // precisions (slices of 32 / L block rows, L lanes per block row), the
+    // bulk-staged windows for FP32 scalar rows (the fastest measured for
+    // each on the benchmark workloads)
     int tstage[4];
     for (int t = 0; t < 4; ++t)
-        tstage[t] = ctx->spmv_stage != 4 ? ctx->spmv_stage : (t == 0 ? 3 : t == 2 ? 1 : 0);
+        tstage[t] = ctx->spmv_stage != 4 ? ctx->spmv_stage : (t == 2 ? 1 : 3);
     // solve slots: copies whose size follows the capacity alone (no sliced
     // ELL, whose padding depends on the system)
     if (P->slots)
@@ -2966,7 +3093,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         // so a warp's set-up (work entry, system, state) is paid per 128 rows
         // (measured 1.8x faster than one chunk on the batched heat meshes; 3x3
         // systems keep one chunk: fewer, longer warps measured slower there).
-        S.xrows = S.sell ? 32 : (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;   // 32: one slice
+        S.xrows = S.sell ? sell_slice_rows(S.bs, P->lanes3)               // one slice
+                         : (S.vec4 ? X_CHUNKS_VEC : 1) * S.crows;
         CFEM_CHECK(!S.c3 || S.xrows <= XR3, CFEM_ERR_UNSUPPORTED,
                    "staged 3x3 work entries hold at most %d block rows", XR3);
         S.nxe = (int32_t)((S.n + S.xrows - 1) / S.xrows);
@@ -2996,6 +3124,16 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
         while (la[t].size() % GROUP) la[t].push_back(make_int2(-1, -1));
         for (int c = 0; c < hs[i].nchunksB; ++c) lb[t].push_back(make_int2(i, c));
         while (lb[t].size() % GROUP) lb[t].push_back(make_int2(-1, -1));
+    }
+    {
+        size_t na = 0, nb = 0;
+        for (int t = 0; t < 4; ++t) {
+            na += la[t].size();
+            nb += lb[t].size();
+        }
+        CFEM_CHECK(na <= list_a && nb <= list_b, CFEM_ERR_INVALID,
+                   "work lists (%zu, %zu entries) exceed their allocation (%zu, %zu)", na, nb,
+                   list_a, list_b);
     }
     int2 *pa[4], *pb[4];
     size_t oa = 0, ob = 0;
@@ -3071,12 +3209,12 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage == 2)
                 glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage == 3) glaunch(p, k_gxl3<double>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 3) glaunch(p, gxl3_kernel<double>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage < 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage == 2)
                 glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage == 3) glaunch(p, k_gxl3<float>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 3) glaunch(p, gxl3_kernel<float>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage < 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }

@@ -179,11 +179,11 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * per warp with 1-D bulk copies (TMA) and loads 3x3 blocks into registers,
  * 2 streams 3x3 blocks through shared memory too, 0 loads both into
  * registers, 3 stores scalar rows and 3x3 block rows in the sliced-ELL
- * layout (windows of 256 rows cut into slices of 32, one row per lane,
- * coalesced slot-major loads, no cross-lane sums), 4 (default) picks per
- * precision and block size what measured fastest: sliced ELL for FP64
- * scalar rows, the staged windows for FP32 scalar rows, registers for 3x3
- * blocks.
+ * layout (windows of 256 rows sorted by length and cut into slices: 32
+ * scalar rows, one per lane, or 32 / SELL3_LANES block rows; coalesced
+ * slot-major loads), 4 (default) picks per precision and block size what
+ * measured fastest: sliced ELL for FP64 scalar rows and for 3x3 blocks, the
+ * staged windows for FP32 scalar rows.
  * BARRIER_TIMEOUT_US: how long (microseconds, 1 .. 60e6; default 4e6) a
  * block of the persistent scheduler waits at its grid barrier before it
  * gives up; the solve then ends with CFEM_ERR_TIMEOUT and the context stays
@@ -193,11 +193,13 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * read when a solve plan is created. SELL_SORT (SpMV staging 3): 1
  * (default) sorts each window of 256 rows by length before cutting it into
  * slices of 32 (less padding), 0 keeps the rows in order (neighbouring
- * rows in a slice: gathers of p that share cache lines). get returns -1 for
- * an unknown parameter. */
+ * rows in a slice: gathers of p that share cache lines). SELL3_LANES
+ * (SpMV staging 3, 3x3 blocks): lanes that share one block row, each over
+ * every L-th block of it (1, 2 or 4 (default); a slice holds 32 / L block
+ * rows). get returns -1 for an unknown parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5, CFEM_PARAM_BARRIER_TIMEOUT_US = 6,
-       CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8 };
+       CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8, CFEM_PARAM_SELL3_LANES = 9 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */

@@ -1,7 +1,8 @@
 """SpMV of the graph scheduler with the matrix streamed through
 shared-memory windows by 1-D bulk copies (staging 1: scalar rows; 2: also
 3x3 blocks) or in the sliced-ELL layout (staging 3: scalar rows, one row
-per lane, slices of 32 length-sorted rows) against the register path
+per lane, slices of 32 length-sorted rows; 3x3 block rows over 1, 2 or 4
+lanes each, slices of 32, 16 or 8 block rows) against the register path
 (staging 0) and a direct FP64 solve:
 the same answers, bitwise batch independence, rows longer than a window,
 short (P1-like, 4 lanes per row) and long (8 lanes) rows, 3x3 rows that
@@ -83,20 +84,23 @@ def _system(torch, rt, A, b, offset):
     return s
 
 
-def _solve(rt, systems, mode, rtol, stage, sort=1):
+def _solve(rt, systems, mode, rtol, stage, sort=1, lanes=4):
     from cloudfem_b200 import _native as N
     from cloudfem_b200.device import pcg
     N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_GRAPH))
     before = rt.get_param(N.PARAM_SPMV_STAGE)
+    lanes_before = rt.get_param(N.PARAM_SELL3_LANES)
     try:
         rt.set_param(N.PARAM_SPMV_STAGE, stage)
         rt.set_param(N.PARAM_SELL_SORT, sort)
+        rt.set_param(N.PARAM_SELL3_LANES, lanes)
         for s in systems:
             s.x.zero_()
         res = pcg(systems, mode, rtol, 20000)
     finally:
         rt.set_param(N.PARAM_SPMV_STAGE, before)
         rt.set_param(N.PARAM_SELL_SORT, 1)
+        rt.set_param(N.PARAM_SELL3_LANES, lanes_before)
         N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
     for r in res:
         assert r.status == N.CFEM_OK, r
@@ -150,9 +154,9 @@ def test_staged_spmv_batch_equals_solo_bitwise(torch, rows, stage):
     systems = [_system(torch, rt, A, np.ones(A.shape[0]), off)
                for A, off in zip(mats, (0, 1, 2))]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, stage)
+        rb, xb = _solve(rt, systems, md, 1e-10, stage, lanes=lanes)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, stage)
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage, lanes=lanes)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
         _, xr = _solve(rt, systems, md, 1e-10, stage)
@@ -176,28 +180,29 @@ def _elastic_system(torch, nx, ny, nz, seed):
                            vals, rhs, x, mask)
 
 
-@pytest.mark.parametrize("stage", [2, 3])
+@pytest.mark.parametrize("stage,lanes", [(2, 4), (3, 1), (3, 2), (3, 4)])
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
-def test_staged_3x3_spmv_matches_register_path(torch, mode, stage):
+def test_staged_3x3_spmv_matches_register_path(torch, mode, stage, lanes):
     """3x3-block systems on the graph scheduler: the staged SpMV (staging
     2: rows that straddle windows, 65-block vertex rows) or the sliced-ELL
-    one (staging 3: one block row per lane) and the register path reach the
-    same answer, and the other path repeats bitwise."""
+    one (staging 3: slices of 32 / lanes block rows, `lanes` lanes per block
+    row) and the register path reach the same answer, and the other path
+    repeats bitwise."""
     from cloudfem_b200 import _native as N
     dm, sysm = _elastic_system(torch, 10, 3, 3, seed=1)
     rt = dm.rt
     md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
     rtol = 1e-11 if mode == "fp64" else 1e-10
     _, (x0,) = _solve(rt, [sysm], md, rtol, 0)
-    r1, (x1,) = _solve(rt, [sysm], md, rtol, stage)
-    _, (x1b,) = _solve(rt, [sysm], md, rtol, stage)
+    r1, (x1,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes)
+    _, (x1b,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes)
     d = np.linalg.norm(x1 - x0) / np.linalg.norm(x0)
     assert d <= (1e-8 if mode == "fp64" else 1e-7), d
     assert np.array_equal(x1, x1b)
 
 
-@pytest.mark.parametrize("stage", [2, 3])
-def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage):
+@pytest.mark.parametrize("stage,lanes", [(2, 4), (3, 2), (3, 4)])
+def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage, lanes):
     """Each 3x3 system's answer is bitwise the same alone and in a batch
     with the staged or sliced-ELL SpMV, in both precisions."""
     from cloudfem_b200 import _native as N
