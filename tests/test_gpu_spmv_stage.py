@@ -154,9 +154,9 @@ def test_staged_spmv_batch_equals_solo_bitwise(torch, rows, stage):
     systems = [_system(torch, rt, A, np.ones(A.shape[0]), off)
                for A, off in zip(mats, (0, 1, 2))]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, stage, lanes=lanes)
+        rb, xb = _solve(rt, systems, md, 1e-10, stage)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, stage, lanes=lanes)
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
         _, xr = _solve(rt, systems, md, 1e-10, stage)
@@ -210,8 +210,8 @@ def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage, lanes):
     rt = built[0][0].rt
     systems = [s for _, s in built]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, stage)
+        rb, xb = _solve(rt, systems, md, 1e-10, stage, lanes=lanes)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, stage)
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage, lanes=lanes)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
