@@ -971,11 +971,12 @@ def run_avt(args, rank, world, local_rank):
         "config": {"workload": f"transient_av_tet10_box_{n}cubed_{steps}_cn_steps",
                    "a_unknowns": int(unknowns), "time_steps": steps,
                    "note": "value and e2e: the public call, A-block DOF-steps per second "
-                           "(device blocks and solves, host power diagnostics)",
+                           "(device blocks, A and V solves and Joule power; fields copied "
+                           "back once at the end)",
                    "P_last": float(r["P"][-1]), "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * unknowns * steps / wall, "unit": "DOF/s",
                 "h2d_bytes_per_step": int(mesh.nodes.nbytes + mesh.elements.nbytes),
-                "d2h_bytes_per_step": int(steps * 3 * mesh.n_nodes * 8)},
+                "d2h_bytes_per_step": int(((steps + 1) + 4 * mesh.n_nodes) * 8)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

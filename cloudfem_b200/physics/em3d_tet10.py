@@ -12,8 +12,10 @@ Drop-in for the assembly of cloudfem/physics/em3d_tet10.py:
   device in place of SuperLU (see its docstring);
 * ``transient_eddy_current_tet10`` (:479-662): theta stepping with a
   symmetric positive definite scaling of the step matrix and one device
-  PCG solve (one graph launch) per step; ``transient_joule_power_tet10``
-  (:665-692) vectorised.
+  PCG solve (one graph launch) per step, the step's V by a second device
+  PCG solve and its Joule power by a device kernel, so the fields stay on
+  the GPU for the whole march; ``transient_joule_power_tet10`` (:665-692)
+  by the same kernel.
 * ``solve_eddy_current_nonlinear_tet10`` (:849-982): the secant B-H Picard
   loop, K rebuilt on the device from the updated per-element reluctivity
   each iteration and each linear phasor solve by device COCG warm-started
@@ -42,7 +44,6 @@ import types
 
 import numpy as np
 import scipy.sparse as sp
-import scipy.sparse.linalg as spla
 from scipy.sparse.csgraph import connected_components
 
 from .. import _native as N
@@ -614,30 +615,50 @@ def _nodal_gradients_all(mesh):
     return np.einsum("pjk,ekl->epjl", dN_dxi, np.linalg.inv(J))
 
 
-def _joule_power(mesh, a_prev, a_new, v, sig_e, vols, grads, h):
-    from ..fem.tet10 import _MASS_REF
-    a_prev = np.asarray(a_prev, dtype=float).reshape(-1, 3)
-    a_new = np.asarray(a_new, dtype=float).reshape(-1, 3)
-    on = sig_e > 0.0
-    els = np.asarray(mesh.elements)[on]
-    Ep = -(a_new[els] - a_prev[els]) / h - np.einsum("epjx,ej->epx", grads[on], v[els])
-    re = np.einsum("epm,eqm->epq", Ep, Ep)
-    Q = np.zeros(len(sig_e))
-    Q[on] = sig_e[on] * vols[on] * np.einsum("pq,epq->e", _MASS_REF, re) / vols[on]
-    return float(np.sum(Q * vols)), Q
+class _JouleDevice:
+    """Device tables of the Tet10 Joule-power kernel (cfem_t10_joule_power)
+    for one mesh: the reference element's dN_j/dxi at its nodes
+    (em3d_tet10.py:122-137), its normalised mass matrix and sigma per
+    element."""
+
+    def __init__(self, dm, sig_e):
+        import torch
+        from ..fem.tet10 import _MASS_REF, shape_functions
+        _, dN_dL = shape_functions(_l_nodes())
+        dn = np.stack([dN_dL[..., 1] - dN_dL[..., 0], dN_dL[..., 2] - dN_dL[..., 0],
+                       dN_dL[..., 3] - dN_dL[..., 0]], axis=-1)
+        dev = dm.rt.device
+        self.dm = dm
+        self.dn = torch.from_numpy(np.ascontiguousarray(dn, dtype=float)).to(dev)
+        self.mref = torch.from_numpy(np.ascontiguousarray(_MASS_REF, dtype=float)).to(dev)
+        self.sigma = torch.from_numpy(np.ascontiguousarray(sig_e, dtype=float)).to(dev)
+
+    def power(self, a_prev, a_new, vcol, v, h, out, q=None):
+        """out[0] = the power of one step (device), q: density per element."""
+        rt, dm = self.dm.rt, self.dm
+        N.check(rt.lib.cfem_t10_joule_power(
+            rt.ctx, dm.n_elems, ptr(dm.elems), ptr(dm.nodes), ptr(self.sigma), ptr(a_prev),
+            ptr(a_new), ptr(vcol), ptr(v), float(h), ptr(self.dn), ptr(self.mref), ptr(out),
+            ptr(q), rt.stream()))
 
 
 def transient_joule_power_tet10(mesh, a_prev, a_new, v, sigma, h):
     """Instantaneous Joule power of one transient step and the per-element
-    density (em3d_tet10.py:665-692), vectorised over the conducting
-    elements."""
-    sig_e = _element_values(mesh, sigma)
-    els = np.asarray(mesh.elements)
-    p = np.asarray(mesh.nodes, dtype=float)[els[:, :4]]
-    J = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]], axis=2)
-    vols = np.abs(np.linalg.det(J)) / 6.0
-    return _joule_power(mesh, a_prev, a_new, np.asarray(v, dtype=float), sig_e, vols,
-                        _nodal_gradients_all(mesh), h)
+    density (em3d_tet10.py:665-692), on the device (one thread per element,
+    fixed-order sum)."""
+    import torch
+    dm = DeviceMesh(mesh)
+    dev = dm.rt.device
+    n = mesh.n_nodes
+    jd = _JouleDevice(dm, _element_values(mesh, sigma))
+
+    def up(a, shape):
+        return torch.from_numpy(np.ascontiguousarray(np.reshape(a, shape), dtype=float)).to(dev)
+    out = torch.zeros(1, dtype=torch.float64, device=dev)
+    q = torch.zeros(mesh.n_elements, dtype=torch.float64, device=dev)
+    jd.power(up(a_prev, 3 * n), up(a_new, 3 * n), torch.arange(n, dtype=torch.int64, device=dev),
+             up(v, n), h, out, q)
+    return float(out.cpu()[0]), q.cpu().numpy()
 
 
 def transient_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, t_end=1.0, dt=0.1,
@@ -655,8 +676,11 @@ def transient_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, t_end=1.0, dt=0.
     air gauge mass), so every step is one device PCG solve with a solve plan
     kept for the whole march (one CUDA graph launch per step) in place of
     the reference's LU; the Dirichlet values stay in x under a fixed-DOF
-    mask. The constraint-consistent V and the Joule power of each step are
-    computed on the host as the reference does.
+    mask. The constraint-consistent V of each step (em3d_tet10.py:485, 527)
+    is a second, warm-started device PCG solve on the conductors'
+    sigma-Laplacian in place of the reference's LU, and the Joule power a
+    device kernel (cfem_t10_joule_power): the fields stay on the GPU for the
+    whole march and come back once at its end.
     """
     import torch
 
@@ -722,16 +746,26 @@ def transient_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, t_end=1.0, dt=0.
     mode, rtol = D.solver_mode(precision, rtol)
     sysA = BlockSystem(rt, nx, 1, lp, li, lv, b, x, mask, keep=(lp, li, lv))
     plan = PcgPlan([sysA], mode, rtol, max_iter)
-    solve_S = spla.factorized(S.tocsc())
-    grads = _nodal_gradients_all(mesh)
-    els = np.asarray(mesh.elements)
-    pc = np.asarray(mesh.nodes, dtype=float)[els[:, :4]]
-    Jc = np.stack([pc[:, 1] - pc[:, 0], pc[:, 2] - pc[:, 0], pc[:, 3] - pc[:, 0]], axis=2)
-    vols = np.abs(np.linalg.det(Jc)) / 6.0
-    GsT = Gs.T.tocsr()
+    # the constraint-consistent V of each step, S v = -Gs^T (a_new - a_prev) / h
+    # (em3d_tet10.py:485, 527): a device FP64 PCG solve (S is the conductors'
+    # sigma-Laplacian with one node pinned per part: SPD), warm-started
+    vmode, vrtol = D.solver_mode("fp64", None)
+    vcol = np.full(n, -1, dtype=np.int64)
+    vcol[v_nodes] = np.arange(n_v)
+    d_vcol = torch.from_numpy(vcol).to(dev)
+    v_b = torch.zeros(max(n_v, 1), dtype=torch.float64, device=dev)
+    v_x = torch.zeros(max(n_v, 1), dtype=torch.float64, device=dev)
+    planV = None
+    if n_v:
+        gp_, gi_, gv_, _ = csr_to_device(rt, Gs.T.tocsr())
+        sp_, si_, sv_, _ = csr_to_device(rt, S)
+        sysV = BlockSystem(rt, n_v, 1, sp_, si_, sv_, v_b, v_x, keep=(sp_, si_, sv_))
+        planV = PcgPlan([sysV], vmode, vrtol)
+    jd = _JouleDevice(dm, sig_e)
+    a_prev_d = x[:3 * n].clone()
+    adot = torch.empty(3 * n, dtype=torch.float64, device=dev)
 
     times = np.linspace(0.0, t_end, n_steps + 1)
-    P = np.zeros(n_steps + 1)
     if history is True:
         rec = np.ones(n_steps + 1, dtype=bool)
     elif isinstance(history, (tuple, list)):
@@ -742,13 +776,13 @@ def transient_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, t_end=1.0, dt=0.
                              f"steps in [0, {t_end}]")
     else:
         rec = np.zeros(n_steps + 1, dtype=bool)
-    a_hist = np.zeros((int(rec.sum()), 3 * n)) if rec.any() else None
-    a_prev = x0[:3 * n].copy()
+    P_d = torch.zeros(n_steps + 1, dtype=torch.float64, device=dev)
+    hist_d = (torch.empty((int(rec.sum()), 3 * n), dtype=torch.float64, device=dev)
+              if rec.any() else None)
     nrec = 0
     if rec[0]:
-        a_hist[0] = a_prev
+        hist_d[0].copy_(a_prev_d)
         nrec = 1
-    v_end = np.zeros(n)
     infos = []
     try:
         for k in range(1, n_steps + 1):
@@ -761,21 +795,28 @@ def transient_eddy_current_tet10(mesh, nu=1.0 / MU0, sigma=0.0, t_end=1.0, dt=0.
             res = plan.solve()
             D.accept(res[0], rtol, f"time step {k}")
             infos.append(res[0])
-            a_new = x[:3 * n].cpu().numpy()
-            adot = (a_new - a_prev) / h
-            v_new = np.zeros(n)
-            v_new[v_nodes] = -solve_S(GsT @ adot)
-            P[k] = _joule_power(mesh, a_prev, a_new, v_new, sig_e, vols, grads, h)[0]
-            a_prev = a_new.copy()
-            v_end = v_new
+            if planV is not None:
+                N.check(lib.cfem_axpby(ctx, 3 * n, 1.0 / h, ptr(x), -1.0 / h, ptr(a_prev_d),
+                                       ptr(adot), rt.stream()))
+                N.check(lib.cfem_spmv(ctx, n_v, 1, ptr(gp_), ptr(gi_), ptr(gv_), -1.0,
+                                      ptr(adot), 0.0, ptr(v_b), rt.stream()))
+                D.accept(planV.solve()[0], vrtol, f"V of time step {k}")
+            jd.power(a_prev_d, x, d_vcol, v_x, h, P_d[k:k + 1])
+            a_prev_d.copy_(x[:3 * n])
             if rec[k]:
-                a_hist[nrec] = a_new
+                hist_d[nrec].copy_(a_prev_d)
                 nrec += 1
     finally:
         plan.close()
+        if planV is not None:
+            planV.close()
     D._record(infos)
-    out = {"times": times, "P": P, "a_end": a_prev.copy(), "v_end": v_end}
-    if a_hist is not None:
+    P = P_d.cpu().numpy()
+    v_end = np.zeros(n)
+    if n_v:
+        v_end[v_nodes] = v_x.cpu().numpy()
+    out = {"times": times, "P": P, "a_end": a_prev_d.cpu().numpy(), "v_end": v_end}
+    if hist_d is not None:
         out["t_hist"] = times[rec]
-        out["a_hist"] = a_hist
+        out["a_hist"] = hist_d.cpu().numpy()
     return out

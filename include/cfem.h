@@ -285,6 +285,26 @@ CFEM_API int cfem_element_stress(cfem_ctx *ctx, const double *d_nodes,
                                  const cfem_coef *temp, double alpha, double T_ref,
                                  double *d_sig, double *d_eps, void *stream);
 
+/* Joule power of one step of the transient Tet10 A-V march
+ * (em3d_tet10.py:665-692, transient_joule_power_tet10): for every element
+ * with d_sigma[e] > 0, the field at its 10 nodes
+ *   E_p = -(a_new_p - a_prev_p) / h - sum_j grad N_j(x_p) v_j,
+ * the density Q_e = sigma_e sum_pq mref_pq E_p . E_q (0 elsewhere), and the
+ * power *d_power = sum_e Q_e V_e, summed in a fixed order. d_elems: 10
+ * nodes per element (int32), d_nodes: 3 doubles per node; a_prev, a_new:
+ * 3 per node (node-major); v on the V nodes: d_vcol[node] is the node's
+ * index in d_v, or -1 (v = 0; d_v may be NULL if no node has one). d_dn:
+ * the reference element's dN_j/dxi_k at its node p (10 x 10 x 3, p-major);
+ * d_mref: its normalised mass matrix (10 x 10, the reference's _MASS_REF).
+ * d_q (optional): Q per element. Geometry from the corners (straight-edged
+ * elements). */
+CFEM_API int cfem_t10_joule_power(cfem_ctx *ctx, int64_t n_elems, const int32_t *d_elems,
+                                  const double *d_nodes, const double *d_sigma,
+                                  const double *d_a_prev, const double *d_a_new,
+                                  const int64_t *d_vcol, const double *d_v, double h,
+                                  const double *d_dn, const double *d_mref, double *d_power,
+                                  double *d_q, void *stream);
+
 /* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
  * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),
  * thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or QP). */

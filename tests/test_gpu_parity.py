@@ -277,6 +277,28 @@ def test_av_transient_golden(cf, golden, precision):
         assert np.linalg.norm(r[k] - ref) <= tol * np.linalg.norm(ref)
 
 
+def test_t10_joule_power_kernel_vs_oracle(cf):
+    """The device Joule-power kernel (cfem_t10_joule_power) against the
+    oracle's restatement of em3d_tet10.py:665-692 on seeded fields over a
+    mesh with conducting and non-conducting elements: power within 1e-12,
+    per-element densities entry-wise within 1e-12, and bitwise the same on a
+    repeat (fixed-order sum)."""
+    from cloudfem_b200.physics import em3d_tet10 as em
+    from oracle import cfem_oracle as O
+    m = cf.mesh.box_mesh_tet10(4, 3, 3)
+    mo = O.box_mesh_tet10(4, 3, 3)
+    rng = np.random.default_rng(7)
+    n = m.n_nodes
+    a0, a1, v = rng.normal(size=3 * n), rng.normal(size=3 * n), rng.normal(size=n)
+    P, Q = em.transient_joule_power_tet10(m, a0, a1, v, C.sigma_fn, 0.01)
+    Po, Qo = O.transient_joule_power_tet10(mo, a0, a1, v, C.sigma_fn, 0.01)
+    assert (Q == 0).any() and (Q > 0).any()
+    assert abs(P - Po) <= 1e-12 * abs(Po), (P, Po)
+    assert np.all(np.abs(Q - Qo) <= 1e-12 * np.abs(Qo) + 1e-300)
+    P2, _ = em.transient_joule_power_tet10(m, a0, a1, v, C.sigma_fn, 0.01)
+    assert P2 == P
+
+
 def test_av_magnetic_energy_golden(cf, golden):
     """W_m = Re(a^H K a)/4 with K assembled on the device."""
     from cloudfem_b200.physics import em3d_tet10 as em
