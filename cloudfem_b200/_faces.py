@@ -1,16 +1,21 @@
-"""Boundary-face integrals (host side; O(surface) work).
+"""Boundary-face integrals on the device (O(surface) work).
 
-Face lists come from the device candidate kernel (DeviceMesh.boundary_faces);
-the per-face integrals below are the reference's rules evaluated over all
-faces at once:
+Face lists come from the device face kernels (DeviceMesh.boundary_faces_device:
+cfem_face_candidates, cfem_face_exterior); the integrals are the reference's
+rules, evaluated by cfem_face_geometry (areas, quadrature points) and
+cfem_face_integrate (per-face terms, then a stable sort by node or pattern
+position and fixed-order sums into the device load vector and matrix):
 
-* P1 Neumann / Robin on 3-node faces with the centroid value
-  (cloudfem/fem/tet_heat.py:136-172);
+* P1 Neumann / Robin on 3-node faces with the centroid value and the exact
+  face mass h A / 12 (1 + d_ij) (cloudfem/fem/tet_heat.py:136-172);
 * Tet10 Neumann / Robin on 6-node faces with the 6-point degree-4 Dunavant
   rule (cloudfem/fem/tet10.py:295-435);
 * P1 traction, centroid value, t A / 3 per node (physics/elastic3d.py:171-186);
 * Tet10 traction with the 3-point degree-2 rule
   (physics/elastic_tet10.py:351-357, 494-508).
+
+Coefficients given as host functions are evaluated at the points the
+device computed; constants never leave the host.
 """
 
 import inspect
@@ -18,7 +23,8 @@ import inspect
 import numpy as np
 import scipy.sparse as sp
 
-from .device import evaluate
+from . import _native as N
+from .device import evaluate, ptr
 
 # 6-point Dunavant rule (barycentric points, weights summing to 1) as
 # tabulated by the reference (tet10.py:300-308).
@@ -54,17 +60,11 @@ FACE_N6 = face_shape6(TRI_L6)
 FACE_N3 = face_shape6(TRI_L3)
 
 
-def corner_geometry(nodes, faces):
-    """Centroid (F, 3) and area (F,) of the corner triangles."""
-    p = nodes[faces[:, :3]]
-    cen = p.mean(axis=1)
-    cr = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
-    return cen, 0.5 * np.linalg.norm(cr, axis=1), p
 
 
 def add_at(F, idx, vals):
     """F[idx] += vals with repeated indices summed (np.add.at semantics),
-    through np.bincount, which is much faster for large face sets."""
+    through np.bincount (host; used by host-side post-processing)."""
     idx = np.asarray(idx).ravel()
     vals = np.asarray(vals).ravel()
     if np.iscomplexobj(vals):
@@ -73,48 +73,6 @@ def add_at(F, idx, vals):
     else:
         F += np.bincount(idx, weights=vals, minlength=len(F))
 
-
-def _as_array(v, n):
-    return np.full(n, v) if np.isscalar(v) else v
-
-
-def coo_csr(rows, cols, data, n):
-    if len(data) == 0:
-        return sp.csr_matrix((n, n))
-    return sp.coo_matrix((np.concatenate(data),
-                          (np.concatenate(rows), np.concatenate(cols))),
-                         shape=(n, n)).tocsr()
-
-
-# ----------------------------------------------------------------- P1 faces
-
-def p1_neumann(nodes, faces, q, F):
-    cen, area, _ = corner_geometry(nodes, faces)
-    qv = _as_array(evaluate(q, cen), len(faces))
-    add_at(F, faces.ravel(), np.repeat(qv * area / 3.0, 3))
-
-
-def p1_robin(nodes, faces, h, tinf, F, rows, cols, data):
-    """Exact face mass h A/12 (1 + d_ij) and ambient load h T_inf A / 3."""
-    cen, area, _ = corner_geometry(nodes, faces)
-    hv = _as_array(evaluate(h, cen), len(faces))
-    tv = _as_array(evaluate(tinf, cen), len(faces))
-    fm = (np.ones((3, 3)) + np.eye(3)) / 12.0
-    rows.append(np.repeat(faces[:, :, None], 3, axis=2).ravel())
-    cols.append(np.repeat(faces[:, None, :], 3, axis=1).ravel())
-    data.append(((hv * area)[:, None, None] * fm).ravel())
-    add_at(F, faces.ravel(), np.repeat(hv * tv * area / 3.0, 3))
-
-
-def p1_traction(nodes, faces, comps, rhs):
-    cen, area, _ = corner_geometry(nodes, faces)
-    for c, v in enumerate(comps):
-        tv = _as_array(evaluate(0.0 if v is None else v, cen), len(faces))
-        add_at(rhs, (3 * faces + c).ravel(),
-                  np.repeat(tv * area / 3.0, 3))
-
-
-# ----------------------------------------------------------------- Tet10 faces
 
 def flux_fn(q):
     """float, f(x, y, z) or time-dependent f(x, y, z, t) (tet10.py:366-381)."""
@@ -130,37 +88,118 @@ def flux_fn(q):
     return (lambda x, y, z, t: q(x, y, z)), False
 
 
-def t10_points(nodes, faces, L):
-    _, area, pc = corner_geometry(nodes, faces)
-    return area, np.einsum("qc,fcd->fqd", L, pc)
+class Rule:
+    """A face quadrature rule as the device kernels take it: barycentric
+    points on the corners, weights, shape values (nq, npf) and, for Robin,
+    the mass tables mt[q] (npf, npf) with K_ab = A sum_q mt[q]_ab w_q h_q."""
+
+    def __init__(self, npf, bary, w, shape, mt):
+        self.npf = npf
+        self.bary = np.ascontiguousarray(bary, dtype=float)
+        self.w = np.ascontiguousarray(w, dtype=float)
+        self.shape = np.ascontiguousarray(shape, dtype=float)
+        self.mt = None if mt is None else np.ascontiguousarray(mt, dtype=float)
+        self.nq = len(self.w)
+        self._dev = {}
+
+    def device(self, rt):
+        """Device copies (bary, w, shape, mt), kept per device."""
+        import torch
+        key = str(rt.device)
+        if key not in self._dev:
+            def up(a):
+                return None if a is None else torch.from_numpy(a).to(rt.device)
+            self._dev[key] = (up(self.bary), up(self.w), up(self.shape), up(self.mt))
+        return self._dev[key]
 
 
-def t10_neumann(nodes, faces, q, t, F):
-    fn, _ = flux_fn(q)
-    area, xq = t10_points(nodes, faces, TRI_L6)
-    qv = evaluate(lambda x, y, z: fn(x, y, z, t), xq)
-    qv = np.broadcast_to(qv, xq.shape[:-1])
-    fe = area[:, None] * np.einsum("qa,fq->fa", FACE_N6, TRI_W6 * qv)
-    add_at(F, faces.ravel(), fe.ravel())
+# P1: the centroid value; Robin with the exact face mass (1 + d_ij) / 12
+P1 = Rule(3, [[1.0 / 3.0] * 3], [1.0], [[1.0 / 3.0] * 3],
+          [(np.ones((3, 3)) + np.eye(3)) / 12.0])
+# Tet10: Dunavant-6 for Neumann and Robin, the 3-point rule for traction
+T10 = Rule(6, TRI_L6, TRI_W6, FACE_N6, np.einsum("qa,qb->qab", FACE_N6, FACE_N6))
+T10_TRACTION = Rule(6, TRI_L3, TRI_W3, FACE_N3, None)
 
 
-def t10_robin(nodes, faces, h, tinf, F, rows, cols, data):
-    area, xq = t10_points(nodes, faces, TRI_L6)
-    hv = np.broadcast_to(evaluate(h, xq), xq.shape[:-1])
-    tv = np.broadcast_to(evaluate(tinf, xq), xq.shape[:-1])
-    Ke = area[:, None, None] * np.einsum("qa,fq,qb->fab", FACE_N6,
-                                         TRI_W6 * hv, FACE_N6)
-    fe = area[:, None] * np.einsum("qa,fq->fa", FACE_N6, TRI_W6 * hv * tv)
-    add_at(F, faces.ravel(), fe.ravel())
-    rows.append(np.repeat(faces[:, :, None], 6, axis=2).ravel())
-    cols.append(np.repeat(faces[:, None, :], 6, axis=1).ravel())
-    data.append(Ke.ravel())
+def _geometry(dm, faces_d, rule, need_pts):
+    """Face areas (device) and, when asked, the quadrature points (host,
+    (F, nq, 3)) for evaluating host functions."""
+    import torch
+    rt = dm.rt
+    nf = int(faces_d.shape[0])
+    area = torch.empty(max(nf, 1), dtype=torch.float64, device=rt.device)
+    pts = (torch.empty((max(nf, 1), rule.nq, 3), dtype=torch.float64, device=rt.device)
+           if need_pts else None)
+    bary = rule.device(rt)[0]
+    N.check(rt.lib.cfem_face_geometry(rt.ctx, rule.npf, nf, ptr(faces_d), ptr(dm.nodes),
+                                      rule.nq, ptr(bary), ptr(pts), ptr(area), rt.stream()))
+    return area, (pts[:nf].cpu().numpy() if need_pts else None)
 
 
-def t10_traction(nodes, faces, comps, rhs):
-    area, xq = t10_points(nodes, faces, TRI_L3)
-    tv = np.stack([np.broadcast_to(evaluate(0.0 if v is None else v, xq),
-                                   xq.shape[:-1]) for v in comps], axis=-1)
-    fe = area[:, None, None] * np.einsum("q,qa,fqc->fac", TRI_W3, FACE_N3, tv)
-    dofs = (3 * faces[:, :, None] + np.arange(3)).reshape(len(faces), -1)
-    add_at(rhs, dofs.ravel(), fe.ravel())
+def _host_values(spec, pts, nf, nq):
+    """A float, or a host function's values at the points, as (nf, nq)."""
+    v = evaluate(spec, pts) if callable(spec) else float(spec)
+    return np.broadcast_to(np.asarray(v, dtype=float), (nf, nq))
+
+
+def _to_device(rt, a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=float).ravel()).to(rt.device)
+
+
+def add_load(dm, faces_d, rule, specs, F):
+    """F (device, ncomp values per node) += A sum_q w_q N_a(x_q) load(x_q)
+    over the faces, one spec per component (None: 0)."""
+    rt = dm.rt
+    nf = int(faces_d.shape[0])
+    if nf == 0:
+        return
+    specs = [0.0 if v is None else v for v in specs]
+    area, pts = _geometry(dm, faces_d, rule, any(callable(v) for v in specs))
+    vals = np.stack([_host_values(v, pts, nf, rule.nq) for v in specs], axis=-1)
+    d_vals = _to_device(rt, vals)
+    _, w, shape, _ = rule.device(rt)
+    N.check(rt.lib.cfem_face_integrate(
+        rt.ctx, rule.npf, nf, ptr(faces_d), ptr(area), rule.nq, ptr(w), ptr(shape),
+        len(specs), ptr(d_vals), ptr(F), None, None, None, None, dm.n_nodes, None,
+        rt.stream()))
+
+
+def add_robin(dm, faces_d, rule, h, tinf, F, K):
+    """Robin convection over the faces: K (device node-pattern values) +=
+    A sum_q mt_q w_q h(x_q), F += A sum_q w_q N_a h(x_q) T_inf(x_q)."""
+    rt = dm.rt
+    nf = int(faces_d.shape[0])
+    if nf == 0:
+        return
+    area, pts = _geometry(dm, faces_d, rule, callable(h) or callable(tinf))
+    hv = _host_values(h, pts, nf, rule.nq)
+    load = hv * _host_values(tinf, pts, nf, rule.nq)
+    d_h, d_load = _to_device(rt, hv), _to_device(rt, load)
+    _, w, shape, mt = rule.device(rt)
+    pat = dm.pattern
+    N.check(rt.lib.cfem_face_integrate(
+        rt.ctx, rule.npf, nf, ptr(faces_d), ptr(area), rule.nq, ptr(w), ptr(shape), 1,
+        ptr(d_load), ptr(F), ptr(d_h), ptr(mt), pat.row_ptr, pat.col, dm.n_nodes, ptr(K),
+        rt.stream()))
+
+
+def face_csr(dm, face_lists, K):
+    """The reference's CSR of face terms (tet_heat.py:160-172): one entry per
+    pair of nodes of a common face (duplicates summed, indices sorted),
+    its value read from the device pattern values K."""
+    n = dm.n_nodes
+    face_lists = [f for f in face_lists if len(f)]
+    if not face_lists:
+        return sp.csr_matrix((n, n))
+    rows = np.concatenate([np.repeat(f[:, :, None], f.shape[1], axis=2).ravel()
+                           for f in face_lists])
+    cols = np.concatenate([np.repeat(f[:, None, :], f.shape[1], axis=1).ravel()
+                           for f in face_lists])
+    S = sp.coo_matrix((np.ones(len(rows)), (rows, cols)), shape=(n, n)).tocsr()
+    S.sum_duplicates()
+    S.sort_indices()
+    full = dm.pattern.to_scipy(1, K)
+    r = np.repeat(np.arange(n), np.diff(S.indptr))
+    S.data = np.asarray(full[r, S.indices]).ravel().astype(float)
+    return S

@@ -104,6 +104,11 @@ SIGNATURES = [
     ("cfem_element_stress", ctypes.c_int,
      [_vp, _vp, _vp, _i64, _i32, _vp, _f64, _f64, ctypes.POINTER(Coef), _f64,
       _f64, _vp, _vp, _vp]),
+    ("cfem_face_geometry", ctypes.c_int,
+     [_vp, _i32, _i64, _vp, _vp, _i32, _vp, _vp, _vp, _vp]),
+    ("cfem_face_integrate", ctypes.c_int,
+     [_vp, _i32, _i64, _vp, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+      _vp, _vp]),
     ("cfem_t10_joule_power", ctypes.c_int,
      [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f64, _vp, _vp, _vp, _vp, _vp]),
     ("cfem_assemble_curlcurl", ctypes.c_int,

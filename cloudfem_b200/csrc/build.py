@@ -15,7 +15,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(os.path.dirname(HERE), "libcfem.so")
 SOURCES = ["cfem_core.cu", "cfem_pattern.cu", "cfem_assemble.cu",
-           "cfem_dirichlet.cu", "cfem_solve.cu", "cfem_complex.cu", "cfem_em.cu"]
+           "cfem_dirichlet.cu", "cfem_solve.cu", "cfem_complex.cu", "cfem_em.cu",
+           "cfem_faces.cu"]
 HEADERS = ["cfem_common.cuh", "cfem_tables.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

@@ -330,12 +330,17 @@ class DeviceMesh:
         the set can share a key with such a face, so counting among the
         candidates is exact.
         """
+        return self.boundary_faces_device(name, tet10).cpu().numpy()
+
+    def boundary_faces_device(self, name, tet10=False):
+        """boundary_faces as a device int64 tensor (F, 3 or 6)."""
         torch = _torch()
         host = self.host
         ids = np.asarray(host.boundaries[name], dtype=np.int64)
         width = 6 if tet10 else 3
+        empty = torch.zeros((0, width), dtype=torch.int64, device=self.rt.device)
         if ids.size == 0 or self.n_elems == 0:
-            return np.zeros((0, width), dtype=np.int64)
+            return empty
         inset = torch.zeros(self.n_nodes, dtype=torch.uint8,
                             device=self.rt.device)
         inset[torch.from_numpy(ids).to(self.rt.device)] = 1
@@ -348,14 +353,14 @@ class DeviceMesh:
             ctypes.byref(cnt), self.rt.stream()))
         nc = cnt.value
         if nc == 0:
-            return np.zeros((0, width), dtype=np.int64)
+            return empty
         ids = torch.empty(nc, dtype=torch.int64, device=self.rt.device)
         nodes = torch.empty(nc * width, dtype=torch.int64, device=self.rt.device)
         nout = N._i64()
         N.check(self.rt.lib.cfem_face_exterior(
             self.rt.ctx, ptr(self.elems), self.npe, 1 if tet10 else 0, ptr(out), nc,
             self.n_nodes, ptr(ids), ptr(nodes), ctypes.byref(nout), self.rt.stream()))
-        return nodes[: nout.value * width].cpu().numpy().reshape(-1, width)
+        return nodes[: nout.value * width].reshape(-1, width)
 
 
 # ------------------------------------------------------------ solver

@@ -10,7 +10,8 @@ Drop-in for cloudfem/fem/tet10.py (``__all__`` at :52-56):
   gradients staged in shared memory.
 * ``assemble_mass_tet10`` (:229-249): rho_cp(centroid) V MASS_REF.
 * ``_boundary_faces10`` (:329-352), ``assemble_boundary_terms_tet10``
-  (:438-464) on 6-node faces with the 6-point Dunavant rule.
+  (:438-464) on 6-node faces with the 6-point Dunavant rule, integrated on
+  the device (``_faces``).
 * ``solve_tet10_poisson`` (:168-178) and ``transient_heat_tet10``
   (:467-548) solve on the device.
 """
@@ -25,7 +26,7 @@ from .. import _faces
 from .._driver import THETA, n_steps_of, solve_block, theta_march
 from ..device import DeviceMesh, fixed_scalar
 from ..mesh.tet10_mesh import EDGES
-from .tet_heat import add_csr_into
+from .tet_heat import _terms, add_into, boundary_csr
 from .tet_poisson import apply_dirichlet  # noqa: F401
 
 __all__ = [
@@ -156,36 +157,36 @@ def _boundary_faces10(mesh, name):
     return DeviceMesh(mesh).boundary_faces(name, tet10=True)
 
 
+def _flux_at(q, t):
+    """A Neumann flux spec at time t: a float, or f(x, y, z) (tet10.py:366-381)."""
+    if not callable(q):
+        return float(q)
+    fn, timedep = _faces.flux_fn(q)
+    return (lambda x, y, z: fn(x, y, z, t)) if timedep else q
+
+
 def _neumann_load(dm, mesh, neumann, t):
-    F = np.zeros(mesh.n_nodes)
-    for name, q in neumann.items():
-        _faces.t10_neumann(mesh.nodes, dm.boundary_faces(name, tet10=True), q,
-                           t, F)
+    """Device Neumann load of the named faces at time t."""
+    _, F, _ = _terms(dm, mesh, {name: _flux_at(q, t) for name, q in neumann.items()},
+                     None, _faces.T10, True)
     return F
 
 
 def _robin_terms(dm, mesh, robin):
-    F = np.zeros(mesh.n_nodes)
-    rows, cols, data = [], [], []
-    for name, (h, tinf) in robin.items():
-        _faces.t10_robin(mesh.nodes, dm.boundary_faces(name, tet10=True), h,
-                         tinf, F, rows, cols, data)
-    return _faces.coo_csr(rows, cols, data, mesh.n_nodes), F
+    """Device Robin terms: (K_add node-pattern values, F_add, face lists)."""
+    return _terms(dm, mesh, None, robin, _faces.T10, True)
 
 
 def assemble_boundary_terms_tet10(mesh, neumann=None, robin=None, t=0.0):
     """(K_add csr, F_add) of Neumann and Robin terms at time t."""
     dm = DeviceMesh(mesh)
     n = mesh.n_nodes
-    F = np.zeros(n)
+    neu = {name: _flux_at(q, t) for name, q in (neumann or {}).items()}
+    K_add, F, faces = _terms(dm, mesh, neu, robin, _faces.T10, True)
     K = sp.csr_matrix((n, n))
-    if neumann:
-        F += _neumann_load(dm, mesh, neumann, t)
     if robin:
-        Kr, Fr = _robin_terms(dm, mesh, robin)
-        K = K + Kr
-        F += Fr
-    return K, F
+        K = K + boundary_csr(dm, K_add, faces)
+    return K, F.cpu().numpy()
 
 
 def transient_heat_tet10(mesh, k=1.0, rho_cp=1.0, f=0.0, bc=None,
@@ -202,9 +203,9 @@ def transient_heat_tet10(mesh, k=1.0, rho_cp=1.0, f=0.0, bc=None,
     dev = dm.rt.device
     K, F = dm.assemble(N.OP_T10_STIFF, coef=k, load=f)
     if robin:
-        K_add, F_add = _robin_terms(dm, mesh, robin)
-        add_csr_into(dm, K, K_add)
-        F = F + torch.from_numpy(F_add).to(dev)
+        K_add, F_add, _ = _robin_terms(dm, mesh, robin)
+        K = add_into(dm, K, K_add)
+        F = F + F_add
     load_fn = None
     if neumann:
         timedep = any(_faces.flux_fn(q)[1] for q in neumann.values())
@@ -215,10 +216,9 @@ def transient_heat_tet10(mesh, k=1.0, rho_cp=1.0, f=0.0, bc=None,
                 Fs = ((1.0 - theta) * _neumann_load(dm, mesh, neumann, step * h)
                       + theta * _neumann_load(dm, mesh, neumann,
                                               (step + 1) * h))
-                return base + torch.from_numpy(Fs).to(dev)
+                return base + Fs
         else:
-            F = F + torch.from_numpy(_neumann_load(dm, mesh, neumann,
-                                                   0.0)).to(dev)
+            F = F + _neumann_load(dm, mesh, neumann, 0.0)
     C, _ = dm.assemble(N.OP_T10_MASS, coef=rho_cp)
     n_steps = n_steps_of(t_end, dt)
     idx, vals = fixed_scalar(mesh, bc)

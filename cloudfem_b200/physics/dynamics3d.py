@@ -108,7 +108,7 @@ def _march(rt, n, Mop, Cop, Kop, Khat_sys, M_sys, F, t_end, n_steps, u, v, beta,
     mode, rtol = solver_mode("fp64", None)
 
     def dvec(a):
-        t = torch.from_numpy(np.ascontiguousarray(a, dtype=float)).to(dev)
+        t = torch.from_numpy(np.array(a, dtype=float)).to(dev)
         if mask is not None:
             t[mask.bool()] = 0.0
         return t

@@ -70,14 +70,13 @@ def _assemble(dm, mesh, op, E, nu, body, traction, T, alpha, T_ref, tet10):
     vals, rhs = dm.assemble_elastic(op, E, nu, body=body, T=T, alpha=alpha,
                                     T_ref=T_ref)
     if traction:
-        extra = np.zeros(3 * mesh.n_nodes)
+        # face loads on the device into a separate vector, then added once
+        # (the reference sums the traction vector before adding it)
+        extra = torch.zeros(3 * mesh.n_nodes, dtype=torch.float64, device=dm.rt.device)
+        rule = _faces.T10_TRACTION if tet10 else _faces.P1
         for name, comps in traction.items():
-            faces = dm.boundary_faces(name, tet10=tet10)
-            if tet10:
-                _faces.t10_traction(mesh.nodes, faces, comps, extra)
-            else:
-                _faces.p1_traction(mesh.nodes, faces, comps, extra)
-        rhs += torch.from_numpy(extra).to(dm.rt.device)
+            _faces.add_load(dm, dm.boundary_faces_device(name, tet10), rule, list(comps), extra)
+        rhs += extra
     return vals, rhs
 
 

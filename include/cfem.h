@@ -285,6 +285,34 @@ CFEM_API int cfem_element_stress(cfem_ctx *ctx, const double *d_nodes,
                                  const cfem_coef *temp, double alpha, double T_ref,
                                  double *d_sig, double *d_eps, void *stream);
 
+/* Boundary-face geometry (tet_heat.py:123-134, tet10.py:354-360): for each
+ * of n_faces faces (npf = 3 or 6 node ids, int64; the first three are the
+ * corners) the corner triangle's area d_area[f] = |e1 x e2| / 2 and, if
+ * d_pts is given, its nq (1..8) quadrature points d_pts[(f nq + q) 3 + d]
+ * = sum_c d_bary[q][c] x_c (nq = 1: the centroid (x0 + x1 + x2) / 3). */
+CFEM_API int cfem_face_geometry(cfem_ctx *ctx, int32_t npf, int64_t n_faces,
+                                const int64_t *d_faces, const double *d_nodes, int32_t nq,
+                                const double *d_bary, double *d_pts, double *d_area,
+                                void *stream);
+/* Boundary-face integrals (Neumann / traction loads, Robin terms;
+ * tet_heat.py:136-172, tet10.py:362-464, elastic3d.py:171-186,
+ * elastic_tet10.py:494-508). Per face, with the rule's weights d_w[q],
+ * shape values d_shape[q][a] and mass tables d_mt[q][a][b]:
+ *   d_F[node_a ncomp + c] += A sum_q d_shape[q][a] (w_q d_load[(f nq + q) ncomp + c])
+ *   d_vals[pos(node_a, node_b)] += A sum_q d_mt[q][a][b] (w_q d_h[f nq + q])
+ * where pos is the entry's position in the node pattern (d_row_ptr, d_col,
+ * n_nodes rows, sorted columns). Either part may be skipped (d_load or d_h
+ * NULL). Contributions to one node or entry are summed in face order and
+ * added once (stable sort by key), so results are bitwise reproducible.
+ * CFEM_ERR_INVALID if a face pair is outside the pattern (nothing added). */
+CFEM_API int cfem_face_integrate(cfem_ctx *ctx, int32_t npf, int64_t n_faces,
+                                 const int64_t *d_faces, const double *d_area, int32_t nq,
+                                 const double *d_w, const double *d_shape, int32_t ncomp,
+                                 const double *d_load, double *d_F, const double *d_h,
+                                 const double *d_mt, const int32_t *d_row_ptr,
+                                 const int32_t *d_col, int64_t n_nodes, double *d_vals,
+                                 void *stream);
+
 /* Joule power of one step of the transient Tet10 A-V march
  * (em3d_tet10.py:665-692, transient_joule_power_tet10): for every element
  * with d_sigma[e] > 0, the field at its 10 nodes
