@@ -666,17 +666,15 @@ def transient_robin():
 def _transient_device_march(dm, mesh, precision, n_steps, rtol):
     """Pattern + K, C, F and Robin terms + theta march on resident inputs;
     returns the final field on the device and the per-step solve records."""
-    import torch
-
     from cloudfem_b200 import _native as N
     from cloudfem_b200._driver import last_solve_info, theta_march
-    from cloudfem_b200.fem.tet_heat import _terms, add_csr_into
+    from cloudfem_b200.fem.tet_heat import _terms, add_into
     p = TRANSIENT_PARAMS
     dm._pattern = None
     K, F = dm.assemble(N.OP_P1_STIFF, coef=p["k"], load=transient_source)
-    K_add, F_add = _terms(dm, mesh, None, transient_robin())
-    add_csr_into(dm, K, K_add)
-    F = F + torch.from_numpy(F_add).to(dm.rt.device)
+    K_add, F_add, _ = _terms(dm, mesh, None, transient_robin())
+    K = add_into(dm, K, K_add)
+    F = F + F_add
     C, _ = dm.assemble(N.OP_P1_MASS, coef=p["rho_cp"])
     empty = np.zeros(0, dtype=np.int64)
     _, T = theta_march(dm, K, C, F, empty, np.zeros(0), n_steps * p["dt"],

@@ -105,24 +105,6 @@ def _dirichlet_values(mesh, bc):
     return dict(zip(idx.tolist(), vals.tolist()))
 
 
-def add_csr_into(dm, vals, K_add):
-    """vals += K_add on the mesh pattern (K + K_add, tet_heat.py:227-230)."""
-    import torch
-    if K_add.nnz == 0:
-        return
-    K_add = K_add.tocsr()
-    K_add.sum_duplicates()
-    K_add.sort_indices()
-    rt = dm.rt
-    dev = rt.device
-    ap = torch.from_numpy(K_add.indptr.astype(np.int32)).to(dev)
-    ai = torch.from_numpy(K_add.indices.astype(np.int32)).to(dev)
-    av = torch.from_numpy(K_add.data.astype(np.float64)).to(dev)
-    N.check(rt.lib.cfem_csr_add_subset(rt.ctx, dm.pattern.handle, N.ptr(ap),
-                                       N.ptr(ai), N.ptr(av), dm.n_nodes,
-                                       N.ptr(vals), rt.stream()))
-
-
 def transient_heat_tet(mesh, k=1.0, rho_cp=1.0, f=0.0, bc=None,
                        neumann=None, robin=None, t_end=1.0, dt=0.1,
                        T0=0.0, method="cn", *, precision="fp64", rtol=None,
