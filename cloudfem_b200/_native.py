@@ -62,6 +62,11 @@ class AssemblyJob(ctypes.Structure):
                 ("d_rhs", _vp)]
 
 
+class MixedJob(ctypes.Structure):
+    _fields_ = [("n_rows", _i64), ("bs", _i32), ("reserved", _i32), ("row_ptr", _vp),
+                ("col", _vp), ("vals64", _vp), ("vals32", _vp)]
+
+
 class LinSys(ctypes.Structure):
     _fields_ = [("n_rows", _i64), ("bs", _i32), ("precond", _i32),
                 ("d_row_ptr", _vp), ("d_col", _vp), ("d_vals64", _vp),
@@ -133,6 +138,7 @@ SIGNATURES = [
       ctypes.POINTER(_i64), _vp]),
     ("cfem_mixed_matrix", ctypes.c_int,
      [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
+    ("cfem_mixed_matrix_batch", ctypes.c_int, [_vp, ctypes.POINTER(MixedJob), _i32, _vp]),
     ("cfem_pcg_solve", ctypes.c_int,
      [_vp, ctypes.POINTER(LinSys), _i32, ctypes.POINTER(SolveStats), _vp]),
     ("cfem_pcg_plan_create", ctypes.c_int,

@@ -193,9 +193,27 @@ class Batch:
             N.check(self.rt.lib.cfem_assemble_batch(
                 self.rt.ctx, op, jobs, len(sel), self.rt.stream()))
 
+    def _mixed_operators(self):
+        """FP32 difference-form operators of every problem from the current
+        FP64 values, in one launch (cfem_mixed_matrix_batch); the FP32
+        arrays are kept between solves."""
+        import torch
+        jobs = (N.MixedJob * len(self.items))()
+        for i, it in enumerate(self.items):
+            if it.get("vals32") is None:
+                it["vals32"] = torch.empty(it["vals"].numel(), dtype=torch.float32,
+                                           device=it["vals"].device)
+            pat = it["dm"].pattern
+            jobs[i] = N.MixedJob(it["dm"].n_nodes, 1, 0, pat.row_ptr, pat.col,
+                                 ptr(it["vals"]), ptr(it["vals32"]))
+        N.check(self.rt.lib.cfem_mixed_matrix_batch(self.rt.ctx, jobs, len(self.items),
+                                                    self.rt.stream()))
+
     def solve(self, precision="mixed", rtol=None, max_iter=None, fresh=True):
         """One batched PCG over every problem; returns SolveResult list."""
         mode, rtol = solver_mode(precision, rtol)
+        if mode == N.SOLVE_MIXED:
+            self._mixed_operators()
         systems = []
         x_all = getattr(self, "x_all", None)
         if fresh and x_all is not None:
@@ -206,7 +224,8 @@ class Batch:
             dm = it["dm"]
             pat = dm.pattern
             sysm = BlockSystem(self.rt, dm.n_nodes, 1, pat.row_ptr, pat.col,
-                               it["vals"], it["rhs"], it["x"], it["mask"])
+                               it["vals"], it["rhs"], it["x"], it["mask"],
+                               vals32=it.get("vals32") if mode == N.SOLVE_MIXED else None)
             it["system"] = sysm
             systems.append(sysm)
         self.results = pcg(systems, mode, rtol, max_iter)

@@ -971,32 +971,82 @@ k_pcg_persistent(const SysDev *__restrict__ sys, SysState *st,
 }
 
 // FP32 difference-form operator: off-diagonal blocks rounded, the diagonal
-// slot holding the rounded FP64 block row sum (see phase_A).
+// slot holding the rounded FP64 block row sum (see phase_A). A group of
+// MX = 8 lanes per (block) row: lane s takes entries s, s + 8, ... (loads
+// and stores coalesced along the row), the FP64 sums meet in a fixed
+// shuffle tree, so every launch shape gives the same bits.
+constexpr int MX = 8;
+
+template <int BS>
+__device__ __forceinline__ void mixed_row(const int32_t *__restrict__ rp,
+                                          const int32_t *__restrict__ ci,
+                                          const double *__restrict__ v64,
+                                          float *__restrict__ v32, int64_t r, bool valid,
+                                          int sub) {
+    constexpr int B2 = BS * BS;
+    double sum[B2];
+#pragma unroll
+    for (int e = 0; e < B2; ++e) sum[e] = 0.0;
+    int32_t kd = -1;
+    if (valid) {
+        for (int32_t k = rp[r] + sub; k < rp[r + 1]; k += MX) {
+            if (ci[k] == r) kd = k;
+#pragma unroll
+            for (int e = 0; e < B2; ++e) {
+                const double a = v64[(int64_t)k * B2 + e];
+                sum[e] += a;
+                v32[(int64_t)k * B2 + e] = (float)a;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = MX / 2; o > 0; o >>= 1) {
+        kd = max(kd, __shfl_xor_sync(0xffffffffu, kd, o));
+#pragma unroll
+        for (int e = 0; e < B2; ++e) sum[e] += __shfl_xor_sync(0xffffffffu, sum[e], o);
+    }
+    __syncwarp();   // the off-diagonal stores above before the diagonal's
+    if (valid && kd >= 0)
+#pragma unroll
+        for (int e = 0; e < B2; ++e)
+            if (e % MX == sub) v32[(int64_t)kd * B2 + e] = (float)sum[e];
+}
+
 template <int BS>
 __global__ void k_mixed_matrix(int64_t n, const int32_t *__restrict__ rp,
                                const int32_t *__restrict__ ci,
                                const double *__restrict__ v64,
                                float *__restrict__ v32) {
-    constexpr int B2 = BS * BS;
-    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    double sum[B2];
-#pragma unroll
-    for (int e = 0; e < B2; ++e) sum[e] = 0.0;
-    int32_t kd = -1;
-    for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
-        if (ci[k] == r) kd = k;
-#pragma unroll
-        for (int e = 0; e < B2; ++e) {
-            const double a = v64[(int64_t)k * B2 + e];
-            sum[e] += a;
-            v32[(int64_t)k * B2 + e] = (float)a;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t r = t / MX;
+    mixed_row<BS>(rp, ci, v64, v32, r, r < n, (int)(t % MX));
+}
+
+// k_mixed_matrix over many systems of one block size in one launch: job j
+// covers global rows [row0_j, row0_j + n_j); a thread per row finds its
+// job by binary search.
+struct MixJob {
+    int64_t row0, n;
+    const int32_t *rp, *ci;
+    const double *v64;
+    float *v32;
+};
+
+template <int BS>
+__global__ void k_mixed_matrix_batch(const MixJob *__restrict__ jobs, int nj, int64_t total) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t g = t / MX;
+    const bool valid = g < total;
+    int lo = 0;
+    if (valid) {
+        int hi = nj - 1;
+        while (lo < hi) {   // last job with row0 <= g
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].row0 <= g) lo = mid; else hi = mid - 1;
         }
     }
-    if (kd >= 0) {
-#pragma unroll
-        for (int e = 0; e < B2; ++e) v32[(int64_t)kd * B2 + e] = (float)sum[e];
-    }
+    const MixJob &J = jobs[lo];
+    mixed_row<BS>(J.rp, J.ci, J.v64, J.v32, valid ? g - J.row0 : 0, valid, (int)(t % MX));
 }
 
 // Graph scheduler: one warp per chunk, one launch per phase group. X runs
@@ -1188,27 +1238,57 @@ __device__ void phase_A_vec1(const SysDev &S, const SysState *st, int64_t r0,
 // The diagonal entry, when the row has one, moves to the row's first slot
 // (the others keep their order): the staged difference-form SpMV takes the
 // row sum from there instead of testing every column against the row.
-template <typename T>
-__global__ void k_pad4(int64_t n, const int32_t *__restrict__ rp,
-                       const int32_t *__restrict__ ci, const T *__restrict__ v,
-                       int32_t *__restrict__ ci4, T *__restrict__ v4) {
-    const int lane = threadIdx.x & 31;
+// All systems of a plan in one launch: job j covers global rows
+// [row0_j, row0_j + n_j); one warp per row finds its job by binary search
+// and writes the row's columns once and its FP32 and / or FP64 values
+// (either may be absent).
+struct PadJob {
+    int64_t row0, n;
+    const int32_t *rp, *ci;
+    const float *v32;
+    float *va4;
+    const double *v64;
+    double *va4d;
+    int32_t *ci4;
+};
+
+__global__ void k_pad4_batch(const PadJob *__restrict__ jobs, int nj, int64_t total) {
+    // 8 lanes per row, four rows per warp step (more rows' loads in flight)
+    const int lane = threadIdx.x & 31, sub = lane & 7, grp = lane >> 3;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-        const int64_t kb = rp[i], len = rp[i + 1] - kb;
-        const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
-        const int64_t m = ((len + 3) >> 2) * 4;
-        int64_t dpos = -1;   // position of the diagonal entry
-        for (int64_t t0 = 0; t0 < len && dpos < 0; t0 += 32) {
-            const unsigned hit =
-                __ballot_sync(0xffffffffu, t0 + lane < len && ci[kb + t0 + lane] == (int32_t)i);
-            if (hit) dpos = t0 + __ffs(hit) - 1;
+    for (int64_t g0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 4; g0 < total;
+         g0 += nw * 4) {
+        const int64_t g = g0 + grp;
+        const bool valid = g < total;
+        int lo = 0;
+        if (valid) {
+            int hi = nj - 1;
+            while (lo < hi) {   // last job with row0 <= g
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].row0 <= g) lo = mid; else hi = mid - 1;
+            }
         }
-        for (int64_t t = lane; t < m; t += 32) {
+        const PadJob &J = jobs[lo];
+        const int64_t i = valid ? g - J.row0 : 0;
+        const int64_t kb = valid ? J.rp[i] : 0, len = valid ? J.rp[i + 1] - kb : 0;
+        // position of the diagonal entry (the first, should a row repeat it)
+        int64_t dpos = INT64_MAX;
+        for (int64_t t = sub; t < len; t += 8)
+            if (J.ci[kb + t] == (int32_t)i && t < dpos) dpos = t;
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            const int64_t other = __shfl_xor_sync(0xffffffffu, dpos, o);
+            dpos = other < dpos ? other : dpos;
+        }
+        if (dpos == INT64_MAX) dpos = -1;
+        const int64_t o = ((kb + 3 * i + 3) >> 2) * 4;
+        const int64_t m = valid ? ((len + 3) >> 2) * 4 : 0;
+        for (int64_t t = sub; t < m; t += 8) {
             // slot t <- entry src: diagonal first, then the others in order
             const int64_t src = dpos < 0 ? t : (t == 0 ? dpos : (t <= dpos ? t - 1 : t));
-            ci4[o + t] = t < len ? ci[kb + src] : (int32_t)i;
-            v4[o + t] = t < len ? v[kb + src] : (T)0;
+            J.ci4[o + t] = t < len ? J.ci[kb + src] : (int32_t)i;
+            if (J.va4) J.va4[o + t] = t < len ? J.v32[kb + src] : 0.0f;
+            if (J.va4d) J.va4d[o + t] = t < len ? J.v64[kb + src] : 0.0;
         }
     }
 }
@@ -2621,11 +2701,49 @@ extern "C" int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
     CFEM_TRY(set_device(ctx->device));
     cudaStream_t s = (cudaStream_t)stream;
     if (bs == 1)
-        CFEM_LAUNCH(k_mixed_matrix<1>, grid_for(n_rows, 128), 128, 0, s, n_rows,
+        CFEM_LAUNCH(k_mixed_matrix<1>, grid_for(n_rows * MX, 128), 128, 0, s, n_rows,
                     d_row_ptr, d_col, d_vals64, d_vals32);
     else
-        CFEM_LAUNCH(k_mixed_matrix<3>, grid_for(n_rows, 128), 128, 0, s, n_rows,
+        CFEM_LAUNCH(k_mixed_matrix<3>, grid_for(n_rows * MX, 128), 128, 0, s, n_rows,
                     d_row_ptr, d_col, d_vals64, d_vals32);
+    return CFEM_OK;
+    CFEM_API_END
+}
+
+extern "C" int cfem_mixed_matrix_batch(cfem_ctx *ctx, const cfem_mixed_job *jobs,
+                                       int32_t n_jobs, void *stream) {
+    CFEM_API_BEGIN
+    CFEM_CHECK(ctx && n_jobs >= 0 && (n_jobs == 0 || jobs), CFEM_ERR_INVALID,
+               "cfem_mixed_matrix_batch: bad args");
+    std::vector<MixJob> by_bs[2];
+    int64_t rows[2] = {0, 0};
+    for (int j = 0; j < n_jobs; ++j) {
+        const cfem_mixed_job &J = jobs[j];
+        CFEM_CHECK(J.n_rows >= 0 && (J.bs == 1 || J.bs == 3) &&
+                       (J.n_rows == 0 || (J.d_row_ptr && J.d_col && J.d_vals64 && J.d_vals32)),
+                   CFEM_ERR_INVALID, "cfem_mixed_matrix_batch: bad job %d", j);
+        if (J.n_rows == 0) continue;
+        const int t = J.bs == 3 ? 1 : 0;
+        by_bs[t].push_back(MixJob{rows[t], J.n_rows, J.d_row_ptr, J.d_col, J.d_vals64, J.d_vals32});
+        rows[t] += J.n_rows;
+    }
+    if (rows[0] + rows[1] == 0) return CFEM_OK;
+    CFEM_TRY(set_device(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int t = 0; t < 2; ++t) {
+        if (by_bs[t].empty()) continue;
+        MixJob *d = nullptr;
+        CFEM_TRY(tmp_alloc(&d, by_bs[t].size(), s));
+        CFEM_CUDA(cudaMemcpyAsync(d, by_bs[t].data(), by_bs[t].size() * sizeof(MixJob),
+                                  cudaMemcpyHostToDevice, s));
+        if (t == 0)
+            CFEM_LAUNCH(k_mixed_matrix_batch<1>, grid_for(rows[t] * MX, 128), 128, 0, s,
+                        (const MixJob *)d, (int)by_bs[t].size(), rows[t]);
+        else
+            CFEM_LAUNCH(k_mixed_matrix_batch<3>, grid_for(rows[t] * MX, 128), 128, 0, s,
+                        (const MixJob *)d, (int)by_bs[t].size(), rows[t]);
+        tmp_free(d, s);
+    }
     return CFEM_OK;
     CFEM_API_END
 }
@@ -2751,6 +2869,8 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 // (Re)build the working copies of the matrix values on stream s.
 static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last = -1) {
     if (last < 0) last = P->n_systems;
+    std::vector<PadJob> pad_jobs;
+    int64_t pad_rows = 0;
     for (int i = first; i < last; ++i) {
         SysDev &S = P->hs[i];
         if (S.bs == 3 && S.sell) {
@@ -2796,12 +2916,35 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
                 else
                     CFEM_LAUNCH(k_sell_fill<double>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n, S.rp,
                                 S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
-            } else if (S.mode == CFEM_SOLVE_MIXED)
-                CFEM_LAUNCH(k_pad4<float>, g, 256, 0, s, S.n, S.rp, S.ci, S.v32,
-                            (int32_t *)S.ci4, (float *)S.va4);
-            CFEM_LAUNCH(k_pad4<double>, g, 256, 0, s, S.n, S.rp, S.ci, S.v64,
-                        (int32_t *)S.ci4, (double *)S.va4d);
+            }
+            // unit-padded copies: one batched launch for all systems below
+            PadJob J;
+            J.row0 = pad_rows;
+            J.n = S.n;
+            J.rp = S.rp;
+            J.ci = S.ci;
+            const bool f32 = S.mode == CFEM_SOLVE_MIXED && !S.sell;
+            J.v32 = f32 ? S.v32 : nullptr;
+            J.va4 = f32 ? (float *)S.va4 : nullptr;
+            J.v64 = S.v64;
+            J.va4d = (double *)S.va4d;
+            J.ci4 = (int32_t *)S.ci4;
+            if (S.n > 0) {
+                pad_jobs.push_back(J);
+                pad_rows += S.n;
+            }
+            (void)g;
         }
+    }
+    if (!pad_jobs.empty()) {
+        PadJob *d_jobs = nullptr;
+        CFEM_TRY(tmp_alloc(&d_jobs, pad_jobs.size(), s));
+        CFEM_CUDA(cudaMemcpyAsync(d_jobs, pad_jobs.data(), pad_jobs.size() * sizeof(PadJob),
+                                  cudaMemcpyHostToDevice, s));
+        const unsigned g = std::min(grid_for(pad_rows * 8, 256), (unsigned)P->ctx->num_sms * 16);
+        CFEM_LAUNCH(k_pad4_batch, g, 256, 0, s, (const PadJob *)d_jobs, (int)pad_jobs.size(),
+                    pad_rows);
+        tmp_free(d_jobs, s);
     }
     return CFEM_OK;
 }

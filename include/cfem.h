@@ -414,6 +414,19 @@ CFEM_API int cfem_mixed_matrix(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
                                const int32_t *d_row_ptr, const int32_t *d_col,
                                const double *d_vals64, float *d_vals32,
                                void *stream);
+/* cfem_mixed_matrix for many systems in one launch per block size (a
+ * batch of meshes: one launch instead of one per system). */
+typedef struct cfem_mixed_job {
+    int64_t n_rows;
+    int32_t bs;                 /* 1 or 3 */
+    int32_t reserved;
+    const int32_t *d_row_ptr;
+    const int32_t *d_col;
+    const double *d_vals64;
+    float *d_vals32;
+} cfem_mixed_job;
+CFEM_API int cfem_mixed_matrix_batch(cfem_ctx *ctx, const cfem_mixed_job *jobs,
+                                     int32_t n_jobs, void *stream);
 
 /* ---- solver -------------------------------------------------------------
  * Jacobi-preconditioned CG on a batch of independent systems. Batches whose

@@ -133,3 +133,36 @@ def test_autotuned_batch_gives_identical_results(tmp_path, monkeypatch):
                      (N.PARAM_GRAPH_ITERS, 2)):
             rt.set_param(p, v)
         N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
+
+
+def test_mixed_matrix_batch_equals_per_system(torch):
+    """cfem_mixed_matrix_batch (one launch per block size over many systems)
+    writes bitwise the FP32 operators that cfem_mixed_matrix writes one
+    system at a time, for scalar and 3x3 systems in one call."""
+    from cloudfem_b200 import _native as N
+    from cloudfem_b200.device import DeviceMesh, ptr
+    from cloudfem_b200.mesh import box_mesh, box_mesh_tet10
+    rt = N.runtime()
+    systems = []
+    for m, op, bs in ((box_mesh(5, 4, 3), N.OP_P1_STIFF, 1),
+                      (box_mesh_tet10(3, 2, 2), N.OP_T10_STIFF, 1),
+                      (box_mesh(4, 3, 3), N.OP_P1_ELAST, 3)):
+        dm = DeviceMesh(m)
+        if bs == 1:
+            vals, _ = dm.assemble(op, coef=lambda x, y, z: 1.0 + x * y)
+        else:
+            vals, _ = dm.assemble_elastic(op, 210e9, 0.3)
+        systems.append((dm, vals, bs))
+    jobs = (N.MixedJob * len(systems))()
+    outs = []
+    for i, (dm, vals, bs) in enumerate(systems):
+        v32 = torch.full((vals.numel(),), float("nan"), dtype=torch.float32, device="cuda")
+        outs.append(v32)
+        jobs[i] = N.MixedJob(dm.n_nodes, bs, 0, dm.pattern.row_ptr, dm.pattern.col, ptr(vals),
+                             ptr(v32))
+    N.check(rt.lib.cfem_mixed_matrix_batch(rt.ctx, jobs, len(systems), rt.stream()))
+    for (dm, vals, bs), got in zip(systems, outs):
+        ref = torch.empty_like(got)
+        N.check(rt.lib.cfem_mixed_matrix(rt.ctx, dm.n_nodes, bs, dm.pattern.row_ptr,
+                                         dm.pattern.col, ptr(vals), ptr(ref), rt.stream()))
+        assert torch.equal(got, ref)
