@@ -1382,6 +1382,27 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         : "memory");
 }
 
+// The same bulk copy with an L2 evict-first policy: the matrix stream of an
+// SpMV passes through L2 once, so it should not push out the vectors the
+// gathers reread (p of a large batch is tens of MB).
+#ifndef CFEM_L2_EVICT_FIRST
+#define CFEM_L2_EVICT_FIRST 1
+#endif
+__device__ __forceinline__ void bulk_load_stream(void *dst, const void *src, uint32_t bytes,
+                                                 unsigned long long *m) {
+#if CFEM_L2_EVICT_FIRST
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(m)), "l"(pol)
+        : "memory");
+#else
+    bulk_load(dst, src, bytes, m);
+#endif
+}
+
 // First unit of global row i whose entries start at kb (unit-padded copy).
 __device__ __forceinline__ int64_t unit_start(int64_t kb, int64_t i) { return (kb + 3 * i + 3) >> 2; }
 
@@ -1428,8 +1449,8 @@ __device__ __forceinline__ StageWin stage_open(StageWarp<TV, W, NB> &sm, const i
         mbar_expect(&sm.mbar[w.buf], bc + bv);
         if (nu) {
             const int64_t u = e0 + w.ub;
-            bulk_load(&sm.c[w.buf][0], ci4 + 4 * u, bc, &sm.mbar[w.buf]);
-            bulk_load(&sm.v[w.buf][0], va4 + 4 * u, bv, &sm.mbar[w.buf]);
+            bulk_load_stream(&sm.c[w.buf][0], ci4 + 4 * u, bc, &sm.mbar[w.buf]);
+            bulk_load_stream(&sm.v[w.buf][0], va4 + 4 * u, bv, &sm.mbar[w.buf]);
         }
     }
     return w;
@@ -1674,8 +1695,8 @@ __device__ __forceinline__ void stage3_issue(Stage3Warp<TV, W> &sm, const int32_
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect(&sm.mbar[b], bc + bv);
     if (nu) {
-        bulk_load(&sm.c[b][0], c3 + 4 * u0, bc, &sm.mbar[b]);
-        bulk_load(&sm.v[b][0], v3 + 36 * u0, bv, &sm.mbar[b]);
+        bulk_load_stream(&sm.c[b][0], c3 + 4 * u0, bc, &sm.mbar[b]);
+        bulk_load_stream(&sm.v[b][0], v3 + 36 * u0, bv, &sm.mbar[b]);
     }
 }
 

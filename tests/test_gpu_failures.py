@@ -78,3 +78,5 @@ def test_grid_barrier_timeout_then_recovery(torch):
         rt.set_param(N.PARAM_BARRIER_HOLD, 2)
     with pytest.raises(ValueError):
         rt.set_param(N.PARAM_BARRIER_TIMEOUT_US, 0)
+    with pytest.raises(ValueError):
+        rt.set_param(N.PARAM_SELL3_LANES, 8)   # slices must hold a chunk's rows

@@ -52,3 +52,5 @@ def test_struct_layouts_match_header():
     # cfem_linsys: 8+4+4 + 7 ptrs + 8 + 4 + 4
     assert ctypes.sizeof(_native.LinSys) == 16 + 7 * 8 + 16 + 8 + 8 + 8
     assert ctypes.sizeof(_native.SolveStats) == 56
+    # cfem_mixed_job: int64, int32, int32, 4 pointers
+    assert ctypes.sizeof(_native.MixedJob) == 8 + 4 + 4 + 4 * 8
