@@ -55,6 +55,7 @@ L2_FLUSH_BYTES = 256 << 20
 SPMV_STAGE = None   # --spmv-stage: None keeps the library default
 SELL_SORT = None    # --sell-sort: None keeps the library default
 SELL3_LANES = None  # --sell3-lanes: None keeps the library default
+SELL3_STAGED = None  # --sell3-staged: None keeps the library default
 
 
 def _set_scheduler(rt, name):
@@ -71,15 +72,22 @@ def _set_scheduler(rt, name):
         rt.set_param(N.PARAM_SELL_SORT, SELL_SORT)
     if SELL3_LANES is not None:
         rt.set_param(N.PARAM_SELL3_LANES, SELL3_LANES)
+    if SELL3_STAGED is not None:
+        rt.set_param(N.PARAM_SELL3_STAGED, SELL3_STAGED)
 
 
-def _block_spmv_kernel(rt):
+def _block_spmv_kernel(rt, precision):
     """(name, profile summary) of the 3x3 SpMV-phase kernel the context's
     staging selects."""
     from cloudfem_b200 import _native as N
     stage = rt.get_param(N.PARAM_SPMV_STAGE)
     if stage in (3, 4):
         lanes = rt.get_param(N.PARAM_SELL3_LANES)
+        staged = rt.get_param(N.PARAM_SELL3_STAGED)
+        if staged == 1 or (staged == 2 and precision == "mixed"):
+            return (f"k_gxl3s (PCG SpMV phase, sliced ELL, {lanes} lanes per block row, "
+                    "slices bulk-copied through shared memory)",
+                    "k_gxl3_tet10_elasticity_80x10x10")
         return (f"k_gxl3 (PCG SpMV phase, sliced ELL, {lanes} lanes per block row: "
                 "q = A p, p update, p.q)", "k_gxl3_tet10_elasticity_80x10x10")
     if stage == 2:
@@ -345,7 +353,7 @@ def run_ours(args, rank, world, local_rank):
         achieved = bytes_spmv / (spmv_ms * 1e-3) / 1e9
     else:
         achieved = bytes_solve / (last.kernel_ms * 1e-3) / 1e9
-    kname, kprof = _block_spmv_kernel(rt)
+    kname, kprof = _block_spmv_kernel(rt, args.precision)
     traffic = (_profiled_traffic(kprof, "fp32" if args.precision == "mixed" else "fp64")
                if kprof else None)
     h2d = mesh.nodes.size * 8 + mesh.elements.size * 4
@@ -1244,11 +1252,16 @@ def main():
     ap.add_argument("--sell3-lanes", type=int, default=None, choices=[1, 2, 4],
                     help="sliced-ELL SpMV of 3x3 blocks: lanes per block row (default: "
                          "the library's)")
+    ap.add_argument("--sell3-staged", type=int, default=None, choices=[0, 1, 2],
+                    help="sliced-ELL SpMV of 3x3 blocks: 1 streams slices through shared "
+                         "memory with bulk copies, 0 loads them into registers, 2 streams "
+                         "FP32 slices only (default: the library's)")
     args = ap.parse_args()
-    global SPMV_STAGE, SELL_SORT, SELL3_LANES
+    global SPMV_STAGE, SELL_SORT, SELL3_LANES, SELL3_STAGED
     SPMV_STAGE = args.spmv_stage
     SELL_SORT = args.sell_sort
     SELL3_LANES = args.sell3_lanes
+    SELL3_STAGED = args.sell3_staged
     if args.precision is None:
         args.precision = "fp64" if args.workload in ("elasticity", "av-transient") else "mixed"
     world = int(os.environ.get("WORLD_SIZE", "1"))

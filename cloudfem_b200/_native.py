@@ -35,6 +35,7 @@ SCHED_AUTO, SCHED_PERSISTENT, SCHED_GRAPH, SCHED_GRAPH_POLLED = 0, 1, 2, 3
 PARAM_T10_WARPS, PARAM_P1_THREADS, PARAM_GRAPH_ITERS, PARAM_PDL, PARAM_SPMV_STAGE = 1, 2, 3, 4, 5
 PARAM_BARRIER_TIMEOUT_US, PARAM_BARRIER_HOLD, PARAM_SELL_SORT = 6, 7, 8
 PARAM_SELL3_LANES = 9
+PARAM_SELL3_STAGED = 10
 
 STATUS_NAMES = {
     CFEM_OK: "ok", CFEM_ERR_INVALID: "invalid argument",

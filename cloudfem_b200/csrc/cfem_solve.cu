@@ -2666,6 +2666,209 @@ k_gxl3(const SysDev *__restrict__ sys, SysState *st, const GridBar *bar,
     group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
 }
 
+// k_gxl3 with the slice streamed through shared memory: a slice's step (a
+// column plane and 9 value planes of 32 lanes) is contiguous in the
+// sliced-ELL copy, so one lane issues two 1-D bulk copies per step into a
+// ring of NS3 stages completing on transaction mbarriers, NS3 steps ahead
+// of their use. The first NS3 steps are issued before the wait for the
+// predecessor kernel (skipped when the system has already finished), so
+// they travel while the previous kernel drains. Every issued copy is
+// waited for before the warp leaves, also on the R / ZERO and early-exit
+// paths; every wait is bounded (2 s) and a warp that gives up records the
+// error and drains its other copies (bounded).
+constexpr int NS3 = 3;
+template <typename T> struct __align__(16) Sell3Ring {
+    T val[NS3][9 * 32];
+    int32_t col[NS3][32];
+    unsigned long long mbar[NS3];
+};
+template <typename T>
+constexpr size_t gxl3s_smem() { return (size_t)GROUP * sizeof(Sell3Ring<T>); }
+
+template <typename T>
+__device__ __forceinline__ void sell3_issue(Sell3Ring<T> &rg, const T *vb, const int32_t *cb,
+                                            int t) {
+    const int b = t % NS3;
+    const uint32_t bv = 9 * 32 * (uint32_t)sizeof(T), bc = 32 * 4;
+    mbar_expect(&rg.mbar[b], bv + bc);
+    bulk_load_stream(&rg.val[b][0], vb + (int64_t)9 * 32 * t, bv, &rg.mbar[b]);
+    bulk_load_stream(&rg.col[b][0], cb + (int64_t)32 * t, bc, &rg.mbar[b]);
+}
+
+// Waits (bounded) for the issued steps [from, to) that were not consumed.
+template <typename T>
+__device__ __forceinline__ void sell3_drain(Sell3Ring<T> &rg, int from, int to) {
+    for (int t = from; t < to; ++t) {
+        const unsigned long long t0 = globaltimer();
+        while (!mbar_test(&rg.mbar[t % NS3], (uint32_t)(t / NS3) & 1u) &&
+               globaltimer() - t0 < 2000000000ull) {
+        }
+    }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(32 * GROUP, 3)
+k_gxl3s(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
+        const int2 *__restrict__ list, int n) {
+    extern __shared__ __align__(16) unsigned char ring_area[];
+    constexpr int RS = 32 / L, NSL = SELL_ROWS / RS;
+    constexpr bool DIFF = sizeof(T) == 4;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * GROUP + w;
+    const int2 e = wid < n ? __ldg(list + wid) : make_int2(-1, -1);
+    const int2 lead = __ldg(list + blockIdx.x * GROUP);   // a real entry (lists pad per system)
+    const SysDev &S = sys[lead.x];
+    Sell3Ring<T> &rg = reinterpret_cast<Sell3Ring<T> *>(ring_area)[w];
+    // the slice's place: fixed for the whole solve
+    const bool mine = e.x >= 0 && (int64_t)e.y * S.xrows < S.n;
+    bool live = false, valid = false;
+    int wst = 0;
+    int64_t row = 0;
+    const T *vb = nullptr;
+    const int32_t *cb = nullptr;
+    if (mine) {
+        const int64_t sl = e.y;
+        const int64_t r0 = (sl / NSL) * SELL_ROWS;
+        const int sidx = (int)(sl % NSL);
+        const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+        live = sidx * RS < nr;
+        if (live) {
+            const int64_t base = __ldg(S.soff + sl);
+            wst = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+            const int rl = __ldg(S.sperm + r0 + sidx * RS + lane / L);
+            valid = rl < nr;
+            row = valid ? r0 + rl : r0;
+            vb = (const T *)S.sval + 9 * base;
+            cb = S.scol + base;
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int b = 0; b < NS3; ++b) mbar_init(&rg.mbar[b]);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    // a finished system stays finished: no prefetch for it
+    const bool done0 = *(volatile const int32_t *)&st[lead.x].phase == PH_DONE;
+    int issued = 0;
+    if (live && !done0) {
+        issued = wst < NS3 ? wst : NS3;
+        if (lane == 0)
+            for (int t = 0; t < issued; ++t) sell3_issue(rg, vb, cb, t);
+    }
+    pdl_wait();
+    const int ph = *(volatile int32_t *)&st[lead.x].phase;
+    const bool go = *(volatile const int *)&bar->active > 0 &&
+                    !*(volatile const int *)&bar->err &&
+                    (ph == PH_A || ph == PH_R || ph == PH_ZERO);   // uniform over the block
+    if (!go) {
+        sell3_drain(rg, 0, issued);
+        return;
+    }
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (mine && ph == PH_A && live && issued < wst && issued < NS3) {
+        // (the prefetch was skipped: the phase changed since) issue now
+        const int k = wst < NS3 ? wst : NS3;
+        if (lane == 0)
+            for (int t = issued; t < k; ++t) sell3_issue(rg, vb, cb, t);
+        issued = k;
+    }
+    if (mine && ph == PH_A && live) {
+        const SysState *sst = &st[e.x];
+        const T beta = (T)vcg(&sst->beta);
+        const T zeta = (T)vcg(&sst->zeta);
+        const int pbuf = vcgi(&sst->pbuf);
+        const T *pin = (const T *)(pbuf ? S.p1 : S.p0);
+        T *pout = (T *)(pbuf ? S.p0 : S.p1);
+        const T *z = (const T *)S.z;
+        T *qv = (T *)S.q;
+        const int u = lane % L;
+        T pi[3], acc[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pi[c] = zeta * __ldg(z + row * 3 + c) + beta * __ldg(pin + row * 3 + c);
+            acc[c] = 0;
+        }
+        int t = 0;
+        for (; t < wst; ++t) {
+            const int b = t % NS3;
+            const bool ok = mbar_wait(&rg.mbar[b], (uint32_t)(t / NS3) & 1u, &bar->err);
+            if (!__all_sync(0xffffffffu, ok)) {
+                sell3_drain(rg, t, issued);   // this step's copy may still be in flight
+                if (lane == 0) atomicExch(&bar->err, 2);
+                break;
+            }
+            const int64_t j = rg.col[b][lane];
+            T a[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) a[q] = rg.val[b][q * 32 + lane];
+            T pj[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pj[d] = zeta * __ldg(z + j * 3 + d) + beta * __ldg(pin + j * 3 + d);
+                if (DIFF) pj[d] = (t == 0 && u == 0) ? pi[d] : pj[d] - pi[d];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[c] += a[c * 3 + d] * pj[d];
+            __syncwarp();   // every lane has read stage b
+            if (issued < wst) {
+                if (lane == 0) {
+                    // the generic reads above before the async-proxy writes
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    sell3_issue(rg, vb, cb, issued);
+                }
+                ++issued;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+        T pq = 0;
+        if (t == wst && valid && u == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int64_t i = row * 3 + c;
+                pout[i] = pi[c];
+                qv[i] = acc[c];
+                pq += pi[c] * acc[c];
+            }
+        }
+        part[0] += (double)pq;
+    } else {
+        sell3_drain(rg, 0, issued);
+        if (mine) {
+            const int64_t r0 = (int64_t)e.y * S.xrows;
+            const int64_t r1 = min(S.n, r0 + S.xrows);
+            if (ph == PH_R) {
+                int bad = 0;
+                run_R<T, 3>(S, &st[e.x], r0, r1, lane, part, &bad);
+            } else if (ph == PH_ZERO) {
+                phase_zero<3>(S, r0, r1, lane);
+            }
+        }
+    }
+    group_store(part, 4, S.partial + (int64_t)(lead.y / GROUP) * 4, lane, w);
+}
+
+template <typename T>
+static void (*gxl3s_kernel(int L))(const SysDev *, SysState *, GridBar *, const int2 *, int) {
+    return L == 1 ? k_gxl3s<T, 1> : L == 2 ? k_gxl3s<T, 2> : k_gxl3s<T, 4>;
+}
+
+template <typename T>
+static int gxl3s_prepare(int L) {
+    const size_t bytes = gxl3s_smem<T>();
+    auto k = gxl3s_kernel<T>(L);
+    CFEM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    int pct = (int)((3 * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+    if (pct > 100) pct = 100;
+    CFEM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    return CFEM_OK;
+}
+
 // The k_gxl3 instance for L lanes per block row (1, 2 or 4: slices of at
 // least chunk_rows(3) block rows, so the work lists stay within their
 // per-chunk allocation).
@@ -2873,6 +3076,8 @@ struct cfem_pcg_plan {
     bool polled = false;
     int giters = 2;               // iterations per body of the solve loop
     int lanes3 = 4;               // sliced ELL of 3x3 systems: lanes per block row
+    int staged3 = 2;              // ... streamed through shared memory (k_gxl3s): 1 both
+                                  // precisions, 2 FP32 only, 0 neither
     // solve slots (cfem_pcg_slots_*): each system of the plan is a slot of
     // fixed capacity whose system is replaced between rounds of iterations
     bool slots = false;
@@ -3076,6 +3281,7 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     P->ctx = ctx;
     P->device = ctx->device;
     P->lanes3 = ctx->sell3_lanes;
+    P->staged3 = ctx->sell3_staged;
     P->n_systems = n_systems;
     CFEM_CUDA(cudaStreamCreateWithFlags(&P->w, cudaStreamNonBlocking));
     CFEM_CUDA(cudaStreamCreateWithFlags(&P->w2, cudaStreamNonBlocking));
@@ -3342,6 +3548,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     if ((tstage[2] == 1 || tstage[2] == 2) && !la[2].empty())
         CFEM_TRY((lpr[2] == 4 ? gxs_prepare<float, 4>() : gxs_prepare<float, 8>()));
     if (tstage[1] == 2 && !la[1].empty()) CFEM_TRY(gxs3_prepare<double>());
+    if (tstage[1] == 3 && P->staged3 == 1 && !la[1].empty()) CFEM_TRY(gxl3s_prepare<double>(P->lanes3));
+    if (tstage[3] == 3 && P->staged3 && !la[3].empty()) CFEM_TRY(gxl3s_prepare<float>(P->lanes3));
     if (tstage[3] == 2 && !la[3].empty()) CFEM_TRY(gxs3_prepare<float>());
     auto iteration = [&](cudaStream_t cs, bool count, cudaEvent_t t0, cudaEvent_t t1) -> int {
         // dependent launches only between kernel nodes (not next to events)
@@ -3373,12 +3581,16 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
             if (t == 0 && stage == 0) glaunch(p, k_gx<double, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage == 2)
                 glaunch_smem(p, k_gxs3<double>, g, 32 * GROUP, gxs3_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 1 && stage == 3) glaunch(p, gxl3_kernel<double>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 3 && P->staged3 == 1)
+                glaunch_smem(p, gxl3s_kernel<double>(P->lanes3), g, 32 * GROUP, gxl3s_smem<double>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 1 && stage == 3 && P->staged3 != 1) glaunch(p, gxl3_kernel<double>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 1 && stage < 2) glaunch(p, k_gx<double, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 2 && stage == 0) glaunch(p, k_gx<float, 1>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage == 2)
                 glaunch_smem(p, k_gxs3<float>, g, 32 * GROUP, gxs3_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
-            if (t == 3 && stage == 3) glaunch(p, gxl3_kernel<float>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 3 && P->staged3)
+                glaunch_smem(p, gxl3s_kernel<float>(P->lanes3), g, 32 * GROUP, gxl3s_smem<float>(), cs, (const SysDev *)d_sys, d_st, d_bar, (const int2 *)pa[t], n);
+            if (t == 3 && stage == 3 && P->staged3 == 0) glaunch(p, gxl3_kernel<float>(P->lanes3), g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (t == 3 && stage < 2) glaunch(p, k_gx<float, 3>, g, 32 * GROUP, cs, (const SysDev *)d_sys, d_st, (const GridBar *)d_bar, (const int2 *)pa[t], n);
             if (count) ++per_iter;
         }

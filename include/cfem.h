@@ -196,10 +196,16 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * rows in a slice: gathers of p that share cache lines). SELL3_LANES
  * (SpMV staging 3, 3x3 blocks): lanes that share one block row, each over
  * every L-th block of it (1, 2 or 4 (default); a slice holds 32 / L block
- * rows). get returns -1 for an unknown parameter. */
+ * rows). SELL3_STAGED: 1 streams each slice's steps through a ring of
+ * three shared-memory stages filled by 1-D bulk copies (the first issued
+ * before the kernel waits for its predecessor), 0 loads them into
+ * registers, 2 (default) streams FP32 slices and loads FP64 ones (the
+ * faster of the two measured for each). get returns -1 for an unknown
+ * parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5, CFEM_PARAM_BARRIER_TIMEOUT_US = 6,
-       CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8, CFEM_PARAM_SELL3_LANES = 9 };
+       CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8, CFEM_PARAM_SELL3_LANES = 9,
+       CFEM_PARAM_SELL3_STAGED = 10 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */

@@ -84,16 +84,18 @@ def _system(torch, rt, A, b, offset):
     return s
 
 
-def _solve(rt, systems, mode, rtol, stage, sort=1, lanes=4):
+def _solve(rt, systems, mode, rtol, stage, sort=1, lanes=4, staged=0):
     from cloudfem_b200 import _native as N
     from cloudfem_b200.device import pcg
     N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_GRAPH))
     before = rt.get_param(N.PARAM_SPMV_STAGE)
     lanes_before = rt.get_param(N.PARAM_SELL3_LANES)
+    staged_before = rt.get_param(N.PARAM_SELL3_STAGED)
     try:
         rt.set_param(N.PARAM_SPMV_STAGE, stage)
         rt.set_param(N.PARAM_SELL_SORT, sort)
         rt.set_param(N.PARAM_SELL3_LANES, lanes)
+        rt.set_param(N.PARAM_SELL3_STAGED, staged)
         for s in systems:
             s.x.zero_()
         res = pcg(systems, mode, rtol, 20000)
@@ -101,6 +103,7 @@ def _solve(rt, systems, mode, rtol, stage, sort=1, lanes=4):
         rt.set_param(N.PARAM_SPMV_STAGE, before)
         rt.set_param(N.PARAM_SELL_SORT, 1)
         rt.set_param(N.PARAM_SELL3_LANES, lanes_before)
+        rt.set_param(N.PARAM_SELL3_STAGED, staged_before)
         N.check(rt.lib.cfem_ctx_set_scheduler(rt.ctx, N.SCHED_AUTO))
     for r in res:
         assert r.status == N.CFEM_OK, r
@@ -180,29 +183,33 @@ def _elastic_system(torch, nx, ny, nz, seed):
                            vals, rhs, x, mask)
 
 
-@pytest.mark.parametrize("stage,lanes", [(2, 4), (3, 1), (3, 2), (3, 4)])
+@pytest.mark.parametrize("stage,lanes,staged", [(2, 4, 0), (3, 1, 0), (3, 2, 0), (3, 4, 0),
+                                                (3, 4, 1), (3, 2, 1)])
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
-def test_staged_3x3_spmv_matches_register_path(torch, mode, stage, lanes):
+def test_staged_3x3_spmv_matches_register_path(torch, mode, stage, lanes, staged):
     """3x3-block systems on the graph scheduler: the staged SpMV (staging
     2: rows that straddle windows, 65-block vertex rows) or the sliced-ELL
     one (staging 3: slices of 32 / lanes block rows, `lanes` lanes per block
     row) and the register path reach the same answer, and the other path
-    repeats bitwise."""
+    repeats bitwise; staged = 1 streams the slices through shared memory."""
     from cloudfem_b200 import _native as N
     dm, sysm = _elastic_system(torch, 10, 3, 3, seed=1)
     rt = dm.rt
     md = N.SOLVE_FP64 if mode == "fp64" else N.SOLVE_MIXED
     rtol = 1e-11 if mode == "fp64" else 1e-10
     _, (x0,) = _solve(rt, [sysm], md, rtol, 0)
-    r1, (x1,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes)
-    _, (x1b,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes)
+    r1, (x1,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes, staged=staged)
+    _, (x1b,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes, staged=staged)
+    if stage == 3 and staged:   # the same arithmetic as the register variant
+        _, (x1r,) = _solve(rt, [sysm], md, rtol, stage, lanes=lanes)
+        assert np.array_equal(x1, x1r)
     d = np.linalg.norm(x1 - x0) / np.linalg.norm(x0)
     assert d <= (1e-8 if mode == "fp64" else 1e-7), d
     assert np.array_equal(x1, x1b)
 
 
-@pytest.mark.parametrize("stage,lanes", [(2, 4), (3, 2), (3, 4)])
-def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage, lanes):
+@pytest.mark.parametrize("stage,lanes,staged", [(2, 4, 0), (3, 2, 0), (3, 4, 0), (3, 4, 1)])
+def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage, lanes, staged):
     """Each 3x3 system's answer is bitwise the same alone and in a batch
     with the staged or sliced-ELL SpMV, in both precisions."""
     from cloudfem_b200 import _native as N
@@ -210,8 +217,8 @@ def test_staged_3x3_spmv_batch_equals_solo_bitwise(torch, stage, lanes):
     rt = built[0][0].rt
     systems = [s for _, s in built]
     for md in (N.SOLVE_FP64, N.SOLVE_MIXED):
-        rb, xb = _solve(rt, systems, md, 1e-10, stage, lanes=lanes)
+        rb, xb = _solve(rt, systems, md, 1e-10, stage, lanes=lanes, staged=staged)
         for i, s in enumerate(systems):
-            r, (x,) = _solve(rt, [s], md, 1e-10, stage, lanes=lanes)
+            r, (x,) = _solve(rt, [s], md, 1e-10, stage, lanes=lanes, staged=staged)
             assert r[0].iterations == rb[i].iterations
             assert np.array_equal(x, xb[i]), (md, i)
