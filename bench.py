@@ -479,6 +479,15 @@ def run_batched_heat(args, rank, world, local_rank):
     solver = BatchSolver(local_rank)
     batch = solver.prepare(problems)
     free = batch.free_dofs
+    if args.one_pass:
+        # one assembly and one mixed solve, nothing else: the launch
+        # sequence a per-launch profiler should see (no timing, no line)
+        batch.assemble()
+        res = batch.solve("mixed", rtol=1e-8)
+        torch.cuda.synchronize()
+        print(f"one pass: {len(res)} systems, {free} free DOFs, "
+              f"{max(r.iterations for r in res)} iterations at most", file=sys.stderr)
+        return None
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     # the configuration's tolerance: CG with FP64 refinement to 1e-8 relative
     # residual (the answer then agrees with FP64 to about 6e-9, within the
@@ -1215,6 +1224,9 @@ def main():
                     help="default: fp64 for the elasticity beam and the A-V transient, "
                          "mixed otherwise")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--one-pass", action="store_true",
+                    help="batched-heat: one assembly and one mixed solve of the batch and "
+                         "exit without a line (for per-launch profilers)")
     ap.add_argument("--workload", default="batched-heat",
                     choices=["elasticity", "batched-heat", "transient-heat", "serving",
                              "av-phasor", "av-transient"],
