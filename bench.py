@@ -808,7 +808,11 @@ def run_transient_heat(args, rank, world, local_rank):
             "kernel": _scalar_spmv_kernel(rt, args.precision) + " (scalar PCG SpMV phase: q = A p, p.q)",
             "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": ach / peak, "bytes_per_launch": int(spmv_b),
-            "launch_ms": float(np.mean(spmv)), "traffic": None,
+            "launch_ms": float(np.mean(spmv)),
+            # DRAM bytes per launch from the committed ncu summary (FP32 staged
+            # kernel, captured at 112^3 and scaled by nonzeros)
+            "traffic": (_profiled_traffic("k_gxs_transient_p1_heat_128cubed", "fp32")
+                        if args.precision == "mixed" else None),
         }
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_transient_heat()
