@@ -339,14 +339,24 @@ __device__ __forceinline__ void t10_scalar_elem(const double *__restrict__ nodes
         double wk[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) wk[q] = c_wq[q] * coef_at(coef, e, q);
-        for (int t = lane; t < 100; t += 32) {
-            int a = t / 10, b = t - (t / 10) * 10;
+        // the 55 pairs a <= b, each written to (a, b) and (b, a): the dot
+        // products are symmetric in floating point, so the matrix is the
+        // same as entry by entry with half the shared-memory reads
+        for (int t = lane; t < 55; t += 32) {
+            // pair t in row-major order of the upper triangle
+            int a = 0, r = t;
+            while (r >= 10 - a) {
+                r -= 10 - a;
+                ++a;
+            }
+            const int b = a + r;
             double s = 0.0;
 #pragma unroll
             for (int q = 0; q < 5; ++q)
                 s += wk[q] * (sG[q][a][0] * sG[q][b][0] + sG[q][a][1] * sG[q][b][1] +
                               sG[q][a][2] * sG[q][b][2]);
-            ke[t] = vol * s;
+            ke[a * 10 + b] = vol * s;
+            ke[b * 10 + a] = vol * s;
         }
         if (fe && lane < 10) {
             double s = 0.0;

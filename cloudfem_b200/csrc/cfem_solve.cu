@@ -477,7 +477,10 @@ __device__ __forceinline__ double dd_residual(double b, double hi, double lo) {
     return __dsub_rn(__dsub_rn(b, hi), lo);
 }
 
-template <bool INIT, int BS>
+// NC: x is read-only for the whole launch (the per-phase kernels of the
+// graph scheduler), so its gathers may go through L1; the persistent kernel,
+// which also writes x, reads it through L2 (ldcg).
+template <bool INIT, int BS, bool NC = false>
 __device__ __forceinline__ void acc_R(const double *__restrict__ v,
                                       const int32_t *__restrict__ ci, int32_t k,
                                       int64_t row, const double *x,
@@ -490,7 +493,7 @@ __device__ __forceinline__ void acc_R(const double *__restrict__ v,
     bool fj[BS];
 #pragma unroll
     for (int d = 0; d < BS; ++d) {
-        xj[d] = ldcg(x + j * BS + d);
+        xj[d] = NC ? __ldg(x + j * BS + d) : ldcg(x + j * BS + d);
         fj[d] = INIT && fixed ? (__ldg(fixed + j * BS + d) != 0) : false;
     }
 #pragma unroll
@@ -506,7 +509,7 @@ __device__ __forceinline__ void acc_R(const double *__restrict__ v,
         }
 }
 
-template <typename T, int BS, bool INIT>
+template <typename T, int BS, bool INIT, bool NC = false>
 __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
                         int64_t r1, int lane, double part[4], int *bad) {
     const int sub = lane & (LANES - 1), grp = lane / LANES;
@@ -527,7 +530,7 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
         if (valid) {
             const int32_t k1 = __ldg(S.rp + row + 1);
             for (int32_t k = __ldg(S.rp + row) + sub; k < k1; k += LANES)
-                acc_R<INIT, BS>(S.v64, S.ci, k, row, S.x, S.fixed, acc, alo, aab, accf, dg);
+                acc_R<INIT, BS, NC>(S.v64, S.ci, k, row, S.x, S.fixed, acc, alo, aab, accf, dg);
         }
 #pragma unroll
         for (int c = 0; c < BS; ++c) {
@@ -608,7 +611,7 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
 // sums and epilogue as phase_R<T, 1, INIT>: each lane of a group of 8 reads
 // whole units of four entries; padding entries (column = own row, value 0)
 // add nothing and are told apart from the real diagonal by position.
-template <typename T, bool INIT>
+template <typename T, bool INIT, bool NC = false>
 __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
                              int64_t r1, int lane, double part[4], int *bad) {
     constexpr int H = 2;
@@ -655,7 +658,7 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
                     bool fj[4];
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
-                        xj[e] = ldcg(S.x + c[e]);
+                        xj[e] = NC ? __ldg(S.x + c[e]) : ldcg(S.x + c[e]);
                         fj[e] = INIT && S.fixed ? (__ldg(S.fixed + c[e]) != 0) : false;
                     }
                     const int64_t pos = (u[h] - u0[h]) * 4;
@@ -725,9 +728,9 @@ template <typename T, int BS>
 __device__ __forceinline__ void run_R(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
                                    int lane, double part[4], int *bad) {
     if (BS == 1 && S.vec4)
-        phase_R_vec1<T, false>(S, st, r0, r1, lane, part, bad);
+        phase_R_vec1<T, false, true>(S, st, r0, r1, lane, part, bad);
     else
-        phase_R<T, BS, false>(S, st, r0, r1, lane, part, bad);
+        phase_R<T, BS, false, true>(S, st, r0, r1, lane, part, bad);
 }
 
 // State transition of a system once all its chunk sums are in.
@@ -2567,7 +2570,7 @@ __device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st
     double hi = 0.0, lo = 0.0, aab = 0.0;
     for (int k = 0; k < w; ++k) {
         const double a = ld_stream(vp + 32 * k);
-        const double xj = ldcg(S.x + ld_stream(cp + 32 * k));
+        const double xj = __ldg(S.x + ld_stream(cp + 32 * k));   // read-only in this launch
         dd_fma(hi, lo, a, xj);
         aab += fabs(a * xj);
     }
