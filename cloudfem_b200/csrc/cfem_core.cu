@@ -74,29 +74,43 @@ __global__ void k_to_fp32(int64_t n, const double *__restrict__ in,
 }
 
 // y = alpha A x + beta y, one thread per block row (setup-time use only).
+// y = alpha A x + beta y over a (block) CSR: SL = 8 lanes per (block) row,
+// lane s taking entries s, s + 8, ... (coalesced along the row), the lanes'
+// sums meeting in a fixed shuffle tree.
+constexpr int SL = 8;
 template <int BS>
 __global__ void k_spmv(int64_t n, const int32_t *__restrict__ rp,
                        const int32_t *__restrict__ ci,
                        const double *__restrict__ v, double alpha,
                        const double *__restrict__ x, double beta,
                        double *__restrict__ y) {
-    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r >= n) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t r = t / SL;
+    const int sub = (int)(t % SL);
     double acc[BS];
 #pragma unroll
     for (int c = 0; c < BS; ++c) acc[c] = 0.0;
-    for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
-        int64_t j = ci[k];
+    if (r < n) {
+        for (int32_t k = rp[r] + sub; k < rp[r + 1]; k += SL) {
+            const int64_t j = ci[k];
 #pragma unroll
-        for (int c = 0; c < BS; ++c)
+            for (int c = 0; c < BS; ++c)
 #pragma unroll
-            for (int d = 0; d < BS; ++d)
-                acc[c] += v[(int64_t)k * BS * BS + c * BS + d] * x[j * BS + d];
+                for (int d = 0; d < BS; ++d)
+                    acc[c] += v[(int64_t)k * BS * BS + c * BS + d] * x[j * BS + d];
+        }
     }
 #pragma unroll
-    for (int c = 0; c < BS; ++c) {
-        double yv = beta == 0.0 ? 0.0 : beta * y[r * BS + c];
-        y[r * BS + c] = alpha * acc[c] + yv;
+    for (int o = SL / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < BS; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if (r < n && sub < BS) {
+#pragma unroll
+        for (int c = 0; c < BS; ++c)
+            if (c == sub) {
+                const double yv = beta == 0.0 ? 0.0 : beta * y[r * BS + c];
+                y[r * BS + c] = alpha * acc[c] + yv;
+            }
     }
 }
 
@@ -327,7 +341,7 @@ int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
     if (n_rows == 0) return CFEM_OK;
     CFEM_TRY(set_device(ctx->device));
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned g = grid_for(n_rows, 128);
+    unsigned g = grid_for(n_rows * SL, 128);
     if (bs == 1)
         CFEM_LAUNCH(k_spmv<1>, g, 128, 0, s, n_rows, d_row_ptr, d_col, d_vals,
                     alpha, d_x, beta, d_y);

@@ -106,6 +106,8 @@ struct SysDev {
     const int64_t *soff;
     const uint8_t *sperm;
     int32_t sell;
+    int32_t lpr;          // bs 1, unit-padded residual phase: lanes per row (4 or 8;
+                          // 0 means 8)
 };
 
 struct SysState {
@@ -611,11 +613,11 @@ __device__ void phase_R(const SysDev &S, const SysState *st, int64_t r0,
 // sums and epilogue as phase_R<T, 1, INIT>: each lane of a group of 8 reads
 // whole units of four entries; padding entries (column = own row, value 0)
 // add nothing and are told apart from the real diagonal by position.
-template <typename T, bool INIT, bool NC = false>
+template <typename T, bool INIT, bool NC = false, int LPR = 8>
 __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
                              int64_t r1, int lane, double part[4], int *bad) {
-    constexpr int H = 2;
-    const int sub = lane & 7, grp = lane >> 3;
+    constexpr int H = 2, NG = 32 / LPR;
+    const int sub = lane % LPR, grp = lane / LPR;
     T *r = (T *)S.r;
     T *z = (T *)S.z;
     T *dinv = (T *)S.dinv;
@@ -624,13 +626,13 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
     const double *va = S.va4d;
     double rr = 0.0, bb = 0.0, aa = 0.0;
     T rz = 0, rp = 0;
-    for (int64_t base = r0; base < r1; base += 4 * H) {
+    for (int64_t base = r0; base < r1; base += NG * H) {
         int64_t row[H], u[H], u0[H], uend[H], len[H];
         bool valid[H];
         double acc[H], alo[H], aab[H], accf[H], dg[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
-            row[h] = base + grp + 4 * h;
+            row[h] = base + grp + NG * h;
             valid[h] = row[h] < r1;
             const int64_t rr_ = valid[h] ? row[h] : r0;
             const int64_t kb = valid[h] ? __ldg(S.rp + rr_) : 0;
@@ -671,16 +673,16 @@ __device__ void phase_R_vec1(const SysDev &S, const SysState *st, int64_t r0,
                         if (INIT && c[e] == row[h] && pos + e < len[h]) dg[h] = a[e];
                     }
                 }
-                u[h] += 8;
+                u[h] += LPR;
             }
         }
 #pragma unroll
         for (int h = 0; h < H; ++h) {
-            group_sum_dd<8>(acc[h], alo[h]);
-            aab[h] = group_sum<8>(aab[h]);
+            group_sum_dd<LPR>(acc[h], alo[h]);
+            aab[h] = group_sum<LPR>(aab[h]);
             if (INIT) {
-                accf[h] = group_sum<8>(accf[h]);
-                dg[h] = group_sum<8>(dg[h]);
+                accf[h] = group_sum<LPR>(accf[h]);
+                dg[h] = group_sum<LPR>(dg[h]);
             }
             if (valid[h] && sub == 0) {
                 const int64_t i = row[h];
@@ -728,7 +730,8 @@ template <typename T, int BS>
 __device__ __forceinline__ void run_R(const SysDev &S, const SysState *st, int64_t r0, int64_t r1,
                                    int lane, double part[4], int *bad) {
     if (BS == 1 && S.vec4)
-        phase_R_vec1<T, false, true>(S, st, r0, r1, lane, part, bad);
+        S.lpr == 4 ? phase_R_vec1<T, false, true, 4>(S, st, r0, r1, lane, part, bad)
+                   : phase_R_vec1<T, false, true, 8>(S, st, r0, r1, lane, part, bad);
     else
         phase_R<T, BS, false, true>(S, st, r0, r1, lane, part, bad);
 }
@@ -902,8 +905,10 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
     int bad = 0;
     if (RUN == RUN_INIT) {
         int flag = 0;
+        // (x is not written while the residual is initialised: L1 gathers)
         if (BS == 1 && S.vec4)
-            phase_R_vec1<T, true>(S, st, r0, r1, lane, part, &flag);
+            S.lpr == 4 ? phase_R_vec1<T, true, true, 4>(S, st, r0, r1, lane, part, &flag)
+                       : phase_R_vec1<T, true, true, 8>(S, st, r0, r1, lane, part, &flag);
         else
             phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
         bad = __any_sync(0xffffffffu, flag != 0);
@@ -3460,6 +3465,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                                                      : (const void *)S.va4d;
                 S.vec4 = 1;
                 S.sell = sell ? 1 : 0;
+                // short rows (P1: up to 16 entries, 4 units) on 4 lanes each
+                S.lpr = S.nnzb <= 16 * S.n ? 4 : 8;
             }
         }
         // Scalar rows from the padded copy: eight chunks per SpMV work entry,
@@ -3995,6 +4002,7 @@ extern "C" int cfem_pcg_slots_assign(cfem_pcg_plan *P, int32_t slot, const cfem_
     SysDev S = T;   // the slot's workspace, lists and copies
     S.n = L->n_rows;
     S.nnzb = nnzb;
+    if (S.vec4) S.lpr = S.nnzb <= 16 * S.n ? 4 : 8;
     S.nchunks = (int32_t)((S.n + S.crows - 1) / S.crows);
     S.ntiles = (S.nchunks + TILE - 1) / TILE;
     S.nchunksB = (int32_t)((S.n + brows(S.bs) - 1) / brows(S.bs));
