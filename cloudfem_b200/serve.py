@@ -78,19 +78,25 @@ class Request:
         return self.bs * self.mesh.n_nodes
 
     def nnz_estimate(self):
-        npe = np.asarray(self.mesh.elements).shape[1]
-        per_row = 27 if npe == 10 else 15
-        return self.dofs * per_row * self.bs
+        # the estimates depend on the mesh and kind only: computed once (the
+        # serving loop asks for them at every admission point)
+        if getattr(self, "_nnz_est", None) is None:
+            npe = np.asarray(self.mesh.elements).shape[1]
+            per_row = 27 if npe == 10 else 15
+            self._nnz_est = self.dofs * per_row * self.bs
+        return self._nnz_est
 
     def bytes_estimate(self):
         """Device bytes while in flight: mesh, pattern and contributions,
         FP64 + FP32 values and working copies, solver vectors."""
-        m = self.mesh
-        npe = np.asarray(m.elements).shape[1]
-        n_el = len(m.elements)
-        nnz = self.nnz_estimate()
-        return int(m.n_nodes * 24 + n_el * npe * 4 + n_el * npe * npe * 24
-                   + nnz * (8 + 4 + 16 + 4) + self.dofs * 8 * 12)
+        if getattr(self, "_bytes_est", None) is None:
+            m = self.mesh
+            npe = np.asarray(m.elements).shape[1]
+            n_el = len(m.elements)
+            nnz = self.nnz_estimate()
+            self._bytes_est = int(m.n_nodes * 24 + n_el * npe * 4 + n_el * npe * npe * 24
+                                  + nnz * (8 + 4 + 16 + 4) + self.dofs * 8 * 12)
+        return self._bytes_est
 
     def size_class(self):
         return int(np.log2(max(self.dofs, 1)))
@@ -241,13 +247,17 @@ class Server:
         t0 = time.perf_counter()
         errors = []
         inflight = set()
+        changed = True   # arrivals or freed slots since the last admission
         while pending or queue or inflight or any(e.busy for e in self._engines.values()):
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
-            # admit the oldest waiting requests into free slots
+                changed = True
+            # admit the oldest waiting requests into free slots (only when an
+            # arrival or a finished request changed the picture)
             budget = self.budget - self._engine_bytes - in_use
-            chosen = admit(queue, self._free_slots, budget, self._slot_class)
+            chosen = admit(queue, self._free_slots, budget, self._slot_class) if changed else []
+            changed = False
             if not chosen and queue and not inflight and \
                     not any(e.busy for e in self._engines.values()):
                 chosen = [queue[0]]   # larger than the whole budget: alone
@@ -268,6 +278,7 @@ class Server:
                         continue
                     inflight.discard(e)
                     for system, r, res in e.poll():
+                        changed = True
                         r.t_done = time.perf_counter() - t0
                         in_use -= r.bytes_estimate()
                         r.info = res
@@ -291,12 +302,16 @@ class Server:
     def _slot_class(self, r):
         """The engine class of a request: its size class, or the next one up
         when it would not fit (rows or stored blocks) the class's slots."""
+        cached = getattr(r, "_slot_cls", None)
+        if cached is not None:
+            return cached
         cls = r.size_class()
         bs = r.bs
         rows = r.mesh.n_nodes
         if rows > -(-(2 ** (cls + 1)) // bs) or r.nnz_estimate() // (bs * bs) > \
                 -(-(2 ** (cls + 1)) // bs) * SLOT_ROW_BLOCKS[r.kind]:
             cls += 1
+        r._slot_cls = cls
         return cls
 
     def _free_slots(self, kind, cls):
