@@ -174,6 +174,34 @@ def solve_eddy_current_nonlinear_tet10_T(mesh, T_elem, omega, B_applied=None, J_
     return a, v, info
 
 
+def _centroid_lookup(centroids, values):
+    """Callable(x, y, z) -> the value of the nearest centroid
+    (induction3d_tet10.py:216-230): exact at the centroids themselves,
+    where the element fields are evaluated. Takes scalars or arrays."""
+    from scipy.spatial import cKDTree
+    tree = cKDTree(np.asarray(centroids, dtype=float))
+    vals = np.asarray(values, dtype=float)
+
+    def fn(x, y, z):
+        pts = np.stack(np.broadcast_arrays(np.asarray(x, dtype=float), np.asarray(y, dtype=float),
+                                           np.asarray(z, dtype=float)), axis=-1)
+        _, idx = tree.query(pts)
+        out = vals[idx]
+        return float(out) if np.ndim(out) == 0 else out
+
+    return fn
+
+
+def _element_source_load(sub, Q_sub):
+    """Nodal load of an element-constant heat source Q_sub [W/m^3]
+    (induction3d_tet10.py:390-404): V Q_e sum_q w_q N_q per element, the
+    f-assembly of assemble_tet10, on the device."""
+    dm = DeviceMesh(sub)
+    _, F = dm.assemble(N.OP_T10_STIFF, coef=0.0,
+                       load=np.ascontiguousarray(np.asarray(Q_sub, dtype=float)))
+    return F.cpu().numpy()
+
+
 def _extract_submesh_tet10(mesh, elem_mask):
     """The masked Tet10 elements as a standalone Tet10Mesh (boundary tags
     not carried over), with the used node ids and the element ids

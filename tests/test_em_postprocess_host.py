@@ -4,6 +4,7 @@ phasor golden case): centroid flux density, exact Joule power and its
 per-element density, the source's complex power, and the B-H model curve."""
 
 import numpy as np
+import pytest
 
 import cases as C
 from conftest import assert_close
@@ -49,3 +50,16 @@ def test_induction_material_laws_match_reference(golden):
     assert_close(ind.steel_cp_T(Tt, cp_slope=1e-3, cp_peak_h=2e6), golden["law_cp"], 1e-15, "cp(T)")
     assert_close(ind.steel_enthalpy_T(Tt, cp_slope=1e-3, cp_peak_h=2e6), golden["law_H"],
                  1e-14, "H(T)")
+
+
+def test_centroid_lookup_scalar_and_array():
+    """The nearest-centroid coefficient of the induction chain
+    (induction3d_tet10.py:216-230) answers scalars with floats and arrays
+    element-wise (so device assembly samples it in one call)."""
+    pytest.importorskip("torch")
+    from cloudfem_b200.physics.induction3d_tet10 import _centroid_lookup
+    cen = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [0.0, 1.0, 0.0]])
+    fn = _centroid_lookup(cen, [3.0, 5.0, 7.0])
+    assert fn(0.1, 0.0, 0.0) == 3.0 and isinstance(fn(0.1, 0.0, 0.0), float)
+    got = fn(np.array([0.9, 0.1, 0.0]), np.array([1.0, 0.0, 0.9]), np.array([1.0, 0.0, 0.1]))
+    np.testing.assert_array_equal(got, [5.0, 3.0, 7.0])

@@ -299,6 +299,25 @@ def test_t10_joule_power_kernel_vs_oracle(cf):
     assert P2 == P
 
 
+def test_element_source_load_sums_to_power(cf):
+    """_element_source_load (induction3d_tet10.py:390-404) on the device
+    against the reference formula evaluated on the host per element
+    (vol Q_e sum_q w_q N_q, scattered to the element's nodes), and
+    ones . F = sum_e Q_e V_e."""
+    from cloudfem_b200.fem.tet10 import element_operators, quadrature
+    from cloudfem_b200.physics.induction3d_tet10 import _element_source_load
+    m = cf.mesh.box_mesh_tet10(3, 2, 2)
+    Q = np.random.default_rng(3).uniform(1e5, 1e6, m.n_elements)
+    F = _element_source_load(m, Q)
+    _, wq = quadrature()
+    ref = np.zeros(m.n_nodes)
+    for e, el in enumerate(np.asarray(m.elements)):
+        _, Nq, _, vol = element_operators(m, el)
+        np.add.at(ref, el, vol * Q[e] * (Nq * wq[:, None]).sum(axis=0))
+    assert np.abs(F - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert abs(F.sum() - float(Q @ m.element_volumes())) <= 1e-12 * F.sum()
+
+
 def test_av_magnetic_energy_golden(cf, golden):
     """W_m = Re(a^H K a)/4 with K assembled on the device."""
     from cloudfem_b200.physics import em3d_tet10 as em
