@@ -108,6 +108,8 @@ struct SysDev {
     int32_t sell;
     int32_t lpr;          // bs 1, unit-padded residual phase: lanes per row (4 or 8;
                           // 0 means 8)
+    int32_t rsell;        // bs 1, mixed, A phase staged: an FP64 sliced-ELL copy
+                          // (scol / sval / soff / sperm) for the residual phase
 };
 
 struct SysState {
@@ -2019,6 +2021,14 @@ using StageWarpOf = StageWarp<T, StageUnits<T>::W, StageUnits<T>::NB>;
 template <typename T>
 constexpr size_t gxs_smem() { return (size_t)GROUP * sizeof(StageWarpOf<T>); }
 
+#ifndef CFEM_RESIDUAL_SELL
+#define CFEM_RESIDUAL_SELL 1   // FP64 sliced-ELL residual copy for mixed P1 systems
+#endif
+// (defined with the sliced-ELL kernels below)
+template <typename T>
+__device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st, int64_t sl,
+                                             int lane, double part[4]);
+
 template <typename T, int LPR>
 __global__ void __launch_bounds__(32 * GROUP, StageUnits<T>::BLOCKS)
 k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
@@ -2046,6 +2056,12 @@ k_gxs(const SysDev *__restrict__ sys, SysState *st, GridBar *bar,
             phase_A_staged<T, sizeof(T) == 4, SU::W, SU::NB, SU::H, LPR>(
                 S, &st[e.x], r0, r1, lane, part, sm, &bar->err, &fail);
             if (fail && lane == 0) atomicExch(&bar->err, 2);
+        } else if (ph == PH_R && S.rsell) {
+            // the entry's slices of 32 rows in the FP64 sliced-ELL copy
+            // (entries are whole multiples of 32 rows, windows of 256 whole
+            // multiples of entries)
+            for (int64_t sl = r0 / 32; sl * 32 < r1; ++sl)
+                phase_R_sell<T>(S, &st[e.x], sl, lane, part);
         } else if (ph == PH_R) {
             int bad = 0;
             run_R<T, 1>(S, &st[e.x], r0, r1, lane, part, &bad);
@@ -3143,6 +3159,9 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
                             s, S.nnzb, S.v64, (double *)S.vsoa);
         } else if (S.vec4) {
             const unsigned g = std::min(grid_for(S.n * 32, 256), (unsigned)P->ctx->num_sms * 16);
+            if (S.rsell)
+                CFEM_LAUNCH(k_sell_fill<double>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n, S.rp,
+                            S.ci, S.v64, S.sperm, S.soff, (int32_t *)S.scol, (double *)S.sval);
             if (S.sell) {
                 if (S.mode == CFEM_SOLVE_MIXED)
                     CFEM_LAUNCH(k_sell_fill<float>, (unsigned)sell_windows(S.n), SELL_ROWS, 0, s, S.n, S.rp,
@@ -3183,14 +3202,15 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
     return CFEM_OK;
 }
 
-// Sliced-ELL layout of every scalar system flagged `sell`: row orders and
+// Sliced-ELL layout of every scalar system flagged `sell` (or `rsell`: an
+// FP64 copy for the residual phase of a mixed system): row orders and
 // slice offsets (k_sell_rank, then an exclusive scan of the slice sizes),
 // then room for the columns and values (filled by plan_copies).
 static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     size_t meta = 0;
     int64_t max_sl = 0;
     for (const SysDev &S : P->hs)
-        if (S.sell) {
+        if (S.sell || S.rsell) {
             const int64_t nw = sell_windows(S.n);
             const int64_t nsl = nw * (SELL_ROWS / sell_slice_rows(S.bs, P->lanes3));
             meta += align256((size_t)nw * SELL_ROWS) + 2 * align256((nsl + 1) * 8);
@@ -3208,7 +3228,7 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     std::vector<int64_t *> sizes_of(P->hs.size(), nullptr);
     for (size_t i = 0; i < P->hs.size(); ++i) {
         SysDev &S = P->hs[i];
-        if (!S.sell) continue;
+        if (!S.sell && !S.rsell) continue;
         const int rs = sell_slice_rows(S.bs, P->lanes3);
         const int64_t nw = sell_windows(S.n), nsl = nw * (SELL_ROWS / rs);
         uint8_t *perm = (uint8_t *)(P->ws_smeta + o);
@@ -3236,16 +3256,16 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     size_t data = 0;
     for (size_t i = 0; i < P->hs.size(); ++i) {
         const SysDev &S = P->hs[i];
-        if (!S.sell) continue;
-        const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
+        if (!S.sell && !S.rsell) continue;
+        const size_t ts = (S.mode == CFEM_SOLVE_MIXED && S.sell) ? 4 : 8;   // rsell: FP64
         data += align256((size_t)totals[i] * 4) + align256((size_t)totals[i] * S.bs * S.bs * ts);
     }
     CFEM_TRY(tmp_alloc(&P->ws_sdata, data, s));
     o = 0;
     for (size_t i = 0; i < P->hs.size(); ++i) {
         SysDev &S = P->hs[i];
-        if (!S.sell) continue;
-        const size_t ts = (S.mode == CFEM_SOLVE_MIXED) ? 4 : 8;
+        if (!S.sell && !S.rsell) continue;
+        const size_t ts = (S.mode == CFEM_SOLVE_MIXED && S.sell) ? 4 : 8;   // rsell: FP64
         S.scol = (const int32_t *)(P->ws_sdata + o);
         o += align256((size_t)totals[i] * 4);
         S.sval = P->ws_sdata + o;
@@ -3467,6 +3487,11 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                 S.sell = sell ? 1 : 0;
                 // short rows (P1: up to 16 entries, 4 units) on 4 lanes each
                 S.lpr = S.nnzb <= 16 * S.n ? 4 : 8;
+                // mixed P1 systems (a few iterations per solve, a residual
+                // phase nearly every iteration: time marches) take their
+                // FP64 residual from a sliced-ELL copy, one row per lane
+                S.rsell = (CFEM_RESIDUAL_SELL && !sell && !P->slots &&
+                           S.mode == CFEM_SOLVE_MIXED && S.lpr == 4) ? 1 : 0;
             }
         }
         // Scalar rows from the padded copy: eight chunks per SpMV work entry,
