@@ -56,6 +56,7 @@ SPMV_STAGE = None   # --spmv-stage: None keeps the library default
 SELL_SORT = None    # --sell-sort: None keeps the library default
 SELL3_LANES = None  # --sell3-lanes: None keeps the library default
 SELL3_STAGED = None  # --sell3-staged: None keeps the library default
+SLOT_SELL3 = None   # --slot-sell3: None keeps the library default
 
 
 def _set_scheduler(rt, name):
@@ -74,6 +75,8 @@ def _set_scheduler(rt, name):
         rt.set_param(N.PARAM_SELL3_LANES, SELL3_LANES)
     if SELL3_STAGED is not None:
         rt.set_param(N.PARAM_SELL3_STAGED, SELL3_STAGED)
+    if SLOT_SELL3 is not None:
+        rt.set_param(N.PARAM_SLOT_SELL3, SLOT_SELL3)
 
 
 def _block_spmv_kernel(rt, precision):
@@ -1272,8 +1275,12 @@ def main():
                     help="sliced-ELL SpMV of 3x3 blocks: 1 streams slices through shared "
                          "memory with bulk copies, 0 loads them into registers, 2 streams "
                          "FP32 slices only (default: the library's)")
+    ap.add_argument("--slot-sell3", type=int, default=None, choices=[0, 1],
+                    help="serving: 3x3 solve slots in the sliced-ELL layout (1) or the "
+                         "entry-major copy (0) (default: the library's)")
     args = ap.parse_args()
-    global SPMV_STAGE, SELL_SORT, SELL3_LANES, SELL3_STAGED
+    global SPMV_STAGE, SELL_SORT, SELL3_LANES, SELL3_STAGED, SLOT_SELL3
+    SLOT_SELL3 = args.slot_sell3
     SPMV_STAGE = args.spmv_stage
     SELL_SORT = args.sell_sort
     SELL3_LANES = args.sell3_lanes

@@ -36,6 +36,7 @@ PARAM_T10_WARPS, PARAM_P1_THREADS, PARAM_GRAPH_ITERS, PARAM_PDL, PARAM_SPMV_STAG
 PARAM_BARRIER_TIMEOUT_US, PARAM_BARRIER_HOLD, PARAM_SELL_SORT = 6, 7, 8
 PARAM_SELL3_LANES = 9
 PARAM_SELL3_STAGED = 10
+PARAM_SLOT_SELL3 = 11
 
 STATUS_NAMES = {
     CFEM_OK: "ok", CFEM_ERR_INVALID: "invalid argument",

@@ -81,6 +81,8 @@ struct cfem_ctx {
     int sell3_lanes = 4;               // sliced ELL of 3x3 blocks: lanes per block row
     int sell3_staged = 2;              // ... through a shared-memory ring: 1 always, 2 in
                                        // FP32 only (the faster choice measured), 0 never
+    int slot_sell3 = 1;                // solve slots of 3x3 systems: sliced ELL (1) or the
+                                       // entry-major copy (0)
     int barrier_timeout_us = 4000000;  // persistent grid-barrier wait limit
     int barrier_hold = 0;              // phantom barrier arrivals (fault injection)
     cudaStream_t work = nullptr;       // capture stream of the graph scheduler

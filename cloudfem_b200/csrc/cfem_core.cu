@@ -260,6 +260,11 @@ int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value) {
                        "sliced-ELL 3x3 staging must be 0, 1 or 2 (got %d)", value);
             ctx->sell3_staged = value;
             return CFEM_OK;
+        case CFEM_PARAM_SLOT_SELL3:
+            CFEM_CHECK(value == 0 || value == 1, CFEM_ERR_INVALID,
+                       "slot sliced-ELL switch must be 0 or 1 (got %d)", value);
+            ctx->slot_sell3 = value;
+            return CFEM_OK;
         case CFEM_PARAM_SELL3_LANES:
             CFEM_CHECK(value == 1 || value == 2 || value == 4, CFEM_ERR_INVALID,
                        "sliced-ELL lanes per 3x3 block row must be 1, 2 or 4 (got %d)", value);
@@ -291,6 +296,7 @@ int cfem_ctx_get_param(const cfem_ctx *ctx, int param) {
         case CFEM_PARAM_SELL_SORT: return ctx->sell_sort;
         case CFEM_PARAM_SELL3_LANES: return ctx->sell3_lanes;
         case CFEM_PARAM_SELL3_STAGED: return ctx->sell3_staged;
+        case CFEM_PARAM_SLOT_SELL3: return ctx->slot_sell3;
         case CFEM_PARAM_BARRIER_TIMEOUT_US: return ctx->barrier_timeout_us;
         case CFEM_PARAM_BARRIER_HOLD: return ctx->barrier_hold;
         default: return -1;

@@ -2241,6 +2241,9 @@ k_greduce(const SysDev *__restrict__ sys, SysState *st, GridBar *bar, int which)
 // unsorted rows: 14 %). The layout depends only on the system's pattern, so
 // sums are the same alone and in any batch.
 constexpr int SELL_ROWS = 256;
+// Longest block row a 3x3 solve slot's sliced-ELL copy is sized for (Tet10
+// vertex rows of box meshes hold up to 65 blocks).
+constexpr int SLOT_SELL_ROW = 96;
 constexpr int SELL_SLICES = SELL_ROWS / 32;
 constexpr int SELL_BLOCKS = 4;     // resident blocks of k_gxl per SM
 __host__ __device__ inline int64_t sell_windows(int64_t n) {
@@ -3106,6 +3109,24 @@ struct cfem_pcg_plan {
     // fixed capacity whose system is replaced between rounds of iterations
     bool slots = false;
     std::vector<int64_t> cap_rows, cap_nnzb;
+    // 3x3 slots in the sliced-ELL layout: entries each slot's copy holds,
+    // two sets of row orders and slice offsets per slot (the system being
+    // assigned ranks into the set the slot's last system did not use, on the
+    // caller's stream, while rounds of the others may still read the other),
+    // the set in use, the slice-size scan's scratch and a pinned word for
+    // the layout's size
+    struct SellMeta {
+        uint8_t *perm;
+        int64_t *sizes;
+        int64_t *soff;
+    };
+    std::vector<int64_t> cap_sell;
+    std::vector<SellMeta> smeta;      // slot i, set k at 2 i + k
+    std::vector<int> mset;
+    std::vector<cudaEvent_t> sev;     // per slot: its last assignment's table update ran
+    char *scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    int64_t *h_total = nullptr;
     std::vector<cfem::SysDev> tmpl;   // slot templates: workspace pointers
     char *tmpl_mem = nullptr;         // the templates' placeholder CSR
     cudaGraph_t pgraph[2] = {nullptr, nullptr};
@@ -3209,11 +3230,12 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
 static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     size_t meta = 0;
     int64_t max_sl = 0;
+    const int sets = P->slots ? 2 : 1;
     for (const SysDev &S : P->hs)
         if (S.sell || S.rsell) {
             const int64_t nw = sell_windows(S.n);
             const int64_t nsl = nw * (SELL_ROWS / sell_slice_rows(S.bs, P->lanes3));
-            meta += align256((size_t)nw * SELL_ROWS) + 2 * align256((nsl + 1) * 8);
+            meta += sets * (align256((size_t)nw * SELL_ROWS) + 2 * align256((nsl + 1) * 8));
             max_sl = std::max(max_sl, nsl + 1);
         }
     if (!meta) return CFEM_OK;
@@ -3225,18 +3247,27 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     CFEM_TRY(tmp_alloc(&scan_tmp, scan_bytes, s));
     size_t o = 0;
     std::vector<int64_t> totals(P->hs.size(), 0);
-    std::vector<int64_t *> sizes_of(P->hs.size(), nullptr);
+    if (P->slots) {
+        P->smeta.assign(2 * P->hs.size(), cfem_pcg_plan::SellMeta{nullptr, nullptr, nullptr});
+        P->mset.assign(P->hs.size(), 0);
+        P->cap_sell.assign(P->hs.size(), 0);
+    }
     for (size_t i = 0; i < P->hs.size(); ++i) {
         SysDev &S = P->hs[i];
         if (!S.sell && !S.rsell) continue;
         const int rs = sell_slice_rows(S.bs, P->lanes3);
         const int64_t nw = sell_windows(S.n), nsl = nw * (SELL_ROWS / rs);
-        uint8_t *perm = (uint8_t *)(P->ws_smeta + o);
-        o += align256((size_t)nw * SELL_ROWS);
-        int64_t *sizes = (int64_t *)(P->ws_smeta + o);
-        o += align256((nsl + 1) * 8);
-        int64_t *soff = (int64_t *)(P->ws_smeta + o);
-        o += align256((nsl + 1) * 8);
+        uint8_t *perm = nullptr;
+        int64_t *sizes = nullptr, *soff = nullptr;
+        for (int k = 0; k < sets; ++k) {
+            perm = (uint8_t *)(P->ws_smeta + o);
+            o += align256((size_t)nw * SELL_ROWS);
+            sizes = (int64_t *)(P->ws_smeta + o);
+            o += align256((nsl + 1) * 8);
+            soff = (int64_t *)(P->ws_smeta + o);
+            o += align256((nsl + 1) * 8);
+            if (P->slots) P->smeta[2 * i + (sets - 1 - k)] = {perm, sizes, soff};
+        }   // (slots: the template ranks into set 0, the last one taken)
         CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
         const int srt = P->ctx->sell_sort;
         if (rs == 32)
@@ -3251,8 +3282,29 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
         S.sperm = perm;
         S.soff = soff;
     }
-    tmp_free(scan_tmp, s);
+    if (P->slots) {          // kept for the systems assigned later
+        P->scan_tmp = scan_tmp;
+        P->scan_bytes = scan_bytes;
+    } else {
+        tmp_free(scan_tmp, s);
+    }
     CFEM_CUDA(cudaStreamSynchronize(s));
+    // Slots: room for any system within the capacity whose longest block
+    // row has at most SLOT_SELL_ROW blocks. Windows sorted by length make a
+    // slice no longer than the shortest row of the slice before it, so a
+    // window's slices hold at most its rows' blocks (+1 for an absent
+    // diagonal), RS x its longest row, and L - 1 per row of rounding to
+    // whole steps. A system beyond that is refused at assignment.
+    for (size_t i = 0; P->slots && i < P->hs.size(); ++i) {
+        const SysDev &S = P->hs[i];
+        if (!S.sell) continue;
+        const int rs = sell_slice_rows(S.bs, P->lanes3), l = 32 / rs;
+        const int64_t nw = sell_windows(S.n);
+        const int64_t bound = S.nnzb + S.n + nw * ((int64_t)rs * SLOT_SELL_ROW +
+                                                   (int64_t)SELL_ROWS * (l - 1));
+        totals[i] = std::max(totals[i], bound);
+        P->cap_sell[i] = totals[i];
+    }
     size_t data = 0;
     for (size_t i = 0; i < P->hs.size(); ++i) {
         const SysDev &S = P->hs[i];
@@ -3290,6 +3342,7 @@ static void plan_free(cfem_pcg_plan *P) {
         if (P->ws_smeta) cudaFreeAsync(P->ws_smeta, P->w);
         if (P->tmpl_mem) cudaFreeAsync(P->tmpl_mem, P->w);
         if (P->ws_sdata) cudaFreeAsync(P->ws_sdata, P->w);
+        if (P->scan_tmp) cudaFreeAsync(P->scan_tmp, P->w);
         cudaStreamSynchronize(P->w);
     }
     for (int i = 0; i < 4; ++i)
@@ -3298,6 +3351,9 @@ static void plan_free(cfem_pcg_plan *P) {
         for (int j = 0; j < 2; ++j)
             if (P->tev[i][j]) cudaEventDestroy(P->tev[i][j]);
     if (P->h_flags) cudaFreeHost(P->h_flags);
+    if (P->h_total) cudaFreeHost(P->h_total);
+    for (cudaEvent_t e : P->sev)
+        if (e) cudaEventDestroy(e);
     if (P->w2) cudaStreamDestroy(P->w2);
     if (P->w) cudaStreamDestroy(P->w);
     (void)cudaGetLastError();
@@ -3414,10 +3470,12 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
     int tstage[4];
     for (int t = 0; t < 4; ++t)
         tstage[t] = ctx->spmv_stage != 4 ? ctx->spmv_stage : (t == 2 ? 1 : 3);
-    // solve slots: copies whose size follows the capacity alone (no sliced
-    // ELL, whose padding depends on the system)
+    // solve slots: scalar rows from the unit-padded copy (its size follows
+    // the capacity alone); 3x3 blocks in the sliced ELL (SLOT_SELL3, room
+    // for a bound on the padding, the layout built at assignment) or from
+    // the entry-major copy
     if (P->slots)
-        for (int t = 0; t < 4; ++t) tstage[t] = (t & 1) ? 0 : 1;
+        for (int t = 0; t < 4; ++t) tstage[t] = (t & 1) ? (ctx->slot_sell3 ? 3 : 0) : 1;
     auto stage_of = [&](const SysDev &S) {
         return tstage[(S.mode == CFEM_SOLVE_MIXED ? 2 : 0) + (S.bs == 3 ? 1 : 0)];
     };
@@ -3977,6 +4035,16 @@ extern "C" int cfem_pcg_slots_create(cfem_ctx *ctx, int32_t n_slots, int32_t bs,
         t.mode = mode;
     }
     int st = plan_build(ctx, L.data(), n_slots, s, P);
+    if (st == CFEM_OK && cudaMallocHost(&P->h_total, sizeof(int64_t)) != cudaSuccess) {
+        P->h_total = nullptr;
+        st = fail(CFEM_ERR_NOMEM, "slot plan: pinned host word");
+    }
+    if (st == CFEM_OK) {
+        P->sev.assign(n_slots, nullptr);
+        for (int i = 0; i < n_slots && st == CFEM_OK; ++i)
+            if (cudaEventCreateWithFlags(&P->sev[i], cudaEventDisableTiming) != cudaSuccess)
+                st = fail(CFEM_ERR_CUDA, "slot plan: events");
+    }
     if (st == CFEM_OK) {
         P->tmpl = P->hs;
         P->cap_rows.assign(n_slots, max_rows);
@@ -4017,6 +4085,40 @@ extern "C" int cfem_pcg_slots_assign(cfem_pcg_plan *P, int32_t slot, const cfem_
     CFEM_CHECK(L->rtol > 0.0 && L->max_iter > 0, CFEM_ERR_INVALID,
                "rtol and max_iter must be positive");
     cudaStream_t s = (cudaStream_t)stream;
+    // 3x3 slots in the sliced ELL: rank the new system's windows and scan
+    // its slice sizes on the caller's stream (after its assembly), into the
+    // row-order set the slot's previous system did not use
+    const bool sell3 = T.bs == 3 && T.sell;
+    int set = 0;
+    if (sell3) {
+        set = 1 - P->mset[slot];
+        const cfem_pcg_plan::SellMeta &M = P->smeta[2 * slot + set];
+        const int rs = sell_slice_rows(3, P->lanes3);
+        const int64_t nw = sell_windows(L->n_rows), nsl = nw * (SELL_ROWS / rs);
+        size_t need = 0;
+        CFEM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, need, (const int64_t *)nullptr,
+                                                (int64_t *)nullptr, nsl + 1, s));
+        CFEM_CHECK(need <= P->scan_bytes && P->h_total, CFEM_ERR_NOMEM,
+                   "slot %d: slice-size scan scratch too small", slot);
+        // rounds queued before the slot's last assignment may still read
+        // this set (a slot freed by cfem_pcg_slots_poll has synchronised
+        // them already; the wait then costs nothing)
+        CFEM_CUDA(cudaStreamWaitEvent(s, P->sev[slot], 0));
+        CFEM_CUDA(cudaMemsetAsync(M.sizes + nsl, 0, sizeof(int64_t), s));
+        const int srt = P->ctx->sell_sort;
+        if (rs == 32)
+            CFEM_LAUNCH(k_sell_rank<32>, (unsigned)nw, SELL_ROWS, 0, s, L->n_rows, L->d_row_ptr,
+                        L->d_col, M.perm, M.sizes, srt);
+        else if (rs == 16)
+            CFEM_LAUNCH(k_sell_rank<16>, (unsigned)nw, SELL_ROWS, 0, s, L->n_rows, L->d_row_ptr,
+                        L->d_col, M.perm, M.sizes, srt);
+        else
+            CFEM_LAUNCH(k_sell_rank<8>, (unsigned)nw, SELL_ROWS, 0, s, L->n_rows, L->d_row_ptr,
+                        L->d_col, M.perm, M.sizes, srt);
+        CFEM_CUDA(cub::DeviceScan::ExclusiveSum(P->scan_tmp, need, M.sizes, M.soff, nsl + 1, s));
+        CFEM_CUDA(cudaMemcpyAsync(P->h_total, M.soff + nsl, sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, s));
+    }
     int32_t nnzb = 0;
     CFEM_CUDA(cudaMemcpyAsync(&nnzb, L->d_row_ptr + L->n_rows, sizeof(int32_t),
                               cudaMemcpyDeviceToHost, s));
@@ -4024,7 +4126,14 @@ extern "C" int cfem_pcg_slots_assign(cfem_pcg_plan *P, int32_t slot, const cfem_
     CFEM_CHECK(nnzb >= 0 && nnzb <= P->cap_nnzb[slot], CFEM_ERR_INVALID,
                "system has %d blocks, slot %d holds %lld", nnzb, slot,
                (long long)P->cap_nnzb[slot]);
+    CFEM_CHECK(!sell3 || *P->h_total <= P->cap_sell[slot], CFEM_ERR_INVALID,
+               "system's sliced-ELL layout has %lld blocks, slot %d holds %lld",
+               (long long)*P->h_total, slot, (long long)P->cap_sell[slot]);
     SysDev S = T;   // the slot's workspace, lists and copies
+    if (sell3) {
+        S.sperm = P->smeta[2 * slot + set].perm;
+        S.soff = P->smeta[2 * slot + set].soff;
+    }
     S.n = L->n_rows;
     S.nnzb = nnzb;
     if (S.vec4) S.lpr = S.nnzb <= 16 * S.n ? 4 : 8;
@@ -4053,7 +4162,9 @@ extern "C" int cfem_pcg_slots_assign(cfem_pcg_plan *P, int32_t slot, const cfem_
     CFEM_CUDA(cudaStreamWaitEvent(w, P->ev[0], 0));
     CFEM_CUDA(cudaMemcpyAsync(P->d_sys + slot, &P->hs[slot], sizeof(SysDev),
                               cudaMemcpyHostToDevice, w));
+    if (sell3) CFEM_CUDA(cudaEventRecord(P->sev[slot], w));
     CFEM_TRY(plan_copies(P, w, slot, slot + 1));
+    if (sell3) P->mset[slot] = set;
     CFEM_CUDA(cudaMemsetAsync(P->d_st + slot, 0, sizeof(SysState), w));
     CFEM_CUDA(cudaMemsetAsync(S.tcnt, 0, (size_t)T.ntiles * sizeof(unsigned), w));
     CFEM_LAUNCH(k_slot_open, 1, 32, 0, w, P->d_bar);

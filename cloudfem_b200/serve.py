@@ -353,6 +353,12 @@ def engine_bytes(eng, mode):
     if eng.bs == 1:
         ne = eng.max_nnzb + 3 * eng.max_rows + 8
         copies = ne * (4 + 8 + (4 if mode == N.SOLVE_MIXED else 0))
+    elif eng.rt.get_param(N.PARAM_SLOT_SELL3) == 1:
+        # sliced ELL: room for block rows of up to 96 blocks (slices of 8
+        # block rows on 4 lanes, windows of 256 rows), two row-order sets
+        nw = -(-eng.max_rows // 256)
+        cap = eng.max_nnzb + eng.max_rows + nw * (8 * 96 + 256 * 3)
+        copies = cap * (bs2 * ts + 4) + 2 * (256 * nw + 16 * (32 * nw + 1))
     else:
         copies = eng.max_nnzb * bs2 * ts
     return eng.n_slots * (vec + copies)

@@ -200,12 +200,16 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * three shared-memory stages filled by 1-D bulk copies (the first issued
  * before the kernel waits for its predecessor), 0 loads them into
  * registers, 2 (default) streams FP32 slices and loads FP64 ones (the
- * faster of the two measured for each). get returns -1 for an unknown
+ * faster of the two measured for each). SLOT_SELL3: solve slots
+ * (cfem_pcg_slots_*) of 3x3 systems store them in the sliced ELL (1,
+ * default; room for rows of up to 96 blocks, the layout built when a
+ * system is assigned, a system needing more refused) or in the entry-major
+ * copy (0); read when the slots are created. get returns -1 for an unknown
  * parameter. */
 enum { CFEM_PARAM_T10_WARPS = 1, CFEM_PARAM_P1_THREADS = 2, CFEM_PARAM_GRAPH_ITERS = 3,
        CFEM_PARAM_PDL = 4, CFEM_PARAM_SPMV_STAGE = 5, CFEM_PARAM_BARRIER_TIMEOUT_US = 6,
        CFEM_PARAM_BARRIER_HOLD = 7, CFEM_PARAM_SELL_SORT = 8, CFEM_PARAM_SELL3_LANES = 9,
-       CFEM_PARAM_SELL3_STAGED = 10 };
+       CFEM_PARAM_SELL3_STAGED = 10, CFEM_PARAM_SLOT_SELL3 = 11 };
 CFEM_API int cfem_ctx_set_param(cfem_ctx *ctx, int param, int value);
 CFEM_API int cfem_ctx_get_param(const cfem_ctx *ctx, int param);
 /* Number of kernels this library launched through `ctx` so far. */
@@ -482,7 +486,11 @@ CFEM_API int cfem_pcg_plan_destroy(cfem_pcg_plan *plan);
  * (status CFEM_SLOT_RUNNING while a system iterates; a finished system keeps
  * its status until the slot is assigned again), ready returns CFEM_OK once
  * the queued rounds have run and CFEM_SLOT_RUNNING before (no wait), release
- * ends a running system or frees a finished one. The caller keeps a system's arrays alive
+ * ends a running system or frees a finished one. 3x3 slots hold the
+ * sliced-ELL layout by default (CFEM_PARAM_SLOT_SELL3): assign then also
+ * refuses (CFEM_ERR_INVALID, nothing changed) a system whose layout exceeds
+ * the slot's room, which a block row of more than 96 blocks can cause.
+ * The caller keeps a system's arrays alive
  * while it is in a slot and reads x after poll reports it finished. Each
  * system's scalars and sums are its own, so its iterates do not depend on
  * the other slots. Calls on one slot plan must come from one thread at a
