@@ -118,8 +118,10 @@ def test_slot_reuse_is_bitwise(torch):
 
 def test_oversized_layout_refused(torch):
     """Rows of 1,000 blocks (one per window of 256 block rows) need about
-    three times the room a slot of this capacity keeps: assign refuses the
-    system and changes nothing; the next system solves."""
+    three times the room a slot of this capacity keeps (89,920 entries
+    against 30,720): assign refuses the system (an invalid argument,
+    ValueError as in the reference) and changes nothing; the next system
+    solves."""
     from cloudfem_b200 import _native as N
     from cloudfem_b200.device import BlockSystem, pcg
     rt = N.runtime()
@@ -143,7 +145,7 @@ def test_oversized_layout_refused(torch):
                       torch.ones(3 * n, dtype=torch.float64, device=dev),
                       torch.zeros(3 * n, dtype=torch.float64, device=dev))
     eng = _engine(rt, 1, 1, N.SOLVE_FP64, n, cap_nnzb)
-    with pytest.raises(RuntimeError, match="sliced-ELL layout"):
+    with pytest.raises(ValueError, match="sliced-ELL layout has 89920 blocks"):
         eng.assign(bad, 1e-10, tag="bad")
     assert eng.free == [0]
     cube = _elastic((3, 3, 3), (1.0, 1.0, 1.0))
