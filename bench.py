@@ -721,7 +721,7 @@ def run_transient_heat(args, rank, world, local_rank):
     dm = DeviceMesh(mesh, local_rank)
     free = mesh.n_nodes                       # Robin everywhere: no fixed DOF
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    rtol = 1e-10 if args.precision == "mixed" else 1e-12
+    rtol = args.transient_rtol or (1e-10 if args.precision == "mixed" else 1e-12)
 
     # accuracy gate: the first 20 steps in both precisions
     gate = min(20, n_steps)
@@ -1255,6 +1255,9 @@ def main():
                          "for per-launch profiling)")
     ap.add_argument("--transient-n", type=int, default=TRANSIENT_N,
                     help="transient-heat: cells per box edge")
+    ap.add_argument("--transient-rtol", type=float, default=None,
+                    help="transient-heat: relative residual per time step (default 1e-10 "
+                         "mixed, 1e-12 FP64)")
     ap.add_argument("--transient-steps", type=int, default=TRANSIENT_STEPS,
                     help="transient-heat: time steps per bench step")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES,
