@@ -2592,9 +2592,28 @@ __device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st
     const int32_t *cp = S.scol + base + lane;
     const double *vp = (const double *)S.sval + base + lane;
     double hi = 0.0, lo = 0.0, aab = 0.0;
-    for (int k = 0; k < w; ++k) {
+    // U slots in flight per lane (their column and value loads, then the
+    // gathers of x, read-only in this launch), summed in slot order
+    constexpr int U = 8;
+    int k = 0;
+    for (; k + U <= w; k += U) {
+        int32_t c[U];
+        double a[U], xj[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) c[j] = ld_stream(cp + 32 * (k + j));
+#pragma unroll
+        for (int j = 0; j < U; ++j) a[j] = ld_stream(vp + 32 * (k + j));
+#pragma unroll
+        for (int j = 0; j < U; ++j) xj[j] = __ldg(S.x + c[j]);
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            dd_fma(hi, lo, a[j], xj[j]);
+            aab += fabs(a[j] * xj[j]);
+        }
+    }
+    for (; k < w; ++k) {
         const double a = ld_stream(vp + 32 * k);
-        const double xj = __ldg(S.x + ld_stream(cp + 32 * k));   // read-only in this launch
+        const double xj = __ldg(S.x + ld_stream(cp + 32 * k));
         dd_fma(hi, lo, a, xj);
         aab += fabs(a * xj);
     }
