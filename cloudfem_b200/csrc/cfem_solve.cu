@@ -898,6 +898,10 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
 // Which phases a kernel handles.
 enum { RUN_INIT = 0, RUN_ALL = 1, RUN_X = 2, RUN_B = 3 };
 
+// (defined with the sliced-ELL kernels below)
+template <typename T>
+__device__ void init_R_sell(const SysDev &S, int64_t lc, int lane, double part[4], int *bad);
+
 template <typename T, int BS, int RUN>
 __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
                           int lc, int lane) {
@@ -908,7 +912,9 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
     if (RUN == RUN_INIT) {
         int flag = 0;
         // (x is not written while the residual is initialised: L1 gathers)
-        if (BS == 1 && S.vec4)
+        if (BS == 1 && S.rsell)
+            init_R_sell<T>(S, lc, lane, part, &flag);
+        else if (BS == 1 && S.vec4)
             S.lpr == 4 ? phase_R_vec1<T, true, true, 4>(S, st, r0, r1, lane, part, &flag)
                        : phase_R_vec1<T, true, true, 8>(S, st, r0, r1, lane, part, &flag);
         else
@@ -2630,6 +2636,65 @@ __device__ __forceinline__ void phase_R_sell(const SysDev &S, const SysState *st
     part[1] += (double)(rv * ldcg(pc + i));
     part[2] += (double)(rv * zv);
     if (!fx) part[3] += aab * aab;
+}
+
+// INIT from the sliced FP64 copy of a mixed P1 system (`rsell`). A window
+// of SELL_ROWS rows holds SELL_ROWS / 16 chunks of 16 rows and SELL_SLICES
+// slices of 32: the warp of the window's chunk 2s takes slice s (one row
+// per lane) and reports its sums, the warp of chunk 2s + 1 reports none, so
+// the chunk partials and their tickets are those of the other INIT paths.
+// Writes what phase_R_vec1<INIT> writes: r = b - A x (compensated sums),
+// the Jacobi inverse from the diagonal (slot 0; 0 there if the pattern has
+// none: a bad row), z, and rr, |b'|^2 (b less the fixed columns' part),
+// r.z and the floor sum.
+template <typename T>
+__device__ void init_R_sell(const SysDev &S, int64_t lc, int lane, double part[4], int *bad) {
+    constexpr int CPW = SELL_ROWS / 16;   // chunks per window
+    const int64_t win = lc / CPW;
+    const int j = (int)(lc % CPW);
+    if (j & 1) return;
+    const int s = j >> 1;
+    const int64_t sl = win * SELL_SLICES + s;
+    const int64_t r0 = win * SELL_ROWS;
+    const int nr = (int)min((int64_t)SELL_ROWS, S.n - r0);
+    if (s * 32 >= nr) return;
+    const int64_t base = __ldg(S.soff + sl);
+    const int w = (int)((__ldg(S.soff + sl + 1) - base) >> 5);
+    const int rl = __ldg(S.sperm + r0 + s * 32 + lane);
+    const int32_t *cp = S.scol + base + lane;
+    const double *vp = (const double *)S.sval + base + lane;
+    const double dg = w > 0 ? ld_stream(vp) : 0.0;
+    double hi = 0.0, lo = 0.0, aab = 0.0, accf = 0.0;
+    for (int k = 0; k < w; ++k) {
+        const int32_t c = ld_stream(cp + 32 * k);
+        const double a = ld_stream(vp + 32 * k);
+        const double xj = __ldg(S.x + c);   // x is not written in INIT
+        const double ax = a * xj;
+        dd_fma(hi, lo, a, xj);
+        aab += fabs(ax);
+        if (S.fixed && __ldg(S.fixed + c) != 0) accf += ax;
+    }
+    if (rl >= nr) return;
+    const int64_t i = r0 + rl;
+    const bool fx = S.fixed ? (__ldg(S.fixed + i) != 0) : false;
+    const double bi = __ldg(S.b + i);
+    const double rt = fx ? 0.0 : dd_residual(bi, hi, lo);
+    double iv = 0.0;
+    if (!fx) {
+        if (!(dg > 0.0) || !isfinite(dg)) *bad = 1;
+        else iv = 1.0 / dg;
+        const double bl = bi - accf;
+        part[1] += bl * bl;
+        part[3] += aab * aab;
+    }
+    const T rv = (T)rt;
+    const T dv = (T)iv;
+    ((T *)S.r)[i] = rv;
+    ((T *)S.dinv)[i] = dv;
+    const T zv = fx ? (T)0 : dv * rv;
+    ((T *)S.z)[i] = zv;
+    part[0] += rt * rt;
+    part[2] += (double)(rv * zv);
 }
 
 // k_gx for scalar systems with the sliced-ELL A phase: one slice of 32
