@@ -3178,7 +3178,9 @@ struct cfem_pcg_plan {
     cudaStream_t w = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t tev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    int *h_flags = nullptr;
+    int *h_flags = nullptr;       // pinned: [0..1] polled active counts, [2] active
+                                  // count sent, [3] error word, [4] loop rounds
+    cfem::SysState *h_st = nullptr;   // pinned: the systems' states after a solve
     cudaStream_t w2 = nullptr;    // captures the loop body
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -3435,6 +3437,7 @@ static void plan_free(cfem_pcg_plan *P) {
         for (int j = 0; j < 2; ++j)
             if (P->tev[i][j]) cudaEventDestroy(P->tev[i][j]);
     if (P->h_flags) cudaFreeHost(P->h_flags);
+    if (P->h_st) cudaFreeHost(P->h_st);
     if (P->h_total) cudaFreeHost(P->h_total);
     for (cudaEvent_t e : P->sev)
         if (e) cudaEventDestroy(e);
@@ -3458,7 +3461,8 @@ static int plan_build(cfem_ctx *ctx, const cfem_linsys *systems, int n_systems,
                                                             : cudaEventDefault));
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2; ++j) CFEM_CUDA(cudaEventCreate(&P->tev[i][j]));
-    CFEM_CUDA(cudaMallocHost(&P->h_flags, 4 * sizeof(int)));
+    CFEM_CUDA(cudaMallocHost(&P->h_flags, 8 * sizeof(int)));
+    CFEM_CUDA(cudaMallocHost(&P->h_st, (size_t)n_systems * sizeof(SysState)));
     std::vector<SysDev> &hs = P->hs;
     hs.assign(n_systems, SysDev{});
     std::vector<int32_t> chunk_sys;
@@ -3916,22 +3920,25 @@ static int plan_run(cfem_pcg_plan *P, cfem_solve_stats *stats, cudaStream_t s) {
         CFEM_CUDA(cudaGraphLaunch(P->exec, w));
     }
     CFEM_CUDA(cudaEventRecord(P->ev[3], w));
-    std::vector<SysState> hst(n_systems);
-    int h_err = 0;
-    CFEM_CUDA(cudaMemcpyAsync(hst.data(), d_st, n_systems * sizeof(SysState),
+    // states, error word and loop rounds into pinned memory: one wait
+    const bool graph_loop = !P->persistent && !P->polled;
+    CFEM_CUDA(cudaMemcpyAsync(P->h_st, d_st, n_systems * sizeof(SysState),
                               cudaMemcpyDeviceToHost, w));
-    CFEM_CUDA(cudaMemcpyAsync(&h_err, &d_bar->err, sizeof(int),
+    CFEM_CUDA(cudaMemcpyAsync(&P->h_flags[3], &d_bar->err, sizeof(int),
                               cudaMemcpyDeviceToHost, w));
+    if (graph_loop)
+        CFEM_CUDA(cudaMemcpyAsync(&P->h_flags[4], &d_bar->rounds, sizeof(unsigned),
+                                  cudaMemcpyDeviceToHost, w));
     CFEM_CUDA(cudaStreamSynchronize(w));
+    const SysState *hst = P->h_st;
+    const int h_err = P->h_flags[3];
     // later work on s sees the solution
     CFEM_CUDA(cudaEventRecord(P->ev[0], w));
     CFEM_CUDA(cudaStreamWaitEvent(s, P->ev[0], 0));
     float kms = 0.0f;
     CFEM_CUDA(cudaEventElapsedTime(&kms, P->ev[2], P->ev[3]));
-    if (!P->persistent && !P->polled) {
-        unsigned rounds = 0;
-        CFEM_CUDA(cudaMemcpy(&rounds, &d_bar->rounds, sizeof(unsigned),
-                             cudaMemcpyDeviceToHost));
+    if (graph_loop) {
+        const unsigned rounds = (unsigned)P->h_flags[4];
         const int64_t bodies = rounds > 0 ? (int64_t)rounds - 1 : 0;
         g_launches.fetch_add(3 + P->per_iter + bodies * (P->giters * P->per_iter + 1),
                              std::memory_order_relaxed);
@@ -4292,12 +4299,13 @@ extern "C" int cfem_pcg_slots_poll(cfem_pcg_plan *P, cfem_solve_stats *stats) {
     CFEM_CHECK(P && P->slots && stats, CFEM_ERR_INVALID, "cfem_pcg_slots_poll: bad args");
     CFEM_TRY(set_device(P->device));
     const int n = P->n_systems;
-    std::vector<SysState> hst(n);
-    int h_err = 0;
-    CFEM_CUDA(cudaMemcpyAsync(hst.data(), P->d_st, n * sizeof(SysState),
+    CFEM_CUDA(cudaMemcpyAsync(P->h_st, P->d_st, n * sizeof(SysState),
                               cudaMemcpyDeviceToHost, P->w));
-    CFEM_CUDA(cudaMemcpyAsync(&h_err, &P->d_bar->err, sizeof(int), cudaMemcpyDeviceToHost, P->w));
+    CFEM_CUDA(cudaMemcpyAsync(&P->h_flags[3], &P->d_bar->err, sizeof(int),
+                              cudaMemcpyDeviceToHost, P->w));
     CFEM_CUDA(cudaStreamSynchronize(P->w));
+    const SysState *hst = P->h_st;
+    const int h_err = P->h_flags[3];
     for (int i = 0; i < n; ++i) {
         cfem_solve_stats &o = stats[i];
         memset(&o, 0, sizeof(o));
