@@ -72,3 +72,36 @@ def test_stream_cap_keeps_the_full_streams_requests():
         else:
             assert np.array_equal(r.k, f.k)
         assert r.dofs < 4 * 5e3
+
+
+class _FakeRt:
+    def __init__(self, slot_sell3):
+        self.slot_sell3 = slot_sell3
+
+    def get_param(self, param):
+        from cloudfem_b200 import _native as N
+        assert param == N.PARAM_SLOT_SELL3
+        return self.slot_sell3
+
+
+class _FakeEngine:
+    def __init__(self, rt, n_slots, bs, max_rows, max_nnzb):
+        self.rt, self.n_slots, self.bs = rt, n_slots, bs
+        self.max_rows, self.max_nnzb = max_rows, max_nnzb
+
+
+def test_engine_bytes_cover_the_sliced_slot_room():
+    """The budget estimate of a 3x3 engine in the sliced ELL counts the
+    room the library keeps per slot (blocks + rows + per window 8 rows of
+    96 blocks and 3 blocks of step rounding per row), columns and values,
+    and two row-order sets; the entry-major copy counts values only."""
+    from cloudfem_b200 import _native as N
+    rows, nnzb = 100_000, 3_000_000
+    nw = -(-rows // 256)
+    room = nnzb + rows + nw * (8 * 96 + 256 * 3)
+    vec = 6 * 3 * rows * 4 + 3 * rows * 8
+    sliced = serve.engine_bytes(_FakeEngine(_FakeRt(1), 2, 3, rows, nnzb), N.SOLVE_MIXED)
+    assert sliced == 2 * (vec + room * (9 * 4 + 4) + 2 * (256 * nw + 16 * (32 * nw + 1)))
+    entry = serve.engine_bytes(_FakeEngine(_FakeRt(0), 2, 3, rows, nnzb), N.SOLVE_MIXED)
+    assert entry == 2 * (vec + nnzb * 9 * 4)
+    assert 1.1 < sliced / entry < 1.4
