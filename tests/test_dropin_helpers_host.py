@@ -82,3 +82,29 @@ def test_sample_points():
     p1 = O.box_mesh(*C.P1_BOX)
     np.testing.assert_allclose(centroids(p1.nodes, p1.elements),
                                p1.nodes[p1.elements].mean(axis=1), rtol=0, atol=1e-15)
+
+
+def test_coefficient_evaluation_in_chunks():
+    """Callables are called on chunks of points: the values equal one call
+    on all points bitwise (and the reference's pointwise values); scalars,
+    constant-returning and scalar-only callables keep their meaning."""
+    from cloudfem_b200 import device as D
+    rng = np.random.default_rng(3)
+    pts = rng.random((3 * D.EVAL_CHUNK + 17, 4, 3))
+    f = lambda x, y, z: np.sin(3 * x) * y + np.exp(-z)  # noqa: E731
+    v = D.evaluate(f, pts)
+    assert v.shape == (3 * D.EVAL_CHUNK + 17, 4)
+    np.testing.assert_array_equal(v, f(pts[..., 0], pts[..., 1], pts[..., 2]))
+    calls = []
+
+    def counted(x, y, z):
+        calls.append(np.size(x))
+        return x + y + z
+    D.evaluate(counted, pts)
+    assert max(calls) == D.EVAL_CHUNK and sum(calls) == pts.size // 3
+    assert D.evaluate(2.5, pts) == 2.5
+    np.testing.assert_array_equal(D.evaluate(lambda x, y, z: 7.0, pts), np.full(pts.shape[:-1], 7.0))
+    few = pts[:5, :1]
+    scalar_only = lambda x, y, z: float(x) * 2.0 + (1.0 if y > 0.5 else 0.0)  # noqa: E731
+    want = [scalar_only(*p) for p in few.reshape(-1, 3)]
+    np.testing.assert_array_equal(D.evaluate(scalar_only, few).ravel(), want)
