@@ -234,11 +234,17 @@ CFEM_API int cfem_pattern_node_csr(const cfem_pattern *p, const int32_t **d_row_
  * d_indptr (n_nodes*bs+1), d_indices (nnz*bs*bs). */
 CFEM_API int cfem_pattern_expand(const cfem_pattern *p, int32_t bs, int32_t *d_indptr,
                         int32_t *d_indices, void *stream);
-/* Block values (nnz*bs*bs, block-major) -> scalar CSR value order. */
+/* Block values (nnz*bs*bs, block-major) -> scalar CSR value order: the
+ * csr_matrix the reference's assemble_elasticity_* return
+ * (elastic3d.py:188, elastic_tet10.py:208-210), built from device blocks. */
 CFEM_API int cfem_block_to_csr(const cfem_pattern *p, int32_t bs,
                       const double *d_bvals, double *d_vals, void *stream);
 
 /* ---- element assembly ---------------------------------------------------
+ * Replaces the element loops of assemble (tet_poisson.py:35-69),
+ * assemble_mass_tet (tet_heat.py:72-94), assemble_tet10 (tet10.py:138-165)
+ * and assemble_mass_tet10 (tet10.py:229-249), and the scalar blocks of
+ * assemble_tet10_av (em3d_tet10.py:172-264) through the NGRAD operators.
  * Computes every element matrix (one thread per P1 element, one warp per
  * Tet10 element with shape gradients staged in shared memory) and reduces
  * them into d_vals in element order per CSR entry (deterministic, no
@@ -343,9 +349,12 @@ CFEM_API int cfem_t10_joule_power(cfem_ctx *ctx, int64_t n_elems, const int32_t 
                                   const double *d_dn, const double *d_mref, double *d_power,
                                   double *d_q, void *stream);
 
-/* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST):
- * Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3 coefs),
- * thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or QP). */
+/* Isotropic elasticity (CFEM_OP_P1_ELAST / CFEM_OP_T10_ELAST): the
+ * element loops of assemble_elasticity_3d (elastic3d.py:105-189) and
+ * assemble_elasticity_tet10 (elastic_tet10.py:135-211) into 3x3 nodal
+ * blocks. Voigt [xx,yy,zz,yz,xz,xy] (elastic3d.py:26-34), body force b (3
+ * coefs), thermal strain alpha (T - T_ref) with T a coef (NODAL, ELEM or
+ * QP). */
 CFEM_API int cfem_assemble_elastic(cfem_ctx *ctx, const cfem_pattern *p, int32_t op,
                           const double *d_nodes, const int32_t *d_elems,
                           double E, double nu, const cfem_coef *body3,
@@ -393,7 +402,9 @@ CFEM_API int cfem_csr_add_subset(cfem_ctx *ctx, const cfem_pattern *p,
                         const int32_t *d_aptr, const int32_t *d_aidx,
                         const double *d_aval, int64_t n_rows,
                         double *d_vals, void *stream);
-/* y = alpha*A x + beta*y for block CSR (bs = 1 or 3), FP64. */
+/* y = alpha*A x + beta*y for block CSR (bs = 1 or 3), FP64: the
+ * matrix-vector products of the time marches (tet_heat.py:264,
+ * tet10.py:536-538, dynamics3d.py:177-186). */
 CFEM_API int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
               const int32_t *d_row_ptr, const int32_t *d_col,
               const double *d_vals, double alpha, const double *d_x,
@@ -415,7 +426,8 @@ CFEM_API int cfem_dirichlet_csr(cfem_ctx *ctx, int64_t n, const int32_t *d_indpt
                        int32_t *d_out_indices, double *d_out_vals,
                        double *d_rhs_out, int64_t *nnz_out, void *stream);
 
-/* FP32 operator for CFEM_SOLVE_MIXED in difference form: off-diagonal
+/* FP32 operator for CFEM_SOLVE_MIXED (a method change; the reference
+ * solves in FP64 only) in difference form: off-diagonal
  * blocks rounded to FP32 and, in each diagonal slot, the FP64 block row
  * sum s_i = sum_j A_ij rounded once. The solver applies it as
  * s_i p_i + sum_{j!=i} A_ij (p_j - p_i), which keeps constant vectors
