@@ -130,11 +130,8 @@ SIGNATURES = [
     ("cfem_face_exterior", ctypes.c_int,
      [_vp, _vp, _i32, _i32, _vp, _i64, _i64, _vp, _vp, ctypes.POINTER(_i64), _vp]),
     ("cfem_axpby", ctypes.c_int, [_vp, _i64, _f64, _vp, _f64, _vp, _vp, _vp]),
-    ("cfem_csr_add_subset", ctypes.c_int,
-     [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     ("cfem_spmv", ctypes.c_int,
      [_vp, _i64, _i32, _vp, _vp, _vp, _f64, _vp, _f64, _vp, _vp]),
-    ("cfem_to_fp32", ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
     ("cfem_dirichlet_csr", ctypes.c_int,
      [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
       ctypes.POINTER(_i64), _vp]),

@@ -67,13 +67,6 @@ __global__ void k_axpby(int64_t n, double a, const double *__restrict__ x,
     }
 }
 
-__global__ void k_to_fp32(int64_t n, const double *__restrict__ in,
-                          float *__restrict__ out) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    for (; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = (float)in[i];
-}
-
-// y = alpha A x + beta y, one thread per block row (setup-time use only).
 // y = alpha A x + beta y over a (block) CSR: SL = 8 lanes per (block) row,
 // lane s taking entries s, s + 8, ... (coalesced along the row), the lanes'
 // sums meeting in a fixed shuffle tree.
@@ -111,28 +104,6 @@ __global__ void k_spmv(int64_t n, const int32_t *__restrict__ rp,
                 const double yv = beta == 0.0 ? 0.0 : beta * y[r * BS + c];
                 y[r * BS + c] = alpha * acc[c] + yv;
             }
-    }
-}
-
-// Adds a canonical CSR addend into pattern values (subset pattern).
-__global__ void k_csr_add_subset(int64_t n, const int32_t *__restrict__ rp,
-                                 const int32_t *__restrict__ col,
-                                 const int32_t *__restrict__ aptr,
-                                 const int32_t *__restrict__ aidx,
-                                 const double *__restrict__ aval,
-                                 double *__restrict__ vals, int *bad) {
-    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    int32_t lo0 = rp[r], hi0 = rp[r + 1];
-    for (int32_t t = aptr[r]; t < aptr[r + 1]; ++t) {
-        int32_t c = aidx[t];
-        int32_t lo = lo0, hi = hi0;
-        while (lo < hi) {
-            int32_t mid = (lo + hi) >> 1;
-            if (col[mid] < c) lo = mid + 1; else hi = mid;
-        }
-        if (lo < hi0 && col[lo] == c) vals[lo] += aval[t];
-        else atomicExch(bad, 1);
     }
 }
 
@@ -322,20 +293,6 @@ int cfem_axpby(cfem_ctx *ctx, int64_t n, double a, const double *d_x,
     CFEM_API_END
 }
 
-int cfem_to_fp32(cfem_ctx *ctx, int64_t n, const double *d_in, float *d_out,
-                 void *stream) {
-    CFEM_API_BEGIN
-    CFEM_CHECK(ctx && d_in && d_out && n >= 0, CFEM_ERR_INVALID,
-               "cfem_to_fp32: bad args");
-    if (n == 0) return CFEM_OK;
-    CFEM_TRY(set_device(ctx->device));
-    unsigned g = grid_for(n, 256);
-    if (g > (unsigned)ctx->num_sms * 16) g = ctx->num_sms * 16;
-    CFEM_LAUNCH(k_to_fp32, g, 256, 0, (cudaStream_t)stream, n, d_in, d_out);
-    return CFEM_OK;
-    CFEM_API_END
-}
-
 int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
               const int32_t *d_row_ptr, const int32_t *d_col,
               const double *d_vals, double alpha, const double *d_x,
@@ -354,32 +311,6 @@ int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
     else
         CFEM_LAUNCH(k_spmv<3>, g, 128, 0, s, n_rows, d_row_ptr, d_col, d_vals,
                     alpha, d_x, beta, d_y);
-    return CFEM_OK;
-    CFEM_API_END
-}
-
-int cfem_csr_add_subset(cfem_ctx *ctx, const cfem_pattern *p,
-                        const int32_t *d_aptr, const int32_t *d_aidx,
-                        const double *d_aval, int64_t n_rows, double *d_vals,
-                        void *stream) {
-    CFEM_API_BEGIN
-    CFEM_CHECK(ctx && p && d_aptr && d_vals && n_rows == p->n_nodes,
-               CFEM_ERR_INVALID, "cfem_csr_add_subset: bad args");
-    if (n_rows == 0) return CFEM_OK;
-    CFEM_TRY(set_device(ctx->device));
-    cudaStream_t s = (cudaStream_t)stream;
-    int *d_bad = nullptr;
-    CFEM_TRY(tmp_alloc(&d_bad, 1, s));
-    CFEM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
-    CFEM_LAUNCH(k_csr_add_subset, grid_for(n_rows, 128), 128, 0, s, n_rows,
-                p->row_ptr, p->col, d_aptr, d_aidx, d_aval, d_vals, d_bad);
-    int bad = 0;
-    CFEM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int),
-                              cudaMemcpyDeviceToHost, s));
-    tmp_free(d_bad, s);
-    CFEM_CUDA(cudaStreamSynchronize(s));
-    CFEM_CHECK(!bad, CFEM_ERR_INVALID,
-               "addend has entries outside the mesh sparsity pattern");
     return CFEM_OK;
     CFEM_API_END
 }

@@ -394,14 +394,6 @@ CFEM_API int cfem_face_exterior(cfem_ctx *ctx, const int32_t *d_elems, int32_t n
  * tet_heat.py:239-240). */
 CFEM_API int cfem_axpby(cfem_ctx *ctx, int64_t n, double a, const double *d_x,
                double b, const double *d_y, double *d_out, void *stream);
-/* Adds a canonical scalar CSR (d_aptr, d_aidx, d_aval; n_rows rows) whose
- * pattern is a subset of the node pattern into d_vals (bs = 1), as
- * K + K_add in tet_heat.py:227-230. Sets CFEM_ERR_INVALID if an entry of
- * the addend is outside the pattern. */
-CFEM_API int cfem_csr_add_subset(cfem_ctx *ctx, const cfem_pattern *p,
-                        const int32_t *d_aptr, const int32_t *d_aidx,
-                        const double *d_aval, int64_t n_rows,
-                        double *d_vals, void *stream);
 /* y = alpha*A x + beta*y for block CSR (bs = 1 or 3), FP64: the
  * matrix-vector products of the time marches (tet_heat.py:264,
  * tet10.py:536-538, dynamics3d.py:177-186). */
@@ -409,9 +401,6 @@ CFEM_API int cfem_spmv(cfem_ctx *ctx, int64_t n_rows, int32_t bs,
               const int32_t *d_row_ptr, const int32_t *d_col,
               const double *d_vals, double alpha, const double *d_x,
               double beta, double *d_y, void *stream);
-/* FP32 copy of n values (the mixed solver's matrix). */
-CFEM_API int cfem_to_fp32(cfem_ctx *ctx, int64_t n, const double *d_in, float *d_out,
-                 void *stream);
 
 /* Dirichlet elimination of tet_poisson.py:72-110 on a scalar CSR:
  * fixed rows become identity rows, fixed columns are removed from free
