@@ -312,7 +312,7 @@ CFEM_API int cfem_face_geometry(cfem_ctx *ctx, int32_t npf, int64_t n_faces,
                                 void *stream);
 /* Boundary-face integrals (Neumann / traction loads, Robin terms;
  * tet_heat.py:136-172, tet10.py:362-464, elastic3d.py:171-186,
- * elastic_tet10.py:494-508). Per face, with the rule's weights d_w[q],
+ * elastic_tet10.py:192-205). Per face, with the rule's weights d_w[q],
  * shape values d_shape[q][a] and mass tables d_mt[q][a][b]:
  *   d_F[node_a ncomp + c] += A sum_q d_shape[q][a] (w_q d_load[(f nq + q) ncomp + c])
  *   d_vals[pos(node_a, node_b)] += A sum_q d_mt[q][a][b] (w_q d_h[f nq + q])
