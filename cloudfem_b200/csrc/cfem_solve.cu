@@ -3309,10 +3309,13 @@ static int plan_copies(cfem_pcg_plan *P, cudaStream_t s, int first = 0, int last
     return CFEM_OK;
 }
 
-// Sliced-ELL layout of every scalar system flagged `sell` (or `rsell`: an
-// FP64 copy for the residual phase of a mixed system): row orders and
+// Sliced-ELL layout of every system flagged `sell` (or `rsell`: an FP64
+// copy for the residual phases of a mixed scalar system): row orders and
 // slice offsets (k_sell_rank, then an exclusive scan of the slice sizes),
-// then room for the columns and values (filled by plan_copies).
+// then room for the columns and values (filled by plan_copies). Slot plans
+// keep two sets of row orders and offsets per slot (the placeholder
+// template ranks into set 0; assignments alternate) and room for any
+// system within the slot's capacity, bounded below.
 static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
     size_t meta = 0;
     int64_t max_sl = 0;
@@ -3353,7 +3356,7 @@ static int sell_layout(cfem_pcg_plan *P, cudaStream_t s) {
             soff = (int64_t *)(P->ws_smeta + o);
             o += align256((nsl + 1) * 8);
             if (P->slots) P->smeta[2 * i + (sets - 1 - k)] = {perm, sizes, soff};
-        }   // (slots: the template ranks into set 0, the last one taken)
+        }   // the last set taken (set 0 of a slot) is ranked now
         CFEM_CUDA(cudaMemsetAsync(sizes + nsl, 0, sizeof(int64_t), s));
         const int srt = P->ctx->sell_sort;
         if (rs == 32)
