@@ -194,7 +194,6 @@ def transient_heat_tet10(mesh, k=1.0, rho_cp=1.0, f=0.0, bc=None,
                          method="cn", *, precision="fp64", rtol=None,
                          max_iter=None):
     """Transient Tet10 heat conduction; returns (times, T_history)."""
-    import torch
     if method not in THETA:
         raise ValueError(f"unknown method {method!r}; "
                          f"use one of {sorted(THETA)}")

@@ -27,7 +27,6 @@ from scipy.special import erf
 from .. import _native as N
 from .._driver import THETA, solver_mode
 from ..device import BlockSystem, DeviceMesh, PcgPlan, centroids, ptr
-from ..fem.tet10 import assemble_mass_tet10
 from ..mesh.tet10_mesh import Tet10Mesh
 from . import em3d_tet10 as em
 from .em3d_tet10 import MU0, bh_secant_mu_r
