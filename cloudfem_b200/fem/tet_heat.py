@@ -18,8 +18,6 @@ Drop-in for cloudfem/fem/tet_heat.py:
   field (the reference factorises A_sys once with SuperLU).
 """
 
-import numpy as np
-
 from .. import _native as N
 from .. import _faces
 from .._driver import THETA, n_steps_of, theta_march
@@ -37,14 +35,6 @@ def assemble_mass_tet(mesh, rho_cp=1.0):
 def _boundary_faces(mesh, name):
     """(F, 3) exterior faces on mesh.boundaries[name]."""
     return DeviceMesh(mesh).boundary_faces(name)
-
-
-def _face_geometry(mesh, tri):
-    """Centroid and area of one triangular face (3 node indices)."""
-    p = mesh.nodes[np.asarray(tri)]
-    cen = p.mean(axis=0)
-    cr = np.cross(p[1] - p[0], p[2] - p[0])
-    return cen, 0.5 * float(np.linalg.norm(cr))
 
 
 def _scalar_fn(v):

@@ -60,11 +60,6 @@ def _dof_map(el):
     return (3 * el[:, None] + np.arange(3)).ravel()
 
 
-def _component_fns(vals):
-    return [(lambda x, y, z: 0.0) if v is None else
-            (v if callable(v) else (lambda x, y, z, v=v: v)) for v in vals]
-
-
 def _assemble(dm, mesh, op, E, nu, body, traction, T, alpha, T_ref, tet10):
     import torch
     vals, rhs = dm.assemble_elastic(op, E, nu, body=body, T=T, alpha=alpha,
@@ -139,17 +134,6 @@ def _as_vector(mesh, u):
 
 
 _EYE3 = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
-
-
-def _grads_p1(mesh):
-    p = mesh.nodes[mesh.elements]
-    m = np.stack([p[:, 1] - p[:, 0], p[:, 2] - p[:, 0],
-                  p[:, 3] - p[:, 0]], axis=2)
-    inv = np.linalg.inv(m)
-    G = np.empty((len(p), 4, 3))
-    G[:, 1:] = inv
-    G[:, 0] = -inv.sum(axis=1)
-    return G, p
 
 
 def _bmat(G):
