@@ -265,26 +265,6 @@ __device__ __forceinline__ bool block_inverse(const double a[9], const bool fx[3
     return true;
 }
 
-// z_c = M r for the dof this lane owns (lane = (row - r0) * BS + c). The
-// three residuals of a block row are exchanged by shuffles, so every lane
-// of the warp must call this.
-template <typename T, int BS>
-__device__ __forceinline__ T apply_prec_lane(const SysDev &S, int64_t row, int c,
-                                             int lane, T rv, bool valid) {
-    const T *dinv = (const T *)S.dinv;
-    if (BS == 3 && S.precond == CFEM_PRECOND_BLOCK) {
-        const int base = lane - c;
-        T r0 = __shfl_sync(0xffffffffu, rv, base >= 0 ? base : 0);
-        T r1 = __shfl_sync(0xffffffffu, rv, base + 1 < 32 ? base + 1 : 31);
-        T r2 = __shfl_sync(0xffffffffu, rv, base + 2 < 32 ? base + 2 : 31);
-        if (!valid) return (T)0;
-        const T *D = dinv + row * 9 + c * 3;
-        return ldcg(D) * r0 + ldcg(D + 1) * r1 + ldcg(D + 2) * r2;
-    }
-    if (!valid) return (T)0;
-    return ldcg(dinv + row * BS + c) * rv;
-}
-
 // ---------------------------------------------------------------- phase A
 // q = A p with p = zeta z + beta p_old (zeta = 1 except right after a
 // true-residual replacement, see advance()). Each lane group of LANES lanes works on
@@ -895,8 +875,9 @@ __device__ void finish_chunk(const SysDev &S, SysState *st, GridBar *bar,
     advance(S, st, bar, ph, tot);
 }
 
-// Which phases a kernel handles.
-enum { RUN_INIT = 0, RUN_ALL = 1, RUN_X = 2, RUN_B = 3 };
+// Which phases a kernel handles: INIT (k_pcg_init) or any (the persistent
+// kernel; the graph scheduler's kernels run their phases themselves).
+enum { RUN_INIT = 0, RUN_ALL = 1 };
 
 // (defined with the sliced-ELL kernels below)
 template <typename T>
@@ -920,17 +901,13 @@ __device__ void run_chunk(const SysDev &S, SysState *st, GridBar *bar, int ph,
         else
             phase_R<T, BS, true>(S, st, r0, r1, lane, part, &flag);
         bad = __any_sync(0xffffffffu, flag != 0);
-    } else if (RUN == RUN_B) {
-        phase_B<T, BS>(S, st, r0, r1, lane, part);
     } else {
         switch (ph) {
             case PH_A:
                 if (sizeof(T) == 4) phase_A<T, BS, true, 2>(S, st, r0, r1, lane, part);
                 else phase_A<T, BS, false, 1>(S, st, r0, r1, lane, part);
                 break;
-            case PH_B:
-                if (RUN == RUN_ALL) phase_B<T, BS>(S, st, r0, r1, lane, part);
-                break;
+            case PH_B: phase_B<T, BS>(S, st, r0, r1, lane, part); break;
             case PH_R: phase_R<T, BS, false>(S, st, r0, r1, lane, part, &bad); break;
             default: phase_zero<BS>(S, r0, r1, lane); break;
         }
@@ -947,8 +924,6 @@ __device__ __forceinline__ void dispatch(const SysDev *__restrict__ sys,
     const SysDev &S = sys[s];
     const int ph = RUN == RUN_INIT ? PH_INIT : *(volatile int32_t *)&st[s].phase;
     if (ph == PH_DONE) return;
-    if (RUN == RUN_X && ph == PH_B) return;
-    if (RUN == RUN_B && ph != PH_B) return;
     const int lc = c - S.chunk0;
     if (lc >= S.nchunks) return;   // a solve slot holding a smaller system
     if (S.mode == CFEM_SOLVE_MIXED) {
@@ -1063,18 +1038,6 @@ __global__ void k_mixed_matrix_batch(const MixJob *__restrict__ jobs, int nj, in
     }
     const MixJob &J = jobs[lo];
     mixed_row<BS>(J.rp, J.ci, J.v64, J.v32, valid ? g - J.row0 : 0, valid, (int)(t % MX));
-}
-
-// Graph scheduler: one warp per chunk, one launch per phase group. X runs
-// the SpMV-type phases (A, R, ZERO) and B the vector update; an iteration is
-// an X launch followed by a B launch.
-template <int RUN>
-__global__ void __launch_bounds__(256, 3)
-k_pcg_step(const SysDev *__restrict__ sys, SysState *st,
-           const int32_t *__restrict__ chunk_sys, int n_chunks, GridBar *bar) {
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (c >= n_chunks) return;
-    dispatch<RUN>(sys, st, bar, chunk_sys, c, threadIdx.x & 31);
 }
 
 
