@@ -12,7 +12,7 @@ position and fixed-order sums into the device load vector and matrix):
   rule (cloudfem/fem/tet10.py:295-435);
 * P1 traction, centroid value, t A / 3 per node (physics/elastic3d.py:171-186);
 * Tet10 traction with the 3-point degree-2 rule
-  (physics/elastic_tet10.py:351-357, 494-508).
+  (physics/elastic_tet10.py:50-66, 192-205).
 
 Coefficients given as host functions are evaluated at the points the
 device computed; constants never leave the host.
@@ -37,7 +37,7 @@ TRI_L6 = np.array([
     [0.816847572980459, 0.091576213509771, 0.091576213509771],
 ])
 TRI_W6 = np.array([0.223381589678011] * 3 + [0.109951743655322] * 3)
-# 3-point degree-2 rule (elastic_tet10.py:352-355)
+# 3-point degree-2 rule (elastic_tet10.py:50-53)
 TRI_L3 = np.array([[2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0],
                    [1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0],
                    [1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0]])
@@ -58,8 +58,6 @@ def face_shape6(l):
 
 FACE_N6 = face_shape6(TRI_L6)
 FACE_N3 = face_shape6(TRI_L3)
-
-
 
 
 def add_at(F, idx, vals):
