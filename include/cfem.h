@@ -193,7 +193,9 @@ CFEM_API int cfem_ctx_trim(cfem_ctx *ctx, uint64_t keep_bytes,
  * read when a solve plan is created. SELL_SORT (SpMV staging 3): 1
  * (default) sorts each window of 256 rows by length before cutting it into
  * slices of 32 (less padding), 0 keeps the rows in order (neighbouring
- * rows in a slice: gathers of p that share cache lines). SELL3_LANES
+ * rows in a slice: gathers of p that share cache lines); 3x3 solve slots
+ * read it again at each assignment, and their room assumes sorted windows
+ * (an unsorted layout that does not fit is refused). SELL3_LANES
  * (SpMV staging 3, 3x3 blocks): lanes that share one block row, each over
  * every L-th block of it (1, 2 or 4 (default); a slice holds 32 / L block
  * rows). SELL3_STAGED: 1 streams each slice's steps through a ring of
